@@ -1,0 +1,305 @@
+"""ctypes front-ends for the two checkers.
+
+* ``Oracle``       -- the CPU restatement (oracle/croma_oracle.c,
+                      built as oracle/_build/liboracle.so).
+* ``ReferenceCPU`` -- the reference's own CPU sources compiled as-is with
+                      oracle/ref_driver.c (oracle/_ref/libcroma_ref_np<N>.so);
+                      present only where the reference tree was available at
+                      build time.
+
+Test infrastructure: only tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py import this module, and only to check or time
+the reference algorithm.  Both expose the same methods with numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_D = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_I = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_U8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+_i = C.c_int
+_d = C.c_double
+
+
+class _Params(C.Structure):
+    _fields_ = [("nb", _i), ("pmin", _d), ("pmax", _d), ("pemin", _d), ("pemax", _d),
+                ("dpp_model", _i), ("ttd_tacc_model", _i), ("t_acc_direct_gyr", _d),
+                ("mach_limit", _d), ("psi", _d), ("eta_dpp_cap", _d), ("nsub_safety", _d),
+                ("nsub_max", _i), ("coeff_interp_min_steps", _i),
+                ("coeff_interp_max_segments", _i), ("reacc_window_mode", _i), ("f_eddy", _d),
+                ("t_off_gyr", _d), ("t_acc_off_gyr", _d)]
+
+
+class _RefConfig(C.Structure):
+    _fields_ = [("pmin", _d), ("pmax", _d), ("pemin", _d), ("pemax", _d), ("dpp_model", _i),
+                ("ttd_tacc_model", _i), ("t_acc_direct_gyr", _d), ("mach_limit", _d),
+                ("psi", _d), ("eta_dpp_cap", _d), ("nsub_safety", _d), ("nsub_max", _i),
+                ("coeff_interp_min_steps", _i), ("coeff_interp_max_segments", _i),
+                ("reacc_window_mode", _i), ("f_eddy", _d), ("t_off_gyr", _d),
+                ("t_acc_off_gyr", _d), ("nthreads", _i)]
+
+
+def _fill(struct, cfg, extra=None):
+    s = struct()
+    for name, _ in struct._fields_:
+        if name == "dpp_model":
+            s.dpp_model = cfg.dpp_model_id()
+        elif extra and name in extra:
+            setattr(s, name, extra[name])
+        elif hasattr(cfg, name):
+            setattr(s, name, getattr(cfg, name))
+    return s
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def _as_d(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+class _Common:
+    nb: int
+
+    def grid(self, species: int):
+        """(p, dp, E, pm1, pp1) for species 0 = proton, 1 = electron."""
+        out = np.empty(3 * self.nb + 2)
+        self._get_grid(species, out)
+        n = self.nb
+        return out[:n].copy(), out[n:2 * n].copy(), out[2 * n:3 * n].copy(), out[3 * n], out[3 * n + 1]
+
+    def ic_row(self, z: float):
+        row = np.empty(self.nb)
+        m1, p1 = _d(), _d()
+        self._ic_row(z, row, m1, p1)
+        return row, m1.value, p1.value
+
+    def pp_cache(self):
+        s = np.empty(self.nb); g = np.empty(self.nb); j = _i()
+        self._pp_cache(s, g, j)
+        return s, g, j.value
+
+    def secondary_kernel(self):
+        f = np.empty(self.nb * self.nb); m = np.empty(self.nb, dtype=np.int32)
+        self._sec(f, m)
+        return f.reshape(self.nb, self.nb), m
+
+    def nsub(self, dt_snap: float, bg: np.ndarray, rad_ic_row: np.ndarray):
+        n = bg.shape[1]
+        nsub = np.empty(n, np.int32); tgt = np.empty(n, np.int32); non = np.empty(n, np.int32)
+        cap = np.zeros(n, np.uint8)
+        err = self._nsub(n, dt_snap, _as_d(bg), _as_d(rad_ic_row), nsub, tgt, non, cap)
+        if err != 0:
+            raise RuntimeError(f"nsub failed: {err}")
+        return nsub, tgt, non, cap
+
+    def buckets(self, nsub: np.ndarray, non: np.ndarray):
+        n = nsub.size
+        bid = np.empty(n, np.int32); idx = np.empty(n, np.int32)
+        steps = np.empty(n, np.int32); ons = np.empty(n, np.int32)
+        offs = np.empty(n, np.int32); cnts = np.empty(n, np.int32); nb = _i()
+        self._buckets(n, np.ascontiguousarray(nsub, np.int32), np.ascontiguousarray(non, np.int32),
+                      bid, idx, steps, ons, offs, cnts, C.byref(nb))
+        k = nb.value
+        return dict(bucket_ids=bid, indices=idx, steps=steps[:k].copy(), onsteps=ons[:k].copy(),
+                    offsets=offs[:k].copy(), counts=cnts[:k].copy(), nbuckets=k)
+
+
+class Oracle(_Common):
+    """The CPU restatement (runtime bin count)."""
+
+    def __init__(self, cfg, threads: int = 0):
+        path = os.path.join(HERE, "_build", "liboracle.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle restated`")
+        L = C.CDLL(path)
+        self.lib = L
+        L.or_create.restype = _vp
+        L.or_create.argtypes = [C.POINTER(_Params)]
+        L.or_destroy.argtypes = [_vp]
+        L.or_get_grid.argtypes = [_vp, _i, _D]
+        L.or_ic_row.argtypes = [_vp, _d, _D, C.POINTER(_d), C.POINTER(_d)]
+        L.or_get_pp_cache.argtypes = [_vp, _D, _D, C.POINTER(_i)]
+        L.or_get_secondary_kernel.argtypes = [_vp, _D, _I]
+        L.or_get_beta_p.argtypes = [_vp, _D]
+        L.or_nsub.argtypes = [_vp, _i, _d, _D, _D, _I, _I, _I, _U8]
+        L.or_buckets.argtypes = [_i, _I, _I, _I, _I, _I, _I, _I, _I, C.POINTER(_i)]
+        L.or_coeff_segments.argtypes = [_vp, _i, _i]
+        L.or_cc_coeffs.argtypes = [_vp, _i, _d, _D, _D, _D, _D, _vp, _vp, _vp, _vp, _D, _D, _D, _D]
+        L.or_evolve_segment.argtypes = [_vp, _i, _i, _d, _i, _i, _i, _D, _D, _D, _D, _D, _D,
+                                        _vp, _vp, _D, _D]
+        L.or_snapshot.argtypes = [_vp, _i, _D, _D, _d, _d, _i, _d, _d, _D, _D, _vp, _vp, _D, _D,
+                                  _I, _I, _I, C.POINTER(_i)]
+        L.or_snapshot_with_ic.argtypes = [_vp, _i, _D, _D, _D, _D, _i, _d, _d, _D, _D, _vp, _vp,
+                                          _D, _D, _I, _I, _I, C.POINTER(_i)]
+        L.or_set_threads.argtypes = [_i]
+        self.cfg = cfg
+        self.nb = cfg.nb
+        p = _fill(_Params, cfg)
+        self.ctx = L.or_create(C.byref(p))
+        if not self.ctx:
+            raise RuntimeError("or_create failed")
+        if threads:
+            L.or_set_threads(threads)
+
+    def __del__(self):
+        try:
+            self.lib.or_destroy(self.ctx)
+        except Exception:
+            pass
+
+    def _get_grid(self, s, out): return self.lib.or_get_grid(self.ctx, s, out)
+    def _ic_row(self, z, row, m1, p1): return self.lib.or_ic_row(self.ctx, z, row, C.byref(m1), C.byref(p1))
+    def _pp_cache(self, s, g, j): return self.lib.or_get_pp_cache(self.ctx, s, g, C.byref(j))
+    def _sec(self, f, m): return self.lib.or_get_secondary_kernel(self.ctx, f, m)
+    def _nsub(self, *a): return self.lib.or_nsub(self.ctx, *a)
+    def _buckets(self, *a): return self.lib.or_buckets(*a)
+
+    def beta_p(self):
+        out = np.empty(self.nb)
+        self.lib.or_get_beta_p(self.ctx, out)
+        return out
+
+    def coeff_segments(self, nsub: int, allow_interp: bool) -> int:
+        return self.lib.or_coeff_segments(self.ctx, int(nsub), int(allow_interp))
+
+    def cc_coeffs(self, dt, bg, rad_ic, rad_ic_m1, rad_ic_p1, mass=None, dis=None, crp=None, cre=None):
+        n = bg.shape[1]; nb = self.nb
+        outs = [np.empty(3 * n * nb) for _ in range(4)]
+        err = self.lib.or_cc_coeffs(self.ctx, n, dt, _as_d(bg), _as_d(rad_ic), _as_d(rad_ic_m1),
+                                    _as_d(rad_ic_p1), _ptr(_as_d(mass)),
+                                    _ptr(None if dis is None else np.ascontiguousarray(dis, np.uint8)),
+                                    _ptr(_as_d(crp)), _ptr(_as_d(cre)), *outs)
+        if err != 0:
+            raise RuntimeError("cc_coeffs failed")
+        return [o.reshape(3, n, nb) for o in outs]
+
+    def evolve_segment(self, nstep, dt, windowed, on_start, on_end, bg, rad_ic, rad_ic_m1,
+                       rad_ic_p1, qpi, qepri, crp, cre, mass=None, dis=None):
+        n = bg.shape[1]
+        err = self.lib.or_evolve_segment(self.ctx, n, nstep, dt, int(windowed), on_start, on_end,
+                                         _as_d(bg), _as_d(rad_ic), _as_d(rad_ic_m1), _as_d(rad_ic_p1),
+                                         _as_d(qpi), _as_d(qepri), _ptr(_as_d(mass)),
+                                         _ptr(None if dis is None else np.ascontiguousarray(dis, np.uint8)),
+                                         crp, cre)
+        if err != 0:
+            raise RuntimeError("evolve_segment failed")
+
+    def snapshot(self, bg_curr, bg_next, z_curr, z_next, allow, dt, elapsed, qpi, qepri, crp, cre,
+                 mass=None, dis=None, ic=None):
+        """Advance crp/cre (cell-major, in place) through one snapshot.
+        ic = (ic_curr, ic_next) rows of nb+2 values to skip the IC integrals."""
+        n = bg_curr.shape[1]
+        nsub = np.empty(n, np.int32); non = np.empty(n, np.int32); bid = np.empty(n, np.int32)
+        nbk = _i()
+        dptr = _ptr(None if dis is None else np.ascontiguousarray(dis, np.uint8))
+        if ic is None:
+            err = self.lib.or_snapshot(self.ctx, n, _as_d(bg_curr), _as_d(bg_next), z_curr, z_next,
+                                       int(allow), dt, elapsed, _as_d(qpi), _as_d(qepri),
+                                       _ptr(_as_d(mass)), dptr, crp, cre, nsub, non, bid, C.byref(nbk))
+        else:
+            err = self.lib.or_snapshot_with_ic(self.ctx, n, _as_d(bg_curr), _as_d(bg_next),
+                                               _as_d(ic[0]), _as_d(ic[1]), int(allow), dt, elapsed,
+                                               _as_d(qpi), _as_d(qepri), _ptr(_as_d(mass)), dptr,
+                                               crp, cre, nsub, non, bid, C.byref(nbk))
+        if err != 0:
+            raise RuntimeError(f"oracle snapshot failed: {err}")
+        return nsub, non, bid, nbk.value
+
+
+def reference_available(nb: int) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", f"libcroma_ref_np{nb}.so"))
+
+
+class ReferenceCPU(_Common):
+    """The reference's own CPU code (compile-time bin count)."""
+
+    _loaded = {}
+
+    def __init__(self, cfg, threads: int = 0):
+        path = os.path.join(HERE, "_ref", f"libcroma_ref_np{cfg.nb}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref`")
+        L = C.CDLL(path)
+        self.lib = L
+        L.ref_configure.argtypes = [C.POINTER(_RefConfig)]
+        L.ref_get_grid.argtypes = [_i, _D]
+        L.ref_ic_row.argtypes = [_d, _D, C.POINTER(_d), C.POINTER(_d)]
+        L.ref_get_pp_cache.argtypes = [_D, _D, C.POINTER(_i)]
+        L.ref_get_secondary_kernel.argtypes = [_D, _I]
+        L.ref_get_beta_p.argtypes = [_D]
+        L.ref_nsub.argtypes = [_i, _d, _D, _D, _I, _I, _I, _U8]
+        L.ref_buckets.argtypes = [_i, _I, _I, _I, _I, _I, _I, _I, _I, C.POINTER(_i)]
+        L.ref_coeff_segments.argtypes = [_i, _i]
+        L.ref_cc_coeffs.argtypes = [_i, _d, _D, _D, _D, _D, _vp, _vp, _vp, _vp, _D, _D, _D, _D]
+        L.ref_evolve_segment.argtypes = [_i, _i, _d, _i, _i, _i, _D, _D, _D, _D, _D, _D, _vp, _vp,
+                                         _D, _D]
+        L.ref_snapshot.argtypes = [_i, _D, _D, _d, _d, _i, _d, _d, _D, _D, _vp, _vp, _D, _D, _I, _I,
+                                   _I, C.POINTER(_i)]
+        self.cfg = cfg
+        self.nb = cfg.nb
+        self.configure(threads)
+
+    def configure(self, threads: int = 0):
+        rc = _fill(_RefConfig, self.cfg, {"nthreads": threads})
+        if self.lib.ref_configure(C.byref(rc)) != 0:
+            raise RuntimeError("ref_configure failed")
+
+    def _get_grid(self, s, out): return self.lib.ref_get_grid(s, out)
+    def _ic_row(self, z, row, m1, p1): return self.lib.ref_ic_row(z, row, C.byref(m1), C.byref(p1))
+    def _pp_cache(self, s, g, j): return self.lib.ref_get_pp_cache(s, g, C.byref(j))
+    def _sec(self, f, m): return self.lib.ref_get_secondary_kernel(f, m)
+    def _nsub(self, n, dt, bg, row, nsub, tgt, non, cap):
+        return self.lib.ref_nsub(n, dt, bg, row, nsub, tgt, non, cap)
+    def _buckets(self, *a): return self.lib.ref_buckets(*a)
+
+    def threads(self) -> int:
+        return self.lib.ref_threads()
+
+    def coeff_segments(self, nsub: int, allow_interp: bool) -> int:
+        return self.lib.ref_coeff_segments(int(nsub), int(allow_interp))
+
+    def cc_coeffs(self, dt, bg, rad_ic, rad_ic_m1, rad_ic_p1, mass=None, dis=None, crp=None, cre=None):
+        n = bg.shape[1]; nb = self.nb
+        outs = [np.empty(3 * n * nb) for _ in range(4)]
+        err = self.lib.ref_cc_coeffs(n, dt, _as_d(bg), _as_d(rad_ic), _as_d(rad_ic_m1),
+                                     _as_d(rad_ic_p1), _ptr(_as_d(mass)),
+                                     _ptr(None if dis is None else np.ascontiguousarray(dis, np.uint8)),
+                                     _ptr(_as_d(crp)), _ptr(_as_d(cre)), *outs)
+        if err != 0:
+            raise RuntimeError("ref cc_coeffs failed")
+        return [o.reshape(3, n, nb) for o in outs]
+
+    def evolve_segment(self, nstep, dt, windowed, on_start, on_end, bg, rad_ic, rad_ic_m1,
+                       rad_ic_p1, qpi, qepri, crp, cre, mass=None, dis=None):
+        n = bg.shape[1]
+        err = self.lib.ref_evolve_segment(n, nstep, dt, int(windowed), on_start, on_end, _as_d(bg),
+                                          _as_d(rad_ic), _as_d(rad_ic_m1), _as_d(rad_ic_p1),
+                                          _as_d(qpi), _as_d(qepri), _ptr(_as_d(mass)),
+                                          _ptr(None if dis is None else np.ascontiguousarray(dis, np.uint8)),
+                                          crp, cre)
+        if err != 0:
+            raise RuntimeError("ref evolve_segment failed")
+
+    def snapshot(self, bg_curr, bg_next, z_curr, z_next, allow, dt, elapsed, qpi, qepri, crp, cre,
+                 mass=None, dis=None, ic=None):
+        if ic is not None:
+            raise ValueError("the reference computes its own IC rows")
+        n = bg_curr.shape[1]
+        nsub = np.empty(n, np.int32); non = np.empty(n, np.int32); bid = np.empty(n, np.int32)
+        nbk = _i()
+        m = _as_d(mass) if mass is not None else np.full(n, 1.0e7)
+        err = self.lib.ref_snapshot(n, _as_d(bg_curr), _as_d(bg_next), z_curr, z_next, int(allow), dt,
+                                    elapsed, _as_d(qpi), _as_d(qepri), _ptr(m),
+                                    _ptr(None if dis is None else np.ascontiguousarray(dis, np.uint8)),
+                                    crp, cre, nsub, non, bid, C.byref(nbk))
+        if err != 0:
+            raise RuntimeError(f"reference snapshot failed: {err}")
+        return nsub, non, bid, nbk.value

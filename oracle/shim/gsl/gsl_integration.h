@@ -1,0 +1,12 @@
+/*
+ * Stand-in for <gsl/gsl_integration.h>: declares only the GSL symbols that the
+ * reference hot-path sources reference.  Their definitions live in
+ * oracle/shim/ref_shims.c.  Test infrastructure, not product.
+ */
+#ifndef CROMA_ORACLE_SHIM_GSL_INTEGRATION_H
+#define CROMA_ORACLE_SHIM_GSL_INTEGRATION_H
+double gsl_sf_gamma(double x);
+double gsl_sf_hyperg_1F1(double a, double b, double x);
+double gsl_sf_hyperg_U(double a, double b, double x);
+double gsl_sf_synchrotron_1(double x);
+#endif

@@ -1,0 +1,98 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+The reference ships no tests, golden vectors or fixtures for this path, so
+its own CPU implementation -- compiled from its sources by
+`make -C oracle ref` into oracle/_ref/libcroma_ref_np<N>.so -- is run here on
+seeded synthetic tracers, and its outputs are stored with their inputs.
+
+Run from the repository root (needs the reference tree at build time):
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+Each case file golden_<name>.npz holds the run configuration, the inputs
+(backgrounds per snapshot, timeline, initial spectra) and the reference's
+outputs after every snapshot (nsub, n_on, bucket ids, spectra), plus the
+IC-cooling rows and the one-time grid tables.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from conftest import load_package  # noqa: E402
+
+load_package()
+from croma_fp_b200 import config, synth  # noqa: E402
+import pyoracle  # noqa: E402
+
+CASES = {
+    # name: (config factory kwargs, ntracer, first snapshot, nsnap run, seed, timeline length)
+    "c0_direct": (("config0", dict(nsub_max=500)), 16, 0, 3, 101, 100),
+    "c0_last": (("config0", dict(nsub_max=500)), 8, 98, 2, 102, 100),
+    "c0_nocap": (("config0", dict(nsub_max=0)), 3, 97, 1, 103, 100),
+    "c1_asa256": (("config1", dict()), 6, 10, 2, 104, 100),
+    "c1_asa128": (("config1", dict(nb=128)), 8, 0, 2, 105, 100),
+    "c2_ttd": (("config2", dict()), 8, 20, 2, 106, 100),
+    "c2_ttd_spect_window": (("config2", dict(ttd_tacc_model=0, reacc_window_mode=1, f_eddy=0.001)),
+                            8, 40, 2, 107, 100),
+    "c0_narrow": (("config0", dict(pemin=1.0, pemax=3.0, nsub_max=500)), 32, 30, 3, 109, 100),
+    "c1_narrow_window": (("config1", dict(nb=128, pmin=0.0, pmax=3.0, pemin=1.0, pemax=3.0,
+                                          reacc_window_mode=1, f_eddy=0.002)), 32, 50, 2, 110, 100),
+    "c4_asa512": (("config4", dict()), 3, 60, 1, 108, 100),
+}
+
+
+def make_case(name, spec):
+    (factory, kw), nt, isnap0, nrun, seed, nsnap = spec
+    cfg = getattr(config, factory)(**kw)
+    ref = pyoracle.ReferenceCPU(cfg)
+    w = synth.Workload(cfg, nt, nsnap, seed=seed)
+    gp, ge = ref.grid(0), ref.grid(1)
+    crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), nt, cfg.species)
+    qpi = np.zeros_like(crp)
+    qepri = np.zeros_like(cre)
+    out = dict(config=json.dumps(cfg.__dict__), ntracer=nt, isnap0=isnap0, nrun=nrun, seed=seed,
+               nsnap=nsnap, z=w.z, dt=w.dt, elapsed=w.elapsed, mass=w.mass,
+               crp0=crp.copy(), cre0=cre.copy())
+    bgs = []
+    for k in range(nrun + 1):
+        bgs.append(w.background(isnap0 + k) if isnap0 + k < nsnap else w.background(isnap0 + k - 1))
+    out["bg"] = np.stack(bgs)
+    for k in range(nrun):
+        isnap = isnap0 + k
+        allow = isnap + 1 < nsnap
+        cur = out["bg"][k]
+        nxt = out["bg"][k + 1] if allow else cur
+        z_next = w.z[isnap + 1] if allow else w.z[isnap]
+        ic = ref.ic_row(w.z[isnap])
+        out[f"ic_row_{k}"] = np.concatenate([ic[0], [ic[1], ic[2]]])
+        nsub, non, bid, nb = ref.snapshot(cur, nxt, float(w.z[isnap]), float(z_next), allow,
+                                          float(w.dt[isnap]), float(w.elapsed[isnap]), qpi, qepri,
+                                          crp, cre, mass=w.mass)
+        out[f"nsub_{k}"] = nsub
+        out[f"non_{k}"] = non
+        out[f"bucket_ids_{k}"] = bid
+        out[f"crp_{k}"] = crp.copy()
+        out[f"cre_{k}"] = cre.copy()
+    out["grid_p"] = np.concatenate([gp[0], gp[1], gp[2], [gp[3], gp[4]]])
+    out["grid_e"] = np.concatenate([ge[0], ge[1], ge[2], [ge[3], ge[4]]])
+    s, g, j = ref.pp_cache()
+    out["sigma_pp"], out["sigmoid_pp"], out["j_pp"] = s, g, j
+    fqe, npmin = ref.secondary_kernel()
+    out["np_min_qe"] = npmin
+    if cfg.nb == 128:
+        out["fqe"] = fqe
+    np.savez_compressed(os.path.join(HERE, f"golden_{name}.npz"), **out)
+    print(name, "nsub range", [(int(out[f"nsub_{k}"].min()), int(out[f"nsub_{k}"].max())) for k in range(nrun)])
+
+
+if __name__ == "__main__":
+    names = sys.argv[1:] or list(CASES)
+    for n in names:
+        make_case(n, CASES[n])
