@@ -1,0 +1,365 @@
+"""Benchmark: tracer-snapshot updates per second of the Fokker-Planck update.
+
+Workload (one "step" = one snapshot of every tracer on a GPU): 65,536
+seeded tracers per GPU, electron + proton spectra with 256 momentum bins
+each (protons p/(m_p c) in [1e-2, 1e6], electrons in [1e-1, 1e6]), ASA
+reacceleration, hadronic secondary electrons, sub-step cap 500, snapshots
+of a 100-snapshot z = 1 -> 0 timeline.  The spectra (2 x 256 x 65,536
+doubles = 268 MB) exceed the 126 MB L2, so no flush is needed between
+steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--path plain|fused]
+    python bench.py --impl reference      # the reference's CPU code, same workload
+
+Prints one JSON line (rank 0).  ``value`` is device-timed throughput with
+inputs resident in HBM; ``e2e`` runs the same snapshots through the C ABI
+with host buffers (background H2D, spectra up and down every snapshot, as
+the reference's rank-state path does).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+NTRACER = 65536
+NSNAP_TIMELINE = 100
+SEED = 20261203
+METRIC = "tracer-snapshot updates/s at <=1e-6 rel err vs FP64, chosen vs plain; p50/p99 latency"
+UNIT = "tracer-snapshot updates/s"
+
+
+def load_package():
+    if "croma_fp_b200" in sys.modules:
+        return sys.modules["croma_fp_b200"]
+    pkg_dir = os.path.join(ROOT, "croma-fp_b200")
+    spec = importlib.util.spec_from_file_location(
+        "croma_fp_b200", os.path.join(pkg_dir, "__init__.py"), submodule_search_locations=[pkg_dir])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["croma_fp_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_config():
+    load_package()
+    from croma_fp_b200 import config
+    return config.config1()
+
+
+def workload_desc(ntracer):
+    return {"workload": "batching: electron_proton with pp secondaries, 256 bins/species, ASA Dpp, "
+                        "nsub capped at 500, z=1->0 over 100 snapshots",
+            "tracers_per_gpu": ntracer, "bins_per_species": 256, "species": "electron_proton",
+            "dpp_mode": "asa", "nsub_max": 500, "precision": "fp64",
+            "l2_policy": "inputs larger than L2 (268 MB of spectra per GPU)"}
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, device_index=0):
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                self.samples.append(float(parts[1]))
+                self.max_mhz = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    self.reasons.add(n)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_reference_rate(cfg, budget_s=12.0, max_tracers=NTRACER):
+    """Reference CPU code (oracle/_ref, all host threads) on a bounded sample
+    of the workload: one snapshot of n tracers, n doubled until the snapshot
+    takes >= budget_s / 4.  The per-snapshot IC-cooling rows (independent of
+    the tracer count) are timed separately and the rate is extrapolated to
+    the full tracer count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    load_package()
+    from croma_fp_b200 import synth
+    kind = "reference" if pyoracle.reference_available(cfg.nb) else "port"
+    impl = pyoracle.ReferenceCPU(cfg) if kind == "reference" else pyoracle.Oracle(cfg)
+    cores = os.cpu_count() or 1
+    w = synth.Workload(cfg, max_tracers, NSNAP_TIMELINE, seed=SEED)
+    isnap = 10
+    t0 = time.perf_counter()
+    impl.ic_row(float(w.z[isnap]))
+    impl.ic_row(float(w.z[isnap + 1]))
+    t_ic = time.perf_counter() - t0
+    gp, ge = impl.grid(0), impl.grid(1)
+    n = 64
+    spent = 0.0
+    while True:
+        bgc = w.background(isnap)[:, :n].copy()
+        bgn = w.background(isnap + 1)[:, :n].copy()
+        crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), n, cfg.species)
+        q = np.zeros_like(crp)
+        t0 = time.perf_counter()
+        impl.snapshot(bgc, bgn, float(w.z[isnap]), float(w.z[isnap + 1]), True, float(w.dt[isnap]),
+                      float(w.elapsed[isnap]), q, np.zeros_like(cre), crp, cre, mass=w.mass[:n])
+        dt = time.perf_counter() - t0
+        spent += dt
+        if dt >= budget_s / 4 or n >= max_tracers or spent > budget_s:
+            break
+        n *= 2
+    per_tracer = max(dt - t_ic, 1e-9) / n
+    t_full = t_ic + per_tracer * max_tracers
+    return {"value": max_tracers / t_full, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"1 snapshot x {n} tracers in {dt:.2f} s (IC rows {t_ic:.2f} s/snapshot), "
+                      f"extrapolated to {max_tracers} tracers per snapshot"}, dt, n
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cfg = workload_config()
+    vals = []
+    first = None
+    for _ in range(args.warmup + args.steps):
+        res, dt, n = cpu_reference_rate(cfg, budget_s=max(2.0, 60.0 / max(1, args.steps + args.warmup)))
+        vals.append(res["value"])
+        first = first or res
+    timed = vals[args.warmup:] or vals
+    value = float(statistics.median(timed))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": NTRACER / value * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": workload_desc(NTRACER), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": first["cores"], "kind": first["kind"],
+                             "sample": first["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)), "measured"
+        except Exception:
+            pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def run_gpu_arm(args):
+    import torch
+    load_package()
+    from croma_fp_b200 import native, synth
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    cfg = workload_config()
+    nt = args.tracers
+    w = synth.Workload(cfg, nt, NSNAP_TIMELINE, seed=SEED + 7919 * rank)
+    fp = native.TracerFP(cfg, path=args.path, device=local)
+    gp, ge = fp.grid(0), fp.grid(1)
+    crp0, cre0 = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), nt, cfg.species)
+    fp.set_state(crp0, cre0, mass=w.mass)
+
+    nsteps_total = args.warmup + args.steps
+    first = 5
+    snaps = list(range(first, first + nsteps_total))
+    bg_dev = torch.empty((nsteps_total + 1, 8, nt), dtype=torch.float64, device=f"cuda:{local}")
+    for k in range(nsteps_total + 1):
+        bg_dev[k].copy_(torch.from_numpy(w.background(first + k)))
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(fp.stream(), device=f"cuda:{local}")
+
+    def do_snapshot(k, isnap):
+        fp.snapshot(bg_dev[k].data_ptr(), bg_dev[k + 1].data_ptr(), float(w.z[isnap]),
+                    float(w.z[isnap + 1]), True, float(w.dt[isnap]), float(w.elapsed[isnap]), sync=False)
+        return fp.last_launch_count()
+
+    for k in range(args.warmup):
+        do_snapshot(k, snaps[k])
+    fp.sync()
+    fp.set_kernel_timing(True)
+    fp.reset_kernel_stats()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches = 0
+    ev0.record(stream)
+    for k in range(args.warmup, nsteps_total):
+        launches += do_snapshot(k, snaps[k])
+    ev1.record(stream)
+    ev1.synchronize()
+    fp.sync()
+    torch.cuda.synchronize()
+    clocks.stop()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    evolve_ms, evolve_n = fp.kernel_stats("evolve")
+    coeff_ms, coeff_n = fp.kernel_stats("coeff")
+    sec_ms, sec_n = fp.kernel_stats("secondary")
+    fp.set_kernel_timing(False)
+    sched = fp.schedule()
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * nt * args.steps / (ms_max / 1e3)
+
+    # ---- e2e through the C ABI with host buffers ----
+    crp_h, cre_h = fp.get_state()
+    bg_host = [w.background(first + k) for k in range(nsteps_total + 1)]
+    e2e_times = []
+    h2d = d2h = 0
+    for k in range(min(args.steps, 3)):
+        isnap = snaps[k]
+        t0 = time.perf_counter()
+        fp.set_state(crp_h, cre_h, mass=w.mass)
+        fp.snapshot(bg_host[k], bg_host[k + 1], float(w.z[isnap]), float(w.z[isnap + 1]), True,
+                    float(w.dt[isnap]), float(w.elapsed[isnap]), sync=False)
+        crp_h, cre_h = fp.get_state()
+        e2e_times.append(time.perf_counter() - t0)
+        h2d = crp_h.nbytes + cre_h.nbytes + w.mass.nbytes + bg_host[k].nbytes * 2
+        d2h = crp_h.nbytes + cre_h.nbytes
+    e2e_s = statistics.median(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * nt / e2e_s
+
+    # ---- roofline of the dominant kernel ----
+    peaks, peak_kind = measured_peaks()
+    nsub = sched["nsub"].astype(np.float64)
+    nb = cfg.nb
+    nspecies = 2
+    if args.path == "plain":
+        # algorithmic bytes of the sub-step kernels (reference data contract):
+        # a, b, c, source and N read, N written per row per sub-step
+        bytes_per_snapshot = float(np.sum(nsub)) * nspecies * nb * 6 * 8
+        alg_bytes_total = bytes_per_snapshot * args.steps
+        per_launch = alg_bytes_total / max(1, evolve_n)
+        avg_launch_ms = evolve_ms / max(1, evolve_n)
+        achieved = per_launch / (avg_launch_ms / 1e3) / 1e9
+        peak = float(peaks.get("hbm_gbs", 6650.0))
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                    "kernel": "plain_steps_kernel", "launches": evolve_n,
+                    "kernel_ms_total": evolve_ms, "share_of_step": evolve_ms / ms if ms > 0 else None,
+                    "alg_bytes_per_launch": per_launch,
+                    "alg_bytes_rule": "per tracer-snapshot: nsub x 2 species x nb x 6 doubles"}
+    else:
+        roofline = {"bound": "hbm", "achieved": None, "peak": None, "unit": "GB/s", "frac": None,
+                    "traffic": None}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu, _, _ = cpu_reference_rate(cfg, budget_s=args.cpu_budget)
+        except Exception as e:  # the checker library may be absent
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "unavailable",
+                   "sample": f"{type(e).__name__}: {e}"}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": dict(workload_desc(nt), parallelism=f"dp{world} (independent tracer shards)",
+                           path=args.path),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "api": "croma_b200_set_state/snapshot/get_state"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "gpu_launches": int(launches),
+            "kernel_ms": {"evolve": evolve_ms, "coeff": coeff_ms, "secondary": sec_ms},
+            "nsub": {"min": int(nsub.min()), "mean": float(nsub.mean()), "max": int(nsub.max())},
+            "nbuckets": sched["nbuckets"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    fp.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--path", default="plain", choices=["plain", "fused"])
+    ap.add_argument("--tracers", type=int, default=NTRACER)
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,415 @@
+// api.cu -- the native C ABI (include/croma_b200.h).
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "croma_ctx.cuh"
+
+struct CromaB200Context {
+    croma::Context impl;
+};
+
+namespace croma {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    set_error(std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) +
+              ") at " + what);
+    return -3;
+}
+
+cudaEvent_t pooled_event(Context &ctx)
+{
+    cudaEvent_t e = nullptr;
+    if (!ctx.event_pool.empty()) {
+        e = ctx.event_pool.back();
+        ctx.event_pool.pop_back();
+        return e;
+    }
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+void timed_begin(Context &ctx, int kind, cudaEvent_t *start)
+{
+    (void)kind;
+    *start = nullptr;
+    if (!ctx.timing) return;
+    *start = pooled_event(ctx);
+    if (*start) cudaEventRecord(*start, ctx.stream);
+}
+
+void timed_end(Context &ctx, int kind, cudaEvent_t start)
+{
+    if (!ctx.timing || !start) return;
+    cudaEvent_t stop = pooled_event(ctx);
+    if (!stop) return;
+    cudaEventRecord(stop, ctx.stream);
+    ctx.timed.push_back({kind, start, stop});
+}
+
+namespace {
+
+void free_state(Context &c)
+{
+    cudaFree(c.d_crp); cudaFree(c.d_cre); cudaFree(c.d_qpi); cudaFree(c.d_qepri);
+    cudaFree(c.d_mass); cudaFree(c.d_dis); cudaFree(c.d_bg); cudaFree(c.d_layout_tmp);
+    c.d_crp = c.d_cre = c.d_qpi = c.d_qepri = c.d_mass = c.d_bg = c.d_layout_tmp = nullptr;
+    c.d_dis = nullptr;
+    cudaFree(c.d_coef); cudaFree(c.d_inje); cudaFree(c.d_seg_ngas);
+    c.d_coef = c.d_inje = c.d_seg_ngas = nullptr;
+    cudaFree(c.d_sched_int); cudaFree(c.d_capped); cudaFree(c.d_cub_tmp);
+    cudaFree(c.d_keys); cudaFree(c.d_vals);
+    c.d_sched_int = nullptr; c.d_capped = nullptr; c.d_cub_tmp = nullptr;
+    c.d_keys = nullptr; c.d_vals = nullptr;
+    c.cap = c.ntracer = 0;
+}
+
+int check_err(Context &c)
+{
+    unsigned err = 0;
+    CROMA_CUDA(cudaMemcpyAsync(&err, c.d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream));
+    CROMA_CUDA(cudaStreamSynchronize(c.stream));
+    if (err) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "kernel reported numerical failure (bits 0x%x: 1 singular pivot, "
+                 "2 NaN at the CC boundary, 4 CMB bound iteration)", err);
+        set_error(buf);
+        CROMA_CUDA(cudaMemsetAsync(c.d_err, 0, sizeof(unsigned), c.stream));
+        return -2;
+    }
+    return 0;
+}
+
+// IC row slot for redshift z (computed on demand), returns device pointer.
+int ic_slot(Context &c, double z, int avoid_slot, double **out)
+{
+    for (int k = 0; k < 2; k++)
+        if (c.ic_valid[k] && c.ic_z[k] == z) { *out = c.d_ic + (size_t)k * kIcSlotDoubles; return k; }
+    const int k = (avoid_slot == 0) ? 1 : 0;
+    int rc = ic_rows(c, z, c.d_ic + (size_t)k * kIcSlotDoubles);
+    if (rc != 0) return rc < 0 ? rc - 100 : -100;
+    c.ic_valid[k] = 1;
+    c.ic_z[k] = z;
+    *out = c.d_ic + (size_t)k * kIcSlotDoubles;
+    c.last_launches += 1;
+    return k;
+}
+
+}  // namespace
+}  // namespace croma
+
+using namespace croma;
+
+extern "C" {
+
+const char *croma_b200_last_error(void) { return g_last_error.c_str(); }
+
+int croma_b200_nb(void) { return NB; }
+
+int croma_b200_create(const CromaB200Config *cfg, int device, CromaB200Context **out)
+{
+    if (cfg == nullptr || out == nullptr) { set_error("null argument"); return -1; }
+    if (cfg->nb != NB) { set_error("config nb does not match this library's bin count"); return -1; }
+    if (cfg->path != CROMA_PATH_PLAIN && cfg->path != CROMA_PATH_FUSED) { set_error("unknown path"); return -1; }
+    if (cfg->dpp_model < 1 || cfg->dpp_model > 4) { set_error("unknown dpp_model"); return -1; }
+    if ((cfg->species_mask & 3) == 0) { set_error("empty species mask"); return -1; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        set_error("no CUDA device available");
+        return -3;
+    }
+    if (device < 0 || device >= ndev) { set_error("device index out of range"); return -1; }
+    CROMA_CUDA(cudaSetDevice(device));
+    auto *h = new (std::nothrow) CromaB200Context();
+    if (!h) { set_error("host allocation failed"); return -4; }
+    Context &c = h->impl;
+    c.cfg = *cfg;
+    c.device = device;
+    ModelParams &mp = c.mp;
+    mp.species_mask = cfg->species_mask & 3;
+    mp.dpp_model = cfg->dpp_model;
+    mp.ttd_brunetti16 = cfg->ttd_tacc_model == 1;
+    mp.t_acc_direct_gyr = cfg->t_acc_direct_gyr;
+    mp.mach_limit = cfg->mach_limit;
+    mp.psi3 = pow(cfg->psi, 3.0);
+    mp.eta_dpp_cap = cfg->eta_dpp_cap;
+    mp.nsub_safety = cfg->nsub_safety;
+    mp.nsub_max = cfg->nsub_max;
+    mp.interp_min_steps = cfg->coeff_interp_min_steps;
+    mp.interp_max_segments = cfg->coeff_interp_max_segments;
+    mp.window_centred = cfg->reacc_window_mode == 1;
+    mp.f_eddy = cfg->f_eddy;
+    mp.t_off_gyr = cfg->t_off_gyr;
+    mp.t_acc_off_gyr = cfg->t_acc_off_gyr;
+    int rc = 0;
+    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) rc = -3;
+    if (rc == 0 && cudaMalloc(&c.d_err, sizeof(unsigned)) != cudaSuccess) rc = -3;
+    if (rc == 0 && cudaMemsetAsync(c.d_err, 0, sizeof(unsigned), c.stream) != cudaSuccess) rc = -3;
+    if (rc == 0 && cudaMalloc(&c.d_ic, 2 * (size_t)kIcSlotDoubles * sizeof(double)) != cudaSuccess) rc = -3;
+    if (rc == 0) rc = build_tables(c);
+    if (rc != 0) {
+        if (g_last_error.empty()) set_error("context creation failed");
+        croma_b200_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return 0;
+}
+
+void croma_b200_destroy(CromaB200Context *h)
+{
+    if (!h) return;
+    Context &c = h->impl;
+    cudaSetDevice(c.device);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    free_state(c);
+    for (auto &t : c.timed) { cudaEventDestroy(t.start); cudaEventDestroy(t.stop); }
+    for (auto e : c.event_pool) cudaEventDestroy(e);
+    cudaFree(c.d_tables);
+    cudaFree(c.d_ic);
+    cudaFree(c.d_err);
+    if (c.stream) cudaStreamDestroy(c.stream);
+    delete h;
+}
+
+int croma_b200_reserve(CromaB200Context *h, int ntracer)
+{
+    if (!h || ntracer <= 0) { set_error("invalid reserve"); return -1; }
+    Context &c = h->impl;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    if (ntracer == c.cap) { c.ntracer = ntracer; return 0; }
+    CROMA_CUDA(cudaStreamSynchronize(c.stream));
+    free_state(c);
+    const size_t n = (size_t)ntracer, st = (size_t)NB * n * sizeof(double);
+    CROMA_CUDA(cudaMalloc(&c.d_crp, st));
+    CROMA_CUDA(cudaMalloc(&c.d_cre, st));
+    CROMA_CUDA(cudaMalloc(&c.d_qpi, st));
+    CROMA_CUDA(cudaMalloc(&c.d_qepri, st));
+    CROMA_CUDA(cudaMalloc(&c.d_mass, n * sizeof(double)));
+    CROMA_CUDA(cudaMalloc(&c.d_dis, n));
+    CROMA_CUDA(cudaMalloc(&c.d_bg, 2 * (size_t)kNbg * n * sizeof(double)));
+    CROMA_CUDA(cudaMalloc(&c.d_layout_tmp, st));
+    CROMA_CUDA(cudaMemsetAsync(c.d_crp, 0, st, c.stream));
+    CROMA_CUDA(cudaMemsetAsync(c.d_cre, 0, st, c.stream));
+    CROMA_CUDA(cudaMemsetAsync(c.d_qpi, 0, st, c.stream));
+    CROMA_CUDA(cudaMemsetAsync(c.d_qepri, 0, st, c.stream));
+    CROMA_CUDA(cudaMemsetAsync(c.d_mass, 0, n * sizeof(double), c.stream));
+    CROMA_CUDA(cudaMemsetAsync(c.d_dis, 0, n, c.stream));
+    c.cap = ntracer;
+    c.ntracer = ntracer;
+    c.has_sources = 0;
+    int rc = schedule_reserve(c, ntracer);
+    if (rc == 0) rc = plain_reserve(c, ntracer);
+    if (rc != 0) { free_state(c); return rc; }
+    return 0;
+}
+
+int croma_b200_set_state(CromaB200Context *h, int ntracer, const double *crp, const double *cre,
+                         const double *qpi, const double *qepri, const double *mass,
+                         const unsigned char *dis)
+{
+    if (!h || ntracer <= 0) { set_error("invalid set_state"); return -1; }
+    Context &c = h->impl;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    if (ntracer != c.cap) {
+        int rc = croma_b200_reserve(h, ntracer);
+        if (rc) return rc;
+    }
+    const size_t st = (size_t)NB * ntracer * sizeof(double);
+    int rc = 0;
+    if (crp && (rc = transpose_to_device(c, crp, c.d_crp, ntracer))) return rc;
+    if (cre && (rc = transpose_to_device(c, cre, c.d_cre, ntracer))) return rc;
+    if (qpi) { if ((rc = transpose_to_device(c, qpi, c.d_qpi, ntracer))) return rc; }
+    else CROMA_CUDA(cudaMemsetAsync(c.d_qpi, 0, st, c.stream));
+    if (qepri) { if ((rc = transpose_to_device(c, qepri, c.d_qepri, ntracer))) return rc; }
+    else CROMA_CUDA(cudaMemsetAsync(c.d_qepri, 0, st, c.stream));
+    c.has_sources = (qpi != nullptr || qepri != nullptr);
+    if (mass) CROMA_CUDA(cudaMemcpyAsync(c.d_mass, mass, ntracer * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    if (dis) CROMA_CUDA(cudaMemcpyAsync(c.d_dis, dis, ntracer, cudaMemcpyHostToDevice, c.stream));
+    else CROMA_CUDA(cudaMemsetAsync(c.d_dis, 0, ntracer, c.stream));
+    CROMA_CUDA(cudaStreamSynchronize(c.stream));
+    return 0;
+}
+
+int croma_b200_get_state(CromaB200Context *h, double *crp, double *cre)
+{
+    if (!h) { set_error("null context"); return -1; }
+    Context &c = h->impl;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    int rc = 0;
+    if (crp && (rc = transpose_to_host(c, c.d_crp, crp, c.cap))) return rc;
+    CROMA_CUDA(cudaStreamSynchronize(c.stream));
+    if (cre && (rc = transpose_to_host(c, c.d_cre, cre, c.cap))) return rc;
+    CROMA_CUDA(cudaStreamSynchronize(c.stream));
+    return check_err(c);
+}
+
+int croma_b200_snapshot(CromaB200Context *h, const CromaB200Snapshot *s, int sync)
+{
+    if (!h || !s || !s->bg_curr) { set_error("invalid snapshot arguments"); return -1; }
+    Context &c = h->impl;
+    if (c.cap <= 0) { set_error("reserve/set_state before snapshot"); return -1; }
+    if (!(s->dt_snap > 0.0)) { set_error("dt_snap must be positive"); return -1; }
+    CROMA_CUDA(cudaSetDevice(c.device));
+    c.last_launches = 0;
+    const size_t n = (size_t)c.cap;
+    const int allow = s->allow_interp ? 1 : 0;
+    const double *bg_curr = s->bg_curr, *bg_next = allow && s->bg_next ? s->bg_next : s->bg_curr;
+    if (!s->bg_on_device) {
+        CROMA_CUDA(cudaMemcpyAsync(c.d_bg, bg_curr, kNbg * n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        if (bg_next != bg_curr)
+            CROMA_CUDA(cudaMemcpyAsync(c.d_bg + kNbg * n, bg_next, kNbg * n * sizeof(double),
+                                       cudaMemcpyHostToDevice, c.stream));
+        bg_curr = c.d_bg;
+        bg_next = (bg_next != s->bg_curr) ? c.d_bg + kNbg * n : c.d_bg;
+    }
+    double *ic_cur = nullptr, *ic_nxt = nullptr;
+    int k_cur = ic_slot(c, s->z_curr, -1, &ic_cur);
+    if (k_cur < 0) return -2;
+    if (allow) {
+        int k_nxt = ic_slot(c, s->z_next, k_cur, &ic_nxt);
+        if (k_nxt < 0) return -2;
+    } else {
+        ic_nxt = ic_cur;
+    }
+    SnapArgs a;
+    a.ntracer = c.cap;
+    a.bg_curr = bg_curr;
+    a.bg_next = bg_next;
+    a.ic_curr = ic_cur;
+    a.ic_next = ic_nxt;
+    a.allow_interp = allow;
+    a.dt_snap = s->dt_snap;
+    a.elapsed = s->elapsed_gyr;
+    a.crp = c.d_crp;
+    a.cre = c.d_cre;
+    a.qpi = c.has_sources ? c.d_qpi : nullptr;
+    a.qepri = c.has_sources ? c.d_qepri : nullptr;
+    a.mass = c.d_mass;
+    a.dis = c.d_dis;
+    a.sched = c.sched;
+    a.err = c.d_err;
+    int rc = run_schedule(c, a);
+    if (rc) return rc;
+    if (c.cfg.path == CROMA_PATH_PLAIN) rc = run_plain(c, a);
+    else { set_error("fused path not built into this library"); return -1; }
+    if (rc) return rc;
+    if (sync) return check_err(c);
+    return 0;
+}
+
+int croma_b200_get_schedule(CromaB200Context *h, int *nsub, int *non, int *target, int *bucket_ids,
+                            int *bucket_indices, int *nbuckets)
+{
+    if (!h) { set_error("null context"); return -1; }
+    Context &c = h->impl;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    const size_t n = (size_t)c.cap * sizeof(int);
+    if (nsub) CROMA_CUDA(cudaMemcpyAsync(nsub, c.sched.nsub, n, cudaMemcpyDeviceToHost, c.stream));
+    if (non) CROMA_CUDA(cudaMemcpyAsync(non, c.sched.non, n, cudaMemcpyDeviceToHost, c.stream));
+    if (target) CROMA_CUDA(cudaMemcpyAsync(target, c.sched.target, n, cudaMemcpyDeviceToHost, c.stream));
+    if (bucket_ids) CROMA_CUDA(cudaMemcpyAsync(bucket_ids, c.sched.bucket_ids, n, cudaMemcpyDeviceToHost, c.stream));
+    if (bucket_indices)
+        CROMA_CUDA(cudaMemcpyAsync(bucket_indices, c.sched.bucket_indices, n, cudaMemcpyDeviceToHost, c.stream));
+    if (nbuckets) CROMA_CUDA(cudaMemcpyAsync(nbuckets, c.sched.nbuckets, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CROMA_CUDA(cudaStreamSynchronize(c.stream));
+    return 0;
+}
+
+int croma_b200_ic_row(CromaB200Context *h, double z, double *row_m1_p1)
+{
+    if (!h || !row_m1_p1) { set_error("null argument"); return -1; }
+    Context &c = h->impl;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    double *d = nullptr;
+    int k = ic_slot(c, z, -1, &d);
+    if (k < 0) return -2;
+    CROMA_CUDA(cudaMemcpyAsync(row_m1_p1, d, (NB + 2) * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    CROMA_CUDA(cudaStreamSynchronize(c.stream));
+    return 0;
+}
+
+int croma_b200_get_grid(CromaB200Context *h, int species, double *out)
+{
+    if (!h || !out || species < 0 || species > 1) { set_error("invalid argument"); return -1; }
+    Context &c = h->impl;
+    memcpy(out, c.h_p[species].data(), NB * sizeof(double));
+    memcpy(out + NB, c.h_dp[species].data(), NB * sizeof(double));
+    memcpy(out + 2 * NB, c.h_E[species].data(), NB * sizeof(double));
+    out[3 * NB] = c.h_pm1[species];
+    out[3 * NB + 1] = c.h_pp1[species];
+    return 0;
+}
+
+int croma_b200_get_secondary_kernel(CromaB200Context *h, double *fqe, int *np_min_qe)
+{
+    if (!h) { set_error("null context"); return -1; }
+    Context &c = h->impl;
+    if (fqe) memcpy(fqe, c.h_fqe.data(), c.h_fqe.size() * sizeof(double));
+    if (np_min_qe) memcpy(np_min_qe, c.h_np_min_qe.data(), c.h_np_min_qe.size() * sizeof(int));
+    return 0;
+}
+
+void *croma_b200_stream(CromaB200Context *h) { return h ? (void *)h->impl.stream : nullptr; }
+
+int croma_b200_sync(CromaB200Context *h)
+{
+    if (!h) { set_error("null context"); return -1; }
+    CROMA_CUDA(cudaSetDevice(h->impl.device));
+    return check_err(h->impl);
+}
+
+int croma_b200_state_device(CromaB200Context *h, double **crp, double **cre)
+{
+    if (!h) { set_error("null context"); return -1; }
+    if (crp) *crp = h->impl.d_crp;
+    if (cre) *cre = h->impl.d_cre;
+    return 0;
+}
+
+int croma_b200_last_launch_count(CromaB200Context *h) { return h ? h->impl.last_launches : 0; }
+
+int croma_b200_set_kernel_timing(CromaB200Context *h, int enable)
+{
+    if (!h) { set_error("null context"); return -1; }
+    h->impl.timing = enable ? 1 : 0;
+    return 0;
+}
+
+int croma_b200_kernel_stats(CromaB200Context *h, int kind, double *total_ms, long long *launches)
+{
+    if (!h || kind < 0 || kind > 3) { set_error("invalid argument"); return -1; }
+    Context &c = h->impl;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    CROMA_CUDA(cudaStreamSynchronize(c.stream));
+    for (auto &t : c.timed) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, t.start, t.stop) == cudaSuccess) {
+            c.kernel_ms[t.kind] += ms;
+            c.kernel_launches[t.kind] += 1;
+        }
+        c.event_pool.push_back(t.start);
+        c.event_pool.push_back(t.stop);
+    }
+    c.timed.clear();
+    if (total_ms) *total_ms = c.kernel_ms[kind];
+    if (launches) *launches = c.kernel_launches[kind];
+    return 0;
+}
+
+int croma_b200_reset_kernel_stats(CromaB200Context *h)
+{
+    if (!h) { set_error("null context"); return -1; }
+    Context &c = h->impl;
+    double ms;
+    croma_b200_kernel_stats(h, 0, &ms, nullptr);
+    for (int k = 0; k < 4; k++) { c.kernel_ms[k] = 0.0; c.kernel_launches[k] = 0; }
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,151 @@
+// croma_ctx.cuh -- the library context: device tables, resident state,
+// workspaces and the per-snapshot schedule.  Internal header.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/croma_b200.h"
+#include "croma_phys.cuh"
+
+#ifndef CROMA_NB
+#error "CROMA_NB (bins per species) must be defined at compile time"
+#endif
+
+namespace croma {
+
+constexpr int NB = CROMA_NB;
+static_assert(NB == 128 || NB == 256 || NB == 512, "supported bin counts: 128, 256, 512");
+
+constexpr int kNbg = 8;   // background fields per tracer
+// One IC slot: the row (nb), its ghost edges (2), then scratch for the
+// outer CMB abscissae of b_IC (up to 2049 points).
+constexpr int kIcSlotDoubles = NB + 2 + 2049;
+
+// Per-tracer schedule written by the sub-step estimator.
+struct Schedule {
+    int *nsub, *non, *target, *nseg;
+    unsigned char *capped;
+    int *bucket_ids, *bucket_indices;
+    int *nbuckets;            // device scalar
+};
+
+// Everything a snapshot kernel needs, passed by value.
+struct SnapArgs {
+    int ntracer;
+    const double *bg_curr, *bg_next;   // [8][ntracer]
+    const double *ic_curr, *ic_next;   // [nb+2] each
+    int allow_interp;
+    double dt_snap, elapsed;
+    double *crp, *cre;                 // [nb][ntracer]
+    const double *qpi, *qepri;         // [nb][ntracer] or null (zero)
+    const double *mass;                // [ntracer]
+    const unsigned char *dis;          // [ntracer] or null
+    Schedule sched;
+    unsigned *err;
+};
+
+struct ModelParams {
+    int species_mask;
+    int dpp_model;
+    int ttd_brunetti16;
+    double t_acc_direct_gyr;
+    double mach_limit;
+    double psi3;                 // psi^3
+    double eta_dpp_cap;
+    double nsub_safety;
+    int nsub_max;
+    int interp_min_steps, interp_max_segments;
+    int window_centred;
+    double f_eddy, t_off_gyr, t_acc_off_gyr;
+};
+
+struct Context {
+    CromaB200Config cfg{};
+    ModelParams mp{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+
+    // host copies of the grids (p, dp, E per species; pm1/pp1)
+    std::vector<double> h_p[2], h_dp[2], h_E[2];
+    double h_pm1[2] = {0, 0}, h_pp1[2] = {0, 0};
+    std::vector<double> h_fqe;        // [nb][nb] transposed [jp][je]
+    std::vector<int> h_np_min_qe;
+
+    double *d_tables = nullptr;       // one block holding every grid table
+    GridTables gt{};
+    IcConsts icc{};
+
+    // IC rows: [2][nb+2], keyed by redshift
+    double *d_ic = nullptr;
+    double ic_z[2] = {0, 0};
+    int ic_valid[2] = {0, 0};
+    int ic_slot_curr = 0;
+
+    // resident state (momentum-major [nb][cap])
+    int cap = 0, ntracer = 0;
+    double *d_crp = nullptr, *d_cre = nullptr;
+    double *d_qpi = nullptr, *d_qepri = nullptr;
+    double *d_mass = nullptr;
+    unsigned char *d_dis = nullptr;
+    int has_sources = 0;
+    double *d_bg = nullptr;           // [2][8][cap] staging for host backgrounds
+
+    // schedule
+    int *d_sched_int = nullptr;
+    unsigned char *d_capped = nullptr;
+    Schedule sched{};
+    void *d_cub_tmp = nullptr;
+    size_t cub_tmp_bytes = 0;
+    unsigned long long *d_keys = nullptr, *d_keys_alt = nullptr;
+    int *d_vals = nullptr, *d_vals_alt = nullptr, *d_seg_aux = nullptr;
+
+    // plain-path workspace
+    double *d_coef = nullptr;         // [2 sets][2 species][3][nb][cap]
+    double *d_inje = nullptr;         // [nb][cap]
+    double *d_seg_ngas = nullptr;     // [cap]
+    double *d_layout_tmp = nullptr;   // [nb][cap] transpose staging
+
+    unsigned *d_err = nullptr;
+    int last_launches = 0;
+    int last_nsub_max = 0;
+
+    // optional per-kernel timing (CUDA events on the context stream)
+    int timing = 0;
+    struct TimedLaunch { int kind; cudaEvent_t start, stop; };
+    std::vector<TimedLaunch> timed;           // recorded, not yet read
+    std::vector<cudaEvent_t> event_pool;
+    double kernel_ms[4] = {0, 0, 0, 0};
+    long long kernel_launches[4] = {0, 0, 0, 0};
+};
+
+// Kernel kinds for the timing hooks.
+enum KernelKind { kKindEvolve = 0, kKindCoeff = 1, kKindSecondary = 2, kKindSchedule = 3 };
+cudaEvent_t pooled_event(Context &ctx);
+void timed_begin(Context &ctx, int kind, cudaEvent_t *start);
+void timed_end(Context &ctx, int kind, cudaEvent_t start);
+
+// Error reporting shared by the translation units.
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+#define CROMA_CUDA(call)                                              \
+    do {                                                              \
+        cudaError_t e__ = (call);                                     \
+        if (e__ != cudaSuccess) return ::croma::cuda_fail(e__, #call); \
+    } while (0)
+
+// tables.cu
+int build_tables(Context &ctx);
+int ic_rows(Context &ctx, double z, double *d_out);
+// schedule.cu
+int schedule_reserve(Context &ctx, int cap);
+int run_schedule(Context &ctx, const SnapArgs &a);
+// plain.cu
+int plain_reserve(Context &ctx, int cap);
+int run_plain(Context &ctx, const SnapArgs &a);
+int transpose_to_device(Context &ctx, const double *h_cell_major, double *d_mom_major, int n);
+int transpose_to_host(Context &ctx, const double *d_mom_major, double *h_cell_major, int n);
+
+}  // namespace croma

@@ -1,0 +1,272 @@
+// croma_phys.cuh -- physics of CROMA's tracer Fokker-Planck update, shared
+// by the host table builders and the sm_100a kernels.
+//
+// Formulas follow the reference (kosukenishiwaki/croma-fp) in its own
+// evaluation order; each function names the file:line it restates.  Host
+// instantiations run on glibc, device ones on CUDA's libm.  Quantities that
+// depend only on the momentum grid (p^2, exp(-1/p), exp(-E/E_max), the
+// Kamae cross section, the Coulomb kinematics) are evaluated once on the
+// host and read by the kernels from GridTables, so the device reuses the
+// reference's exact values for them.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define CROMA_HD __host__ __device__ __forceinline__
+#else
+#define CROMA_HD inline
+#endif
+
+namespace croma {
+
+// Physical constants: src/CONSTANTS.c:3-19.
+constexpr double kC = 2.999e+10;
+constexpr double kGeV = 1.6e-3;
+constexpr double kEV = 1.6e-12;
+constexpr double kMsun = 1.99e+33;
+constexpr double kMpc = 3.0857e+24;
+constexpr double kKpc = 3.0857e+21;
+constexpr double kGyr = 3.1536e+16;
+constexpr double kHPlanck = 6.63e-27;
+constexpr double kMp = 0.938;
+constexpr double kMe = 0.511e-3;
+constexpr double kMb = 1.0e-27;
+constexpr double kMpiCh = 1.40e-1;
+constexpr double kMmu = 1.05e-1;
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kEpMax = 1.0e7;          // tracer_fp_coef.c:262
+
+enum DppModel { kDppAsa = 1, kDppTtd = 2, kDppOff = 3, kDppDirect = 4 };
+
+// Error bits raised by kernels into the context's device error word.
+enum ErrBits : unsigned {
+    kErrSingular = 1u,      // Thomas pivot |d| <= 1e-300 (fp_shared_core.c:235-245)
+    kErrCcNan = 2u,         // NaN at the right CC boundary (Chang_Cooper.c:166-183)
+    kErrIcNewton = 4u,      // CMB bound iteration did not converge
+    kErrBadInput = 8u,
+};
+
+// Maximum bins per species supported by the kernels.
+constexpr int kMaxNb = 512;
+
+// Per-species grid tables (device pointers), built once per context.
+struct SpeciesTables {
+    const double *p, *dp, *E;
+    const double *p2;           // p^2 (FP_Coef.c:97, 141)
+    const double *exp_cut;      // exp(-1/p) (FP_Coef.c:98, 142)
+    const double *two_over_p;   // 2/p used in B = radp - 2 Dpp / p (fp_shared_core.c:2401)
+    const double *expE;         // exp(-E/E_max) (protons; FP_Coef.c:699)
+    const double *inv_dx_next;  // unused placeholder for layout stability
+    double pm1, pp1;
+    double pm1_p2, pp1_p2, pm1_exp_cut, pp1_exp_cut;
+    double expE_m1, expE_p1;    // exp(-m_p sqrt(1+p^2)/E_max) at the ghost edges
+};
+
+struct GridTables {
+    SpeciesTables s[2];         // 0 = proton, 1 = electron
+    // proton Coulomb kinematics (b_Coulomb_p, FP_Coef.c:438-449)
+    const double *cp_Ep;        // gamma m_p - m_p
+    const double *cp_kin;       // gamma - 1
+    const double *cp_inv_betap2;// 1 / (p^2/(1+p^2))
+    double cpm1_Ep, cpm1_kin, cpm1_inv_betap2;
+    double cpp1_Ep, cpp1_kin, cpp1_inv_betap2;
+    const double *sig_eff;      // sigma_pp(max(j, j_pp)) * sigmoid (fp_shared_core.c:760-765)
+    // electron kinematics (prepare_cre_losses_1d, fp_shared_core.c:818-841)
+    const double *ce_beta2;     // p^2/(1+p^2)
+    double cem1_beta2, cep1_beta2;
+    // secondary electrons (prepare_secondary_kernel_flat, transposed [jp][je])
+    const double *fqe;
+    int fqe_jp0;
+    int nb;
+};
+
+// ----------------------------------------------------------------------
+// Losses
+// ----------------------------------------------------------------------
+CROMA_HD double coulomb_kernel(double x)   // b_Coulomb_kernel, FP_Coef.c:451-453
+{
+    return 0.5 * sqrt(kPi) * erf(sqrt(x)) - sqrt(x) * exp(-x);
+}
+
+// b_Coulomb_p, FP_Coef.c:438-449, with the grid-only kinematics passed in.
+CROMA_HD double coulomb_p(double n, double kbt, double Ep, double kinetic, double inv_betap2)
+{
+    const double xp = Ep / kbt;
+    const double xe = xp * (kMe / kMp);
+    const double sum = coulomb_kernel(xe) + coulomb_kernel(xp) * (kMe / kMp);
+    const double thermal = 1.0 - kbt / (2.0 * kMp * kinetic);
+    if (thermal < 0.0) return 0.0;
+    return kGyr * kC / (kMp * kGeV) * sum * n * inv_betap2 * thermal * 3.5e-29;
+}
+
+// b_Coulomb_p from p, as the sub-step estimator calls it (tracer_fp_nsub.c:260-263).
+CROMA_HD double coulomb_p_from_p(double n, double p, double kbt)
+{
+    const double p2 = p * p;
+    const double gamma = sqrt(1.0 + p2);
+    const double betap2 = p2 / (1.0 + p2);
+    const double kinetic = gamma - 1.0;
+    const double Ep = gamma * kMp - kMp;
+    const double xp = Ep / kbt;
+    const double xe = xp * (kMe / kMp);
+    const double sum = coulomb_kernel(xe) + coulomb_kernel(xp) * (kMe / kMp);
+    const double thermal = 1.0 - kbt / (2.0 * kMp * kinetic);
+    if (thermal < 0.0) return 0.0;
+    return kGyr * kC / (kMp * kGeV) * sum * n * (1.0 / betap2) * thermal * 3.5e-29;
+}
+
+CROMA_HD double b_synch(double p, double B)        // FP_Coef.c:454-462
+{
+    const double b_ratio = B * 1.0e+6 / 3.2;
+    return 4.8e-4 * p * p * b_ratio * b_ratio * 9.11e-28 * 3.0e+10 * 3.1536e+16;
+}
+
+CROMA_HD double b_coulomb_e(double n, double pe)   // FP_Coef.c:464-469
+{
+    const double pe2 = pe * pe;
+    const double beta2 = pe2 / (1.0 + pe2);
+    return 3.05e-29 * n * (1.0 + log(pe / n) / 74.8) / (kMe * kGeV) * kC * kGyr / beta2;
+}
+
+// ----------------------------------------------------------------------
+// Acceleration times (FP_Coef.c:624-678)
+// ----------------------------------------------------------------------
+CROMA_HD double i_theta(double x)
+{
+    return x * x * x * x / 4.0 + x * x - (1.0 + 2.0 * x * x) * log(x) - 5.0 / 4.0;
+}
+
+CROMA_HD double tacc_ttd(int model_brunetti16, double L, double cs, double Ms, double v)
+{
+    const double x = cs / kC;
+    if (model_brunetti16) {
+        const double theta = i_theta(x);
+        if (!(x > 0.0) || !(theta > 0.0) || !(Ms > 0.0) || !(L > 0.0) || !(cs > 0.0)) return 0.0;
+        const double r = Ms / 0.5;
+        return 2.5e-3 / (x * theta) * (1.0 / (r * r * r * r)) * (L / (300.0 * kKpc)) *
+               (1.0 / (cs / 1500.0e5));
+    }
+    const double kL = 2.0 * kPi / L;
+    const double k_cut = 1.04e+4 * (Ms * Ms * Ms * Ms) * kL;
+    const double kWk_L = 0.5 * (v * v);
+    const double kWk_cut = kWk_L * (1.0 / sqrt(k_cut / kL));
+    return kC / kPi / i_theta(x) / k_cut / kWk_cut / kGyr;
+}
+
+CROMA_HD double tacc_asa(double psi3, double L, double cs, double Ms, double beta_pl)
+{
+    return sqrt(6.0 / 5.0) / 12.0 * (kC / cs / cs) * L / sqrt(beta_pl) / (Ms * Ms * Ms) * psi3 / kGyr;
+}
+
+CROMA_HD double effective_mach(double mach_limit, double dv, double cs)
+{
+    if (cs <= 0.0) return 0.0;
+    double m = dv / cs;
+    if (m < 0.0) m = 0.0;
+    if (mach_limit > 0.0 && m > mach_limit) m = mach_limit;
+    return m;
+}
+
+// ----------------------------------------------------------------------
+// Chang-Cooper face weights: cc_eval_face_weights, Chang_Cooper.c:22-40.
+// For |w| >= 0.1 the three exponentials of the reference collapse to one:
+// with aw = |w|, -aw/2 + w/2 and -aw/2 - w/2 are exactly 0 and -aw in some
+// order, and exp(0) == 1 exactly.
+// ----------------------------------------------------------------------
+CROMA_HD void face_weights(double w, double &wp, double &wm)
+{
+    if (fabs(w) < 0.1) {
+        const double w2 = w * w;
+        const double den = 1.0 + w2 / 24.0 + (w2 * w2) / 1920.0;
+        wp = exp(0.5 * w) / den;
+        wm = exp(-0.5 * w) / den;
+    } else {
+        const double aw = fabs(w);
+        const double e = exp(-aw);
+        const double den = 1.0 - e;
+        const double big = aw / den;
+        const double small = aw * e / den;
+        wp = (w >= 0.0) ? big : small;
+        wm = (w >= 0.0) ? small : big;
+    }
+}
+
+CROMA_HD double face_delta(double w)
+{
+    return 1.0 / w - 1.0 / (exp(w) - 1.0);
+}
+
+// cc_prepare_face_weight, Chang_Cooper.c:42-64 (delta not produced).
+CROMA_HD void face(double bl, double br, double cl, double cr, double xl, double xr,
+                   double &wp, double &wm, double &w)
+{
+    wp = 0.0; wm = 0.0; w = 0.0;
+    if (fabs(cl) <= 1.0e-200) return;
+    w = 0.5 * (bl + br) / (0.5 * (cl + cr)) * (xr - xl);
+    face_weights(w, wp, wm);
+}
+
+// ----------------------------------------------------------------------
+// Inverse-Compton cooling (FP_Coef.c:361-436, 480-539)
+// ----------------------------------------------------------------------
+struct IcConsts {
+    double cmb_pref;      // 8 pi c c c pow(m_e/h, 3) (FP_Coef.c:402)
+    double cmb_pref_d;    // same with the derivative's constants (FP_Coef.c:412)
+    double k_d;           // 1.38 * pow(10, -16) (FP_Coef.c:410)
+    double log10_90;      // 90 log(10)
+};
+
+CROMA_HD double ic_kernel(double eps0, double gamma, double eps)   // IC_kernel :379-389
+{
+    const double re = 2.82e-13;
+    const double kappa = eps / (4.0 * eps0 * gamma * (gamma - eps));
+    if (kappa <= 0.0) return 0.0;
+    const double t = 4.0 * eps0 * kappa * gamma;
+    double C = 2.0 * kappa * log(kappa) + (1.0 + 2.0 * kappa) * (1.0 - kappa) +
+               (t * t) / (2.0 * (1.0 + 4.0 * eps0 * gamma * kappa)) * (1.0 - kappa);
+    return 2.0 * kPi * re * re * kC / (gamma * gamma * eps0) * C;
+}
+
+CROMA_HD double cmb_density(const IcConsts &k, double eps, double z)   // :391-406
+{
+    const double Tcmb = 2.757 * (1.0 + z);
+    const double X = eps * 9.11e-28 * kC * kC / (1.38e-16 * Tcmb);
+    if (X > k.log10_90) return 0.0;
+    const double ex = exp(X);
+    if (ex - 1.0 < 1.0e-40) {
+        return k.cmb_pref * eps / (9.11e-28 * kC * kC * (1.0 + 0.5 * X + X / 6.0) / (1.38e-16 * Tcmb));
+    }
+    return k.cmb_pref * (eps * eps) / (ex - 1.0);
+}
+
+CROMA_HD double cmb_density_deps(const IcConsts &k, double eps, double z)   // :407-413
+{
+    const double Tcmb = 2.757 * (1.0 + z);
+    const double X = eps * 9.11e-28 * kC * kC / (k.k_d * Tcmb);
+    const double ex = exp(X);
+    return k.cmb_pref_d * eps / (ex - 1.0) *
+           (2.0 - eps * 9.11e-28 * kC * kC * ex / (k.k_d * Tcmb * (ex - 1.0)));
+}
+
+// Inner integral b_IC_integrand (FP_Coef.c:512-539)
+CROMA_HD double b_ic_integrand(double eps0, double gamma, double emin, double emax)
+{
+    const double da = 0.50e-1;
+    const int N = (int)round((log10(emax) - log10(emin)) / da);
+    double a = log10(emin), epsnew = emin, integral = 0.0;
+    double newC = ic_kernel(eps0, gamma, epsnew);
+    for (int i = 0; i < N; i++) {
+        a = a + da;
+        const double eps = epsnew;
+        epsnew = pow(10.0, a);
+        const double deps = epsnew - eps;
+        const double C = newC;
+        newC = ic_kernel(eps0, gamma, epsnew);
+        integral = integral + 0.5 * (eps * C + epsnew * newC) * deps;
+    }
+    return integral;
+}
+
+}  // namespace croma

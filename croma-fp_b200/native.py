@@ -1,0 +1,214 @@
+"""ctypes binding of the native C ABI (include/croma_b200.h) and a small
+Python front end, ``TracerFP``, that runs snapshots through it.
+
+The library must be built first (``python croma-fp_b200/build.py`` or
+``__graft_entry__.build()``); loading fails loudly when it is missing or
+when no CUDA device is present -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .config import RunConfig
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBDIR = os.path.join(HERE, "lib")
+
+PATHS = {"plain": 0, "fused": 1}
+
+_d, _i, _vp = C.c_double, C.c_int, C.c_void_p
+
+
+class CromaB200Config(C.Structure):
+    _fields_ = [("nb", _i), ("species_mask", _i), ("pmin", _d), ("pmax", _d), ("pemin", _d),
+                ("pemax", _d), ("dpp_model", _i), ("ttd_tacc_model", _i), ("t_acc_direct_gyr", _d),
+                ("mach_limit", _d), ("psi", _d), ("eta_dpp_cap", _d), ("nsub_safety", _d),
+                ("nsub_max", _i), ("coeff_interp_min_steps", _i), ("coeff_interp_max_segments", _i),
+                ("reacc_window_mode", _i), ("f_eddy", _d), ("t_off_gyr", _d), ("t_acc_off_gyr", _d),
+                ("path", _i)]
+
+
+class CromaB200Snapshot(C.Structure):
+    _fields_ = [("bg_curr", _vp), ("bg_next", _vp), ("bg_on_device", _i), ("z_curr", _d),
+                ("z_next", _d), ("allow_interp", _i), ("dt_snap", _d), ("elapsed_gyr", _d)]
+
+
+_LIBS: dict = {}
+
+
+def library_path(nb: int) -> str:
+    return os.path.join(LIBDIR, f"libcroma_b200_np{nb}.so")
+
+
+def load_library(nb: int) -> C.CDLL:
+    if nb in _LIBS:
+        return _LIBS[nb]
+    path = library_path(nb)
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `python croma-fp_b200/build.py {nb}`")
+    L = C.CDLL(path)
+    P = C.POINTER
+    L.croma_b200_last_error.restype = C.c_char_p
+    L.croma_b200_create.argtypes = [P(CromaB200Config), _i, P(_vp)]
+    L.croma_b200_destroy.argtypes = [_vp]
+    L.croma_b200_reserve.argtypes = [_vp, _i]
+    L.croma_b200_set_state.argtypes = [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.croma_b200_get_state.argtypes = [_vp, _vp, _vp]
+    L.croma_b200_snapshot.argtypes = [_vp, P(CromaB200Snapshot), _i]
+    L.croma_b200_get_schedule.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.croma_b200_ic_row.argtypes = [_vp, _d, _vp]
+    L.croma_b200_get_grid.argtypes = [_vp, _i, _vp]
+    L.croma_b200_get_secondary_kernel.argtypes = [_vp, _vp, _vp]
+    L.croma_b200_stream.argtypes = [_vp]
+    L.croma_b200_stream.restype = _vp
+    L.croma_b200_sync.argtypes = [_vp]
+    L.croma_b200_state_device.argtypes = [_vp, P(_vp), P(_vp)]
+    L.croma_b200_last_launch_count.argtypes = [_vp]
+    L.croma_b200_set_kernel_timing.argtypes = [_vp, _i]
+    L.croma_b200_kernel_stats.argtypes = [_vp, _i, P(_d), P(C.c_longlong)]
+    L.croma_b200_reset_kernel_stats.argtypes = [_vp]
+    _LIBS[nb] = L
+    return L
+
+
+class CromaError(RuntimeError):
+    pass
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def _c(a, dtype=np.float64):
+    return None if a is None else np.ascontiguousarray(a, dtype=dtype)
+
+
+class TracerFP:
+    """One device-resident batch of tracers advanced snapshot by snapshot."""
+
+    def __init__(self, cfg: RunConfig, path: str = "plain", device: int = 0):
+        self.cfg = cfg
+        self.nb = cfg.nb
+        self.lib = load_library(cfg.nb)
+        c = CromaB200Config()
+        for name, _ in CromaB200Config._fields_:
+            if name == "dpp_model":
+                c.dpp_model = cfg.dpp_model_id()
+            elif name == "species_mask":
+                c.species_mask = cfg.species_mask()
+            elif name == "path":
+                c.path = PATHS[path]
+            else:
+                setattr(c, name, getattr(cfg, name))
+        h = _vp()
+        self._check(self.lib.croma_b200_create(C.byref(c), device, C.byref(h)))
+        self.h = h
+        self.ntracer = 0
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = self.lib.croma_b200_last_error().decode()
+            raise CromaError(f"croma_b200 call failed ({rc}): {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.croma_b200_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state ----------------------------------------------------------
+    def set_state(self, crp, cre, qpi=None, qepri=None, mass=None, dis=None):
+        crp, cre = _c(crp), _c(cre)
+        n = crp.shape[0]
+        qpi, qepri, mass = _c(qpi), _c(qepri), _c(mass)
+        dis = _c(dis, np.uint8)
+        self._check(self.lib.croma_b200_set_state(self.h, n, _p(crp), _p(cre), _p(qpi), _p(qepri),
+                                                  _p(mass), _p(dis)))
+        self.ntracer = n
+
+    def get_state(self):
+        crp = np.empty((self.ntracer, self.nb))
+        cre = np.empty((self.ntracer, self.nb))
+        self._check(self.lib.croma_b200_get_state(self.h, _p(crp), _p(cre)))
+        return crp, cre
+
+    def state_device(self):
+        a, b = _vp(), _vp()
+        self._check(self.lib.croma_b200_state_device(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    # -- snapshots ------------------------------------------------------
+    def snapshot(self, bg_curr, bg_next, z_curr, z_next, allow, dt, elapsed, sync=True):
+        """Advance one snapshot.  bg_* are host arrays [8][ntracer] or device
+        addresses (ints)."""
+        s = CromaB200Snapshot()
+        if isinstance(bg_curr, int):
+            s.bg_curr, s.bg_next, s.bg_on_device = bg_curr, bg_next, 1
+            keep = None
+        else:
+            bc = _c(bg_curr)
+            bn = _c(bg_next) if bg_next is not None else bc
+            keep = (bc, bn)
+            s.bg_curr, s.bg_next, s.bg_on_device = bc.ctypes.data, bn.ctypes.data, 0
+        s.z_curr, s.z_next, s.allow_interp = z_curr, z_next, int(bool(allow))
+        s.dt_snap, s.elapsed_gyr = dt, elapsed
+        self._check(self.lib.croma_b200_snapshot(self.h, C.byref(s), int(bool(sync))))
+        del keep
+
+    def sync(self):
+        self._check(self.lib.croma_b200_sync(self.h))
+
+    def schedule(self):
+        n = self.ntracer
+        out = {k: np.empty(n, np.int32) for k in ("nsub", "non", "target", "bucket_ids", "bucket_indices")}
+        nb = np.zeros(1, np.int32)
+        self._check(self.lib.croma_b200_get_schedule(self.h, _p(out["nsub"]), _p(out["non"]),
+                                                     _p(out["target"]), _p(out["bucket_ids"]),
+                                                     _p(out["bucket_indices"]), _p(nb)))
+        out["nbuckets"] = int(nb[0])
+        return out
+
+    # -- tables ---------------------------------------------------------
+    def ic_row(self, z):
+        out = np.empty(self.nb + 2)
+        self._check(self.lib.croma_b200_ic_row(self.h, z, _p(out)))
+        return out[:self.nb], out[self.nb], out[self.nb + 1]
+
+    def grid(self, species):
+        out = np.empty(3 * self.nb + 2)
+        self._check(self.lib.croma_b200_get_grid(self.h, species, _p(out)))
+        n = self.nb
+        return out[:n], out[n:2 * n], out[2 * n:3 * n], out[3 * n], out[3 * n + 1]
+
+    def secondary_kernel(self):
+        f = np.empty((self.nb, self.nb))
+        m = np.empty(self.nb, np.int32)
+        self._check(self.lib.croma_b200_get_secondary_kernel(self.h, _p(f), _p(m)))
+        return f, m
+
+    def stream(self) -> int:
+        return self.lib.croma_b200_stream(self.h) or 0
+
+    def last_launch_count(self) -> int:
+        return self.lib.croma_b200_last_launch_count(self.h)
+
+    KERNEL_KINDS = {"evolve": 0, "coeff": 1, "secondary": 2}
+
+    def set_kernel_timing(self, enable: bool):
+        self._check(self.lib.croma_b200_set_kernel_timing(self.h, int(bool(enable))))
+
+    def kernel_stats(self, kind: str):
+        ms, n = _d(), C.c_longlong()
+        self._check(self.lib.croma_b200_kernel_stats(self.h, self.KERNEL_KINDS[kind], C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def reset_kernel_stats(self):
+        self._check(self.lib.croma_b200_reset_kernel_stats(self.h))

@@ -1,0 +1,137 @@
+/*
+ * croma_b200.h -- native C ABI of the B200 tracer Fokker-Planck library
+ * (libcroma_b200_np<N>.so, N = bins per species: 128, 256 or 512).
+ *
+ * This is the batched, device-resident form of the per-snapshot sequence
+ * that the reference's snapshot driver runs for the tracer FP update
+ * (include/tracer_fp_solve.inc in kosukenishiwaki/croma-fp):
+ *
+ *   IC-cooling rows   tracer_fp_prepare_ic_cooling_snapshot (src/tracer_fp_synch.c:242-294)
+ *   nsub / n_on       tracer_fp_prepare_nsub_loss_endpoints + tracer_fp_compute_nsubsteps_from_endpoints
+ *                     (src/tracer_fp_nsub.c:94-282)
+ *   buckets           tracer_bucket_build_snapshot (src/tracer_fp_bucket.c:208-262)
+ *   evolve            tracer_fp_batch_execute_parallel / run_tracer_pipeline
+ *                     (src/tracer_fp_batch.c:651-1126, src/fp_cuda_tracer_backend.cu:1530-1567)
+ *
+ * The reference-compatible entry points (run_tracer_pipeline and friends)
+ * are declared in fp_cuda_backend.h and implemented on the same kernels.
+ *
+ * All functions return 0 on success and a negative code on failure
+ * (-1 invalid argument or state, -2 numerical failure reported by a kernel,
+ * -3 CUDA error, -4 allocation failure); they never exit the process.
+ * croma_b200_last_error() describes the last failure of the calling thread.
+ * Pointers are plain host or device addresses as stated per argument.
+ */
+#ifndef CROMA_B200_H
+#define CROMA_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CromaB200Context CromaB200Context;
+
+/* Dpp_mode values (FP_MOMENTUMDIFF_MODEL_*, include/fp_shared_core.h:227-233). */
+enum { CROMA_DPP_ASA = 1, CROMA_DPP_TTD = 2, CROMA_DPP_OFF = 3, CROMA_DPP_DIRECT_TACC = 4 };
+
+/* Which evolve kernel family runs. */
+enum {
+    CROMA_PATH_PLAIN = 0,   /* FP64, reference data contract: CC rows materialised per
+                               segment, one Thomas system per thread per sub-step */
+    CROMA_PATH_FUSED = 1    /* FP64, on-chip: rows built, factored and swept per tracer
+                               inside one kernel, warp-cooperative substitution */
+};
+
+/* Species bits: bit 0 protons, bit 1 electrons.  A species outside the mask
+ * must have zero spectra and zero source; it is then left untouched, which
+ * is exactly what the implicit solve returns for it. */
+enum { CROMA_SPECIES_PROTON = 1, CROMA_SPECIES_ELECTRON = 2 };
+
+typedef struct {
+    int nb;                          /* bins per species; must equal the library's N */
+    int species_mask;
+    double pmin, pmax;               /* log10 proton grid bounds (params.c:55) */
+    double pemin, pemax;             /* log10 electron grid bounds (params.c:56) */
+    int dpp_model;                   /* CROMA_DPP_* */
+    int ttd_tacc_model;              /* 0 spectral, 1 brunetti16 (params.c:74-75) */
+    double t_acc_direct_gyr;
+    double mach_limit;               /* params.c:77 */
+    double psi;                      /* params.c:76 */
+    double eta_dpp_cap;              /* params.c:78; <= 0 disables */
+    double nsub_safety;              /* tracer_nsub_safety, params.c:83 */
+    int nsub_max;                    /* tracer_nsub_max; 0 = no cap */
+    int coeff_interp_min_steps;      /* params.c:85 */
+    int coeff_interp_max_segments;   /* params.c:86 */
+    int reacc_window_mode;           /* 0 always on, 1 centred */
+    double f_eddy;
+    double t_off_gyr;
+    double t_acc_off_gyr;
+    int path;                        /* CROMA_PATH_* */
+} CromaB200Config;
+
+typedef struct {
+    const double *bg_curr;   /* [8][ntracer] field-major: n_gas, kbt, b_field, divv_gyr,
+                                l_turb_mpc, dv_imc, cs, beta_pl (the TracerFpBackgroundSlot
+                                fields of include/tracer_fp_types.h) */
+    const double *bg_next;   /* same for the next snapshot (ignored unless allow_interp) */
+    int bg_on_device;        /* 1: device pointers, 0: host pointers */
+    double z_curr, z_next;
+    int allow_interp;        /* background interpolation across the snapshot */
+    double dt_snap;          /* Gyr */
+    double elapsed_gyr;      /* time at the start of the snapshot */
+} CromaB200Snapshot;
+
+const char *croma_b200_last_error(void);
+int croma_b200_nb(void);                       /* bins per species compiled into this library */
+
+int croma_b200_create(const CromaB200Config *cfg, int device, CromaB200Context **out);
+void croma_b200_destroy(CromaB200Context *ctx);
+
+/* Device workspace and state for up to ntracer tracers. */
+int croma_b200_reserve(CromaB200Context *ctx, int ntracer);
+
+/* Host <-> device spectra, cell-major host arrays [ntracer][nb] (the
+ * reference's layout).  NULL skips an array; sources default to zero. */
+int croma_b200_set_state(CromaB200Context *ctx, int ntracer, const double *crp,
+                         const double *cre, const double *qpi, const double *qepri,
+                         const double *mass_msun, const unsigned char *disable_adiabatic);
+int croma_b200_get_state(CromaB200Context *ctx, double *crp, double *cre);
+
+/* One snapshot on the context's stream; asynchronous unless sync != 0. */
+int croma_b200_snapshot(CromaB200Context *ctx, const CromaB200Snapshot *snap, int sync);
+
+/* Schedule of the last snapshot (host arrays of ntracer ints); NULL skips. */
+int croma_b200_get_schedule(CromaB200Context *ctx, int *nsub, int *n_on, int *target_nsub,
+                            int *bucket_ids, int *bucket_indices, int *nbuckets);
+
+/* IC-cooling row for one redshift (host output: row[nb], then m1, p1). */
+int croma_b200_ic_row(CromaB200Context *ctx, double z, double *row_m1_p1);
+
+/* Grid and one-time tables (host outputs): p, dp, E [nb] then pm1, pp1. */
+int croma_b200_get_grid(CromaB200Context *ctx, int species, double *out);
+int croma_b200_get_secondary_kernel(CromaB200Context *ctx, double *fqe_flat, int *np_min_qe);
+
+/* The context's CUDA stream (cudaStream_t) and a blocking wait on it. */
+void *croma_b200_stream(CromaB200Context *ctx);
+int croma_b200_sync(CromaB200Context *ctx);
+
+/* Device pointers of the resident spectra, momentum-major [nb][ntracer]. */
+int croma_b200_state_device(CromaB200Context *ctx, double **crp, double **cre);
+
+/* Kernel launches issued by the last croma_b200_snapshot call. */
+int croma_b200_last_launch_count(CromaB200Context *ctx);
+
+/* Optional per-kernel timing with CUDA events on the context stream.
+ * kind: 0 evolve (sub-step) kernels, 1 coefficient kernels, 2 secondary
+ * source kernels.  kernel_stats waits for the stream and returns the
+ * accumulated device time and launch count since the last reset. */
+int croma_b200_set_kernel_timing(CromaB200Context *ctx, int enable);
+int croma_b200_kernel_stats(CromaB200Context *ctx, int kind, double *total_ms, long long *launches);
+int croma_b200_reset_kernel_stats(CromaB200Context *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
