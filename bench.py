@@ -351,7 +351,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--path", default="plain", choices=["plain", "fused"])
+    ap.add_argument("--path", default="fused", choices=["plain", "fused"])
     ap.add_argument("--tracers", type=int, default=NTRACER)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -171,6 +171,7 @@ void croma_b200_destroy(CromaB200Context *h)
     for (auto &t : c.timed) { cudaEventDestroy(t.start); cudaEventDestroy(t.stop); }
     for (auto e : c.event_pool) cudaEventDestroy(e);
     cudaFree(c.d_tables);
+    cudaFree(c.d_np_min_qe);
     cudaFree(c.d_ic);
     cudaFree(c.d_err);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -204,7 +205,7 @@ int croma_b200_reserve(CromaB200Context *h, int ntracer)
     c.ntracer = ntracer;
     c.has_sources = 0;
     int rc = schedule_reserve(c, ntracer);
-    if (rc == 0) rc = plain_reserve(c, ntracer);
+    if (rc == 0) rc = cell_major(c) ? fused_reserve(c, ntracer) : plain_reserve(c, ntracer);
     if (rc != 0) { free_state(c); return rc; }
     return 0;
 }
@@ -222,11 +223,18 @@ int croma_b200_set_state(CromaB200Context *h, int ntracer, const double *crp, co
     }
     const size_t st = (size_t)NB * ntracer * sizeof(double);
     int rc = 0;
-    if (crp && (rc = transpose_to_device(c, crp, c.d_crp, ntracer))) return rc;
-    if (cre && (rc = transpose_to_device(c, cre, c.d_cre, ntracer))) return rc;
-    if (qpi) { if ((rc = transpose_to_device(c, qpi, c.d_qpi, ntracer))) return rc; }
+    auto up = [&](const double *h, double *d) -> int {
+        if (cell_major(c)) {
+            CROMA_CUDA(cudaMemcpyAsync(d, h, st, cudaMemcpyHostToDevice, c.stream));
+            return 0;
+        }
+        return transpose_to_device(c, h, d, ntracer);
+    };
+    if (crp && (rc = up(crp, c.d_crp))) return rc;
+    if (cre && (rc = up(cre, c.d_cre))) return rc;
+    if (qpi) { if ((rc = up(qpi, c.d_qpi))) return rc; }
     else CROMA_CUDA(cudaMemsetAsync(c.d_qpi, 0, st, c.stream));
-    if (qepri) { if ((rc = transpose_to_device(c, qepri, c.d_qepri, ntracer))) return rc; }
+    if (qepri) { if ((rc = up(qepri, c.d_qepri))) return rc; }
     else CROMA_CUDA(cudaMemsetAsync(c.d_qepri, 0, st, c.stream));
     c.has_sources = (qpi != nullptr || qepri != nullptr);
     if (mass) CROMA_CUDA(cudaMemcpyAsync(c.d_mass, mass, ntracer * sizeof(double), cudaMemcpyHostToDevice, c.stream));
@@ -242,9 +250,17 @@ int croma_b200_get_state(CromaB200Context *h, double *crp, double *cre)
     Context &c = h->impl;
     CROMA_CUDA(cudaSetDevice(c.device));
     int rc = 0;
-    if (crp && (rc = transpose_to_host(c, c.d_crp, crp, c.cap))) return rc;
+    const size_t st = (size_t)NB * c.cap * sizeof(double);
+    auto down = [&](const double *d, double *h) -> int {
+        if (cell_major(c)) {
+            CROMA_CUDA(cudaMemcpyAsync(h, d, st, cudaMemcpyDeviceToHost, c.stream));
+            return 0;
+        }
+        return transpose_to_host(c, d, h, c.cap);
+    };
+    if (crp && (rc = down(c.d_crp, crp))) return rc;
     CROMA_CUDA(cudaStreamSynchronize(c.stream));
-    if (cre && (rc = transpose_to_host(c, c.d_cre, cre, c.cap))) return rc;
+    if (cre && (rc = down(c.d_cre, cre))) return rc;
     CROMA_CUDA(cudaStreamSynchronize(c.stream));
     return check_err(c);
 }
@@ -296,8 +312,7 @@ int croma_b200_snapshot(CromaB200Context *h, const CromaB200Snapshot *s, int syn
     a.err = c.d_err;
     int rc = run_schedule(c, a);
     if (rc) return rc;
-    if (c.cfg.path == CROMA_PATH_PLAIN) rc = run_plain(c, a);
-    else { set_error("fused path not built into this library"); return -1; }
+    rc = (c.cfg.path == CROMA_PATH_PLAIN) ? run_plain(c, a) : run_fused(c, a);
     if (rc) return rc;
     if (sync) return check_err(c);
     return 0;

@@ -73,6 +73,7 @@ struct Context {
     double h_pm1[2] = {0, 0}, h_pp1[2] = {0, 0};
     std::vector<double> h_fqe;        // [nb][nb] transposed [jp][je]
     std::vector<int> h_np_min_qe;
+    int *d_np_min_qe = nullptr;       // [nb]
 
     double *d_tables = nullptr;       // one block holding every grid table
     GridTables gt{};
@@ -145,6 +146,12 @@ int run_schedule(Context &ctx, const SnapArgs &a);
 // plain.cu
 int plain_reserve(Context &ctx, int cap);
 int run_plain(Context &ctx, const SnapArgs &a);
+// fused.cu
+int fused_reserve(Context &ctx, int cap);
+int run_fused(Context &ctx, const SnapArgs &a);
+// layout of the resident spectra: cell-major [tracer][nb] for the fused path,
+// momentum-major [nb][tracer] for the plain path
+inline bool cell_major(const Context &ctx) { return ctx.cfg.path == CROMA_PATH_FUSED; }
 int transpose_to_device(Context &ctx, const double *h_cell_major, double *d_mom_major, int n);
 int transpose_to_host(Context &ctx, const double *d_mom_major, double *h_cell_major, int n);
 

@@ -286,7 +286,7 @@ int build_tables(Context &ctx)
         CROMA_CUDA(cudaStreamSynchronize(ctx.stream));
         cudaFree(d_vals);
         cudaFree(d_aux);
-        cudaFree(d_npmin);
+        ctx.d_np_min_qe = d_npmin;
         // first proton bin any electron bin draws from (fp_shared_core.c:1615-1623)
         int jp0 = n;
         for (int je = 0; je < n; je++) {

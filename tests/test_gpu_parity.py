@@ -1,4 +1,4 @@
-"""GPU parity of the plain FP64 path against the golden fixtures (outputs
+"""GPU parity of the FP64 evolve paths (plain and fused) against the golden fixtures (outputs
 of the reference's own CPU code) through the C ABI.
 
 Bar: nsub, n_on and bucket ids bit-exact; spectra within 1e-10 relative
@@ -31,9 +31,10 @@ def _run_case(name, path):
     return c, fp, results
 
 
+@pytest.mark.parametrize("path", ["plain", "fused"])
 @pytest.mark.parametrize("name", case_names())
-def test_plain_matches_reference(name):
-    c, fp, results = _run_case(name, "plain")
+def test_path_matches_reference(name, path):
+    c, fp, results = _run_case(name, path)
     d = c.d
     for k, (sched, crp, cre) in enumerate(results):
         assert np.array_equal(sched["nsub"], d[f"nsub_{k}"]), f"nsub mismatch at step {k}"
