@@ -58,7 +58,9 @@ struct SpeciesTables {
     const double *exp_cut;      // exp(-1/p) (FP_Coef.c:98, 142)
     const double *two_over_p;   // 2/p used in B = radp - 2 Dpp / p (fp_shared_core.c:2401)
     const double *expE;         // exp(-E/E_max) (protons; FP_Coef.c:699)
-    const double *inv_dx_next;  // unused placeholder for layout stability
+    const double *inv_dx;       // 1 / dp
+    const double *inv_dxl;      // 1 / (p[j] - p[j-1])   (j >= 1)
+    const double *inv_dxr;      // 1 / (p[j+1] - p[j])   (j <= nb-2)
     double pm1, pp1;
     double pm1_p2, pp1_p2, pm1_exp_cut, pp1_exp_cut;
     double expE_m1, expE_p1;    // exp(-m_p sqrt(1+p^2)/E_max) at the ghost edges
@@ -73,8 +75,10 @@ struct GridTables {
     double cpm1_Ep, cpm1_kin, cpm1_inv_betap2;
     double cpp1_Ep, cpp1_kin, cpp1_inv_betap2;
     const double *sig_eff;      // sigma_pp(max(j, j_pp)) * sigmoid (fp_shared_core.c:760-765)
+    const double *cp_inv2mpkin; // 1 / (2 m_p (gamma - 1))
     // electron kinematics (prepare_cre_losses_1d, fp_shared_core.c:818-841)
     const double *ce_beta2;     // p^2/(1+p^2)
+    const double *ce_inv_beta2; // (1+p^2)/p^2
     double cem1_beta2, cep1_beta2;
     // secondary electrons (prepare_secondary_kernel_flat, transposed [jp][je])
     const double *fqe;
@@ -87,6 +91,16 @@ struct GridTables {
 // ----------------------------------------------------------------------
 CROMA_HD double coulomb_kernel(double x)   // b_Coulomb_kernel, FP_Coef.c:451-453
 {
+    return 0.5 * sqrt(kPi) * erf(sqrt(x)) - sqrt(x) * exp(-x);
+}
+
+// The same kernel with its saturated tail taken exactly: for x > 40,
+// erf(sqrt(x)) rounds to 1 (erfc(6.32) < 1e-18) and sqrt(x) exp(-x) < 3e-17
+// is below half an ulp of 0.5 sqrt(pi), so the double result is exactly
+// 0.5 sqrt(pi).
+CROMA_HD double coulomb_kernel_fast(double x)
+{
+    if (x > 40.0) return 0.5 * sqrt(kPi);
     return 0.5 * sqrt(kPi) * erf(sqrt(x)) - sqrt(x) * exp(-x);
 }
 

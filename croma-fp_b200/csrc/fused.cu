@@ -2,21 +2,26 @@
 // system, the spectrum held in registers across a coefficient segment.
 //
 // Per segment slot and system the warp
-//   1. builds its Chang-Cooper rows on chip: lane l owns rows
-//      [l*R, (l+1)*R) (R = nb/32); neighbouring terms and face weights come
-//      from the adjacent lanes by shuffles (losses / Dpp / CC assembly of
+//   1. evaluates the loss / diffusion terms of every bin and the Chang-Cooper
+//      face weights in rolled, lane-strided loops into the warp's slice of
+//      shared memory (losses / Dpp / CC assembly of
 //      src/fp_shared_core.c:729-842, 1241-1317, 2358-2431 and
 //      src/Chang_Cooper.c:22-184);
-//   2. factors the tridiagonal matrix once (it is constant over the
-//      segment's sub-steps): the Thomas pivots d_i = b_i - a_i c_{i-1}/d_{i-1}
-//      are a chain of Moebius maps, composed per lane as 2x2 matrices and
-//      combined across lanes by a warp scan; each lane then re-runs the
-//      exact recurrence on its rows from the scanned incoming pivot;
-//   3. runs every sub-step as two first-order linear recurrences (forward
-//      elimination and back substitution of fp_thomas_solve_ws,
-//      src/fp_shared_core.c:226-257), each an affine warp scan: a local pass
-//      per lane, five shuffle levels, and a second local pass.
+//   2. assembles its rows a, b, c in registers -- lane l owns rows
+//      [l*R, (l+1)*R), R = nb/32 -- and factors the tridiagonal matrix once,
+//      since it is constant over the segment's sub-steps: the Thomas pivots
+//      d_i = b_i - a_i c_{i-1}/d_{i-1} are a chain of Moebius maps, composed
+//      per lane as 2x2 matrices and combined across lanes by a warp scan; each
+//      lane then re-runs the exact recurrence on its rows from the scanned
+//      incoming pivot;
+//   3. runs every sub-step as the two first-order linear recurrences of
+//      fp_thomas_solve_ws (src/fp_shared_core.c:226-257), each an affine warp
+//      scan: a local pass per lane, five shuffle levels, a second local pass.
 //
+// Shared-memory rows are stored at (m % R) * 33 + m / R, so the blocked reads
+// of step 2 (lane l, row l*R + r and its neighbours) hit 32 distinct banks.
+// Divisions by grid quantities use reciprocals tabulated on the host; the
+// results agree with the reference's divisions to an ulp per operation.
 // The secondary-electron source of each segment (a dense [tracers x nb] .
 // [nb x nb] product, prepare_secondary_sources_cell_major,
 // src/fp_shared_core.c:1591-1672) runs as a tiled kernel before the slot.
@@ -27,7 +32,9 @@ namespace croma {
 
 namespace {
 
-constexpr int kRpl = NB / 32;   // rows per lane
+constexpr int kR = NB / 32;          // rows per lane
+constexpr int kSw = 33 * kR;         // swizzled row-array length
+constexpr int kWarps = 4;            // warps (systems) per block
 constexpr unsigned kFull = 0xffffffffu;
 
 struct FusedParams {
@@ -39,6 +46,7 @@ struct FusedParams {
     const int *np_min_qe;    // [nb]
 };
 
+__device__ __forceinline__ int swz(int m) { return (m % kR) * 33 + m / kR; }
 __device__ __forceinline__ double sup(double v, int d) { return __shfl_up_sync(kFull, v, d); }
 __device__ __forceinline__ double sdn(double v, int d) { return __shfl_down_sync(kFull, v, d); }
 
@@ -53,108 +61,194 @@ __device__ __forceinline__ void rescale2(double &m00, double &m01, double &m10, 
     m00 *= sc; m01 *= sc; m10 *= sc; m11 *= sc;
 }
 
+// Per-tracer constants of species S for one segment.
+template <int S>
+struct SegTerms {
+    const GridTables *gt;
+    double n_gas, kbt, inv_kbt, inv_n, adiab;
+    double synch_coeff, coulomb_coeff;
+    double dt, dt_over_tloss_pref;   // protons: dt / T = sig_eff * dt_over_tloss_pref
+    double dtT_e;                    // electrons: dt / 1e100
+    double dpp_inv, dpp_scale;
+    int dpp_fill;
+    const double *ric, *ric_next;
+    double alpha;
+    int interp;
+
+    // B = radp - 2 Dpp / p, C = Dpp, dT = dt / tloss at bin j
+    __device__ __forceinline__ void at(int j, double &B, double &C, double &dT) const
+    {
+        const SpeciesTables &st = gt->s[S];
+        const double p = st.p[j];
+        const double p2 = st.p2[j];
+        double D;
+        if (!dpp_fill) D = p2 * (1.0 / (4.0 * 1.0e+5));
+        else if (S == 0) D = p2 * dpp_inv * st.expE[j] * st.exp_cut[j];
+        else D = p2 * dpp_inv * st.exp_cut[j];
+        D *= dpp_scale;
+        double radp;
+        if (S == 0) {
+            const double xp = gt->cp_Ep[j] * inv_kbt;
+            const double xe = xp * (kMe / kMp);
+            const double sum = coulomb_kernel_fast(xe) + coulomb_kernel_fast(xp) * (kMe / kMp);
+            const double thermal = 1.0 - kbt * gt->cp_inv2mpkin[j];
+            const double coul = (thermal < 0.0)
+                ? 0.0
+                : kGyr * kC / (kMp * kGeV) * sum * n_gas * gt->cp_inv_betap2[j] * thermal * 3.5e-29;
+            radp = coul + adiab * p;
+            dT = gt->sig_eff[j] * dt_over_tloss_pref;
+        } else {
+            const double r = interp ? lerp(ric[j], ric_next[j], alpha) : ric[j];
+            const double coulomb = coulomb_coeff * (1.0 + log(p * inv_n) * (1.0 / 74.8)) * gt->ce_inv_beta2[j];
+            radp = synch_coeff * p2 + r + coulomb + adiab * p;
+            dT = dtT_e;
+        }
+        B = radp - st.two_over_p[j] * D;
+        C = D;
+    }
+};
+
+template <int S>
+__device__ __forceinline__ SegTerms<S> seg_terms(const GridTables &gt, const Bg &bg, int dis,
+                                                 const SnapArgs &a, const SegInfo &g)
+{
+    SegTerms<S> T;
+    T.gt = &gt;
+    T.n_gas = bg.n_gas;
+    T.kbt = bg.kbt;
+    T.inv_kbt = 1.0 / bg.kbt;
+    T.inv_n = 1.0 / bg.n_gas;
+    T.adiab = 1.0 / 3.0 * (dis ? 0.0 : bg.divv);
+    const double b_ratio = bg.b_field * 1.0e+6 / 3.2;
+    T.synch_coeff = 4.8e-4 * b_ratio * b_ratio * 9.11e-28 * 3.0e+10 * 3.1536e+16;
+    T.coulomb_coeff = 3.05e-29 * bg.n_gas * kC * kGyr / (kMe * kGeV);
+    T.dt = g.dt;
+    T.dt_over_tloss_pref = g.dt / (1.0 / (0.5 * kC * bg.n_gas) / kGyr);
+    T.dtT_e = g.dt / 1.0e+100;
+    T.ric = a.ic_curr;
+    T.ric_next = a.ic_next;
+    T.alpha = g.alpha;
+    T.interp = g.nseg > 1;
+    T.dpp_inv = 0.0;
+    T.dpp_scale = 1.0;
+    T.dpp_fill = 0;
+    return T;
+}
+
+struct WarpSmem {
+    double B[kSw], C[kSw], D[kSw], Wp[kSw], Wm[kSw];
+};
+
 // The factored matrix of one system, distributed over the warp.
+template <bool SRC>
 struct Factor {
-    double inv[kRpl];    // 1 / d_i
-    double h[kRpl];      // a_i / d_i      (forward recurrence)
-    double q[kRpl];      // c_i / d_i      (back substitution)
-    double sd[kRpl];     // dt * source_i / d_i
+    double inv[kR];      // 1 / d_i
+    double h[kR];        // a_i / d_i      (forward recurrence)
+    double q[kR];        // c_i / d_i      (back substitution)
+    double sd[SRC ? kR : 1];  // dt * source_i / d_i
     double hk[5], qk[5]; // warp-scan multipliers per level
 };
 
-// Rows of the lane, then the factorisation.  Returns nonzero error bits.
-__device__ unsigned factorize(const SpeciesTerms &T, const double *src_dt, int lane, Factor &F)
+// Terms, faces, rows and the factorisation of one system.
+template <int S, bool SRC>
+__device__ unsigned factorize(const SegTerms<S> &T, const double *sdt, int lane, WarpSmem &sm,
+                              Factor<SRC> &F)
 {
-    const SpeciesTables &st = T.gt->s[T.s];
-    const double *x = st.p, *dx = st.dp;
-    const double dt = T.dt;
-    const int row0 = lane * kRpl;
+    const SpeciesTables &st = T.gt->s[S];
+    const double *x = st.p;
     unsigned err = 0;
 
-    double B[kRpl], C[kRpl], dT[kRpl];
-#pragma unroll
-    for (int r = 0; r < kRpl; r++) {
-        const Terms tt = T.at(row0 + r);
-        B[r] = tt.B;
-        C[r] = tt.C;
-        dT[r] = tt.dtT;
+    // terms, lane-strided
+#pragma unroll 1
+    for (int k = 0; k < kR; k++) {
+        const int j = k * 32 + lane;
+        double B, C, D;
+        T.at(j, B, C, D);
+        sm.B[swz(j)] = B;
+        sm.C[swz(j)] = C;
+        sm.D[swz(j)] = D;
     }
-    const double Bn = sdn(B[0], 1), Cn = sdn(C[0], 1);
-    const double Bp = sup(B[kRpl - 1], 1), Cp = sup(C[kRpl - 1], 1);
-
-    // faces j = row0 + r, between bins j and j+1 (j <= nb-2)
-    double Wp[kRpl], Wm[kRpl], w_nm1 = 0.0;
-#pragma unroll
-    for (int r = 0; r < kRpl; r++) {
-        const int j = row0 + r;
-        Wp[r] = 0.0;
-        Wm[r] = 0.0;
+    __syncwarp();
+    // faces j (between bins j and j+1), lane-strided
+#pragma unroll 1
+    for (int k = 0; k < kR; k++) {
+        const int j = k * 32 + lane;
+        double wp = 0.0, wm = 0.0;
         if (j <= NB - 2) {
-            const double Br = (r + 1 < kRpl) ? B[r + 1] : Bn;
-            const double Cr = (r + 1 < kRpl) ? C[r + 1] : Cn;
-            double w;
-            face(B[r], Br, C[r], Cr, x[j], x[j + 1], Wp[r], Wm[r], w);
-            if (j == NB - 2) w_nm1 = w;
+            const double cl = sm.C[swz(j)];
+            if (fabs(cl) > 1.0e-200) {
+                const double w = (sm.B[swz(j)] + sm.B[swz(j + 1)]) / (cl + sm.C[swz(j + 1)]) *
+                                 (x[j + 1] - x[j]);
+                face_weights(w, wp, wm);
+            }
         }
+        sm.Wp[swz(j)] = wp;
+        sm.Wm[swz(j)] = wm;
     }
-    const double WpP = sup(Wp[kRpl - 1], 1), WmP = sup(Wm[kRpl - 1], 1);
+    __syncwarp();
 
-    // rows a, b, c (cc_build_{left,interior,right}, Chang_Cooper.c:66-184)
-    double A[kRpl], Bd[kRpl], Cc[kRpl];
+    // rows a, b, c of this lane (cc_build_{left,interior,right}, Chang_Cooper.c:66-184)
+    const int row0 = lane * kR;
+    double A[kR], Bd[kR], Cc[kR];
 #pragma unroll
-    for (int r = 0; r < kRpl; r++) {
+    for (int r = 0; r < kR; r++) {
         const int m = row0 + r;
-        const double k = dt / (1.0 * dx[m]);
-        const double pB = (r > 0) ? B[r - 1] : Bp, pC = (r > 0) ? C[r - 1] : Cp;
-        const double nB = (r + 1 < kRpl) ? B[r + 1] : Bn, nC = (r + 1 < kRpl) ? C[r + 1] : Cn;
-        const double wpm = (r > 0) ? Wp[r - 1] : WpP, wmm = (r > 0) ? Wm[r - 1] : WmP;
-        double av, bv, cv;
+        const double k = T.dt * st.inv_dx[m];
+        const double Cm = sm.C[r * 33 + lane], Bm = sm.B[r * 33 + lane], Dm = sm.D[r * 33 + lane];
+        double av = 0.0, bv, cv = 0.0;
         if (m == 0) {
-            if (fabs(C[r]) > 1.0e-200) {
-                av = 0.0;
-                bv = 1.0 + k * (0.0 + 0.5 * (C[r] + nC) / (x[1] - x[0]) * Wm[r]) + dT[r];
-                cv = k * 0.5 * (C[r] + nC) / (x[1] - x[0]) * Wp[r];
+            const double nC = sm.C[swz(1)], nB = sm.B[swz(1)];
+            if (fabs(Cm) > 1.0e-200) {
+                const double cm12 = 0.5 * (Cm + nC) * st.inv_dxr[0];
+                bv = 1.0 + k * (0.0 + cm12 * sm.Wm[swz(0)]) + Dm;
+                cv = k * cm12 * sm.Wp[swz(0)];
             } else {
-                av = 0.0;
-                bv = 1.0 + k * 0.0 + dT[r];
-                cv = k * 1.0 * 0.5 * (B[r] + nB);
+                bv = 1.0 + k * 0.0 + Dm;
+                cv = k * 1.0 * 0.5 * (Bm + nB);
             }
-        } else if (m == NB - 1) {
-            if (fabs(C[r]) > 1.0e-200) {
-                av = k * (0.5 * (C[r] + pC)) / (x[m] - x[m - 1]) * wmm;
-                bv = 1.0 + k * ((0.5 * (C[r] + pC)) / (x[m] - x[m - 1]) * wpm) + dT[r];
-                if (isnan(av)) err |= kErrCcNan;
-            } else {
-                const double dlt = (fabs(pC) > 1.0e-200) ? face_delta(w_nm1) : 0.0;
-                av = -dlt * 0.5 * (B[r] + pB) * dt / (1.0 * dx[m]);
-                bv = 1.0 + k * (0.5 * (pB + B[r])) + dT[r];
-            }
-            cv = 0.0;
-        } else if (fabs(C[r]) > 1.0e-200) {
-            const double dxm_12 = x[m] - x[m - 1];
-            const double dxm12 = x[m + 1] - x[m];
-            const double cm_12 = 0.5 * (C[r] + pC);
-            const double cm12 = 0.5 * (C[r] + nC);
-            av = k * cm_12 / dxm_12 * wmm;
-            bv = 1.0 + k * (cm_12 / dxm_12 * wpm + cm12 / dxm12 * Wm[r]) + dT[r];
-            cv = k * cm12 / dxm12 * Wp[r];
         } else {
-            const double bm_12 = 0.5 * (B[r] + pB);
-            const double bm12 = 0.5 * (B[r] + nB);
-            av = 0.0;
-            bv = 1.0 + k * (1.0 * bm_12 - 0.0 * bm12) + dT[r];
-            cv = k * 1.0 * bm12;
+            const double pC = sm.C[swz(m - 1)], pB = sm.B[swz(m - 1)];
+            const double wpm = sm.Wp[swz(m - 1)], wmm = sm.Wm[swz(m - 1)];
+            if (m == NB - 1) {
+                if (fabs(Cm) > 1.0e-200) {
+                    const double cm_12 = 0.5 * (Cm + pC) * st.inv_dxl[m];
+                    av = k * cm_12 * wmm;
+                    bv = 1.0 + k * (cm_12 * wpm) + Dm;
+                    if (isnan(av)) err |= kErrCcNan;
+                } else {
+                    double dlt = 0.0;
+                    if (fabs(pC) > 1.0e-200)
+                        dlt = face_delta((pB + Bm) / (pC + Cm) * (x[m] - x[m - 1]));
+                    av = -dlt * 0.5 * (Bm + pB) * k;
+                    bv = 1.0 + k * (0.5 * (pB + Bm)) + Dm;
+                }
+            } else {
+                const double nC = sm.C[swz(m + 1)], nB = sm.B[swz(m + 1)];
+                if (fabs(Cm) > 1.0e-200) {
+                    const double cm_12 = 0.5 * (Cm + pC) * st.inv_dxl[m];
+                    const double cm12 = 0.5 * (Cm + nC) * st.inv_dxr[m];
+                    av = k * cm_12 * wmm;
+                    bv = 1.0 + k * (cm_12 * wpm + cm12 * sm.Wm[swz(m)]) + Dm;
+                    cv = k * cm12 * sm.Wp[swz(m)];
+                } else {
+                    // interior row below the diffusion floor: every delta the
+                    // reference reads here is zero (Chang_Cooper.c:91-103)
+                    bv = 1.0 + k * (0.5 * (Bm + pB)) + Dm;
+                    cv = k * 1.0 * 0.5 * (Bm + nB);
+                }
+            }
         }
         A[r] = av;
         Bd[r] = bv;
         Cc[r] = cv;
     }
+    __syncwarp();
 
     // ---- pivots: composed Moebius maps d -> b - a c_prev / d ----
-    const double c_in = sup(Cc[kRpl - 1], 1);   // c of the row before this lane's first
+    const double c_in = sup(Cc[kR - 1], 1);   // c of the row before this lane's first
     double t00 = 1.0, t01 = 0.0, t10 = 0.0, t11 = 1.0;
 #pragma unroll
-    for (int r = 0; r < kRpl; r++) {
+    for (int r = 0; r < kR; r++) {
         const double cprev = (r > 0) ? Cc[r - 1] : (lane > 0 ? c_in : 0.0);
         const double e = A[r] * cprev;
         const double n00 = Bd[r] * t00 - e * t10;
@@ -177,13 +271,10 @@ __device__ unsigned factorize(const SpeciesTerms &T, const double *src_dt, int l
             rescale2(t00, t01, t10, t11);
         }
     }
-    // incoming projective pivot (p, q) of this lane: exclusive prefix applied to (1, 0)
     double vp = sup(t00, 1), vq = sup(t10, 1);
-    if (lane == 0) { vp = 1.0; vq = 0.0; }
-    // cp of the previous row: -c_prev / d_prev with d_prev = vp / vq
     double cp_prev = (lane == 0) ? 0.0 : -c_in * vq / vp;
 #pragma unroll
-    for (int r = 0; r < kRpl; r++) {
+    for (int r = 0; r < kR; r++) {
         const int m = row0 + r;
         const double den = Bd[r] + A[r] * cp_prev;
         if (fabs(den) <= 1.0e-300) err |= kErrSingular;
@@ -191,14 +282,14 @@ __device__ unsigned factorize(const SpeciesTerms &T, const double *src_dt, int l
         F.inv[r] = inv;
         F.h[r] = A[r] * inv;
         F.q[r] = (m == NB - 1) ? 0.0 : Cc[r] * inv;
-        F.sd[r] = src_dt[r] * inv;
+        if (SRC) F.sd[r] = sdt[r] * inv;
         cp_prev = -Cc[r] * inv;
     }
 
     // ---- warp-scan multipliers of the two linear recurrences ----
     double H = 1.0, Q = 1.0;
 #pragma unroll
-    for (int r = 0; r < kRpl; r++) {
+    for (int r = 0; r < kR; r++) {
         H *= F.h[r];
         Q *= F.q[r];
     }
@@ -211,17 +302,19 @@ __device__ unsigned factorize(const SpeciesTerms &T, const double *src_dt, int l
         if (lane >= off) H *= Hu;
         if (lane + off < 32) Q *= Qd;
     }
+    (void)vp;
     return err;
 }
 
 // One implicit sub-step: N <- M^{-1} (N + dt src) with the factored M.
-__device__ __forceinline__ void substep(const Factor &F, int lane, double N[kRpl])
+template <bool SRC>
+__device__ __forceinline__ void substep(const Factor<SRC> &F, int lane, double N[kR])
 {
-    double y[kRpl];
+    double y[kR];
     double acc = 0.0;
 #pragma unroll
-    for (int r = 0; r < kRpl; r++) {
-        y[r] = fma(N[r], F.inv[r], F.sd[r]);
+    for (int r = 0; r < kR; r++) {
+        y[r] = SRC ? fma(N[r], F.inv[r], F.sd[r]) : N[r] * F.inv[r];
         acc = fma(F.h[r], acc, y[r]);
     }
 #pragma unroll
@@ -233,13 +326,13 @@ __device__ __forceinline__ void substep(const Factor &F, int lane, double N[kRpl
     double prev = sup(acc, 1);
     if (lane == 0) prev = 0.0;
 #pragma unroll
-    for (int r = 0; r < kRpl; r++) {
+    for (int r = 0; r < kR; r++) {
         prev = fma(F.h[r], prev, y[r]);
         y[r] = prev;
     }
     acc = 0.0;
 #pragma unroll
-    for (int r = kRpl - 1; r >= 0; r--) acc = fma(F.q[r], acc, y[r]);
+    for (int r = kR - 1; r >= 0; r--) acc = fma(F.q[r], acc, y[r]);
 #pragma unroll
     for (int lv = 0; lv < 5; lv++) {
         const int off = 1 << lv;
@@ -249,40 +342,46 @@ __device__ __forceinline__ void substep(const Factor &F, int lane, double N[kRpl
     prev = sdn(acc, 1);
     if (lane == 31) prev = 0.0;
 #pragma unroll
-    for (int r = kRpl - 1; r >= 0; r--) {
+    for (int r = kR - 1; r >= 0; r--) {
         prev = fma(F.q[r], prev, y[r]);
         N[r] = prev;
     }
 }
 
-__global__ void __launch_bounds__(128) fused_slot_kernel(FusedParams P)
+// Systems of species S for tracers with a segment in this slot: warp w of
+// block b handles tracer b * kWarps + w.
+template <int S, bool SRC>
+__global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) fused_slot_kernel(FusedParams P)
 {
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    extern __shared__ double4 smem_raw[];
+    WarpSmem *smem = reinterpret_cast<WarpSmem *>(smem_raw);
+    const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const SnapArgs &a = P.a;
-    const int t = gw >> 1, s = gw & 1;
+    const int t = blockIdx.x * kWarps + w;
     if (t >= a.ntracer) return;
-    if (!(P.mp.species_mask & (1 << s))) return;
     const SegInfo g = seg_info(a.sched, t, P.slot, a.dt_snap);
     if (!g.active) return;
     const Bg bg = load_bg(a, t, g);
     const double tacc = segment_tacc(P.mp, a, g);
     const int dis = a.dis ? a.dis[t] : 0;
-    SpeciesTerms T = make_species_terms(P.gt, s, bg, dis, a, g);
-    const int row0 = lane * kRpl;
+    SegTerms<S> T = seg_terms<S>(P.gt, bg, dis, a, g);
+    const int row0 = lane * kR;
 
-    double *Nrow = (s == 0 ? a.crp : a.cre) + (size_t)t * NB + row0;
-    double N[kRpl];
+    double *Nrow = (S == 0 ? a.crp : a.cre) + (size_t)t * NB + row0;
+    double N[kR];
 #pragma unroll
-    for (int r = 0; r < kRpl; r += 2) {
+    for (int r = 0; r < kR; r += 2) {
         const double2 v = *reinterpret_cast<const double2 *>(Nrow + r);
         N[r] = v.x;
         N[r + 1] = v.y;
     }
-    const double *src = (s == 0) ? a.qpi : (P.inje ? P.inje : a.qepri);
-    double sdt[kRpl];
+    double sdt[SRC ? kR : 1];
+    if (SRC) {
+        const double *src = (S == 0) ? a.qpi : (P.inje ? P.inje : a.qepri);
 #pragma unroll
-    for (int r = 0; r < kRpl; r++) sdt[r] = src ? g.dt * src[(size_t)t * NB + row0 + r] : g.dt * 0.0;
+        for (int r = 0; r < kR; r++) sdt[r] = g.dt * src[(size_t)t * NB + row0 + r];
+    }
 
     const DppForm on = dpp_form(P.mp, P.mp.dpp_model, bg, tacc);
     const double on_scale = (P.mp.dpp_model != kDppOff)
@@ -290,22 +389,24 @@ __global__ void __launch_bounds__(128) fused_slot_kernel(FusedParams P)
                         a.cre + (size_t)t * NB, 1)
         : 1.0;
 
-    Factor F;
+    Factor<SRC> F;
     int cur = -1;
     unsigned err = 0;
+#pragma unroll 1
     for (int istep = 0; istep < g.steps; istep++) {
         const int want = (!g.windowed || (istep >= g.sl && istep < g.el)) ? 0 : 1;
         if (want != cur) {
-            T.dform = want == 0 ? on : DppForm{0, 0.0};
+            T.dpp_fill = want == 0 ? on.fill : 0;
+            T.dpp_inv = want == 0 ? on.inv : 0.0;
             T.dpp_scale = want == 0 ? on_scale : 1.0;
-            err |= factorize(T, sdt, lane, F);
+            err |= factorize<S, SRC>(T, sdt, lane, smem[w], F);
             cur = want;
         }
-        substep(F, lane, N);
+        substep<SRC>(F, lane, N);
     }
     if (err && lane == 0) atomicOr(a.err, err);
 #pragma unroll
-    for (int r = 0; r < kRpl; r += 2)
+    for (int r = 0; r < kR; r += 2)
         *reinterpret_cast<double2 *>(Nrow + r) = make_double2(N[r], N[r + 1]);
 }
 
@@ -369,6 +470,28 @@ __global__ void __launch_bounds__(256) fused_secondary_kernel(FusedParams P, dou
     }
 }
 
+template <int S, bool SRC>
+cudaError_t launch_one(Context &ctx, const FusedParams &P)
+{
+    constexpr size_t smem = kWarps * sizeof(WarpSmem);
+    static bool configured = false;   // per instantiation; set before the first launch
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(fused_slot_kernel<S, SRC>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    const int blocks = (P.a.ntracer + kWarps - 1) / kWarps;
+    fused_slot_kernel<S, SRC><<<blocks, kWarps * 32, smem, ctx.stream>>>(P);
+    return cudaGetLastError();
+}
+
+template <int S>
+cudaError_t launch_slot(Context &ctx, const FusedParams &P, bool src)
+{
+    return src ? launch_one<S, true>(ctx, P) : launch_one<S, false>(ctx, P);
+}
+
 }  // namespace
 
 int fused_reserve(Context &ctx, int cap)
@@ -387,14 +510,13 @@ int run_fused(Context &ctx, const SnapArgs &a)
     P.mp = ctx.mp;
     P.np_min_qe = ctx.d_np_min_qe;
     const int nslots = ctx.mp.interp_max_segments < 1 ? 1 : ctx.mp.interp_max_segments;
-    const int both = (ctx.mp.species_mask & 3) == 3;
-    const long long nthreads = 2LL * a.ntracer * 32;
-    const int blocks = (int)((nthreads + 127) / 128);
+    const int protons = ctx.mp.species_mask & CROMA_SPECIES_PROTON;
+    const int electrons = ctx.mp.species_mask & CROMA_SPECIES_ELECTRON;
     for (int slot = 0; slot < nslots && slot < 64; slot++) {
         P.slot = slot;
         cudaEvent_t ev = nullptr;
         P.inje = nullptr;
-        if (both) {
+        if (protons && electrons) {
             dim3 sg((a.ntracer + 63) / 64, (NB + 63) / 64), sb(16, 16);
             timed_begin(ctx, kKindSecondary, &ev);
             fused_secondary_kernel<<<sg, sb, 0, ctx.stream>>>(P, ctx.d_inje);
@@ -403,9 +525,15 @@ int run_fused(Context &ctx, const SnapArgs &a)
             P.inje = ctx.d_inje;
         }
         timed_begin(ctx, kKindEvolve, &ev);
-        fused_slot_kernel<<<blocks, 128, 0, ctx.stream>>>(P);
+        if (protons) {
+            CROMA_CUDA(launch_slot<0>(ctx, P, a.qpi != nullptr));
+            ctx.last_launches += 1;
+        }
+        if (electrons) {
+            CROMA_CUDA(launch_slot<1>(ctx, P, P.inje != nullptr || a.qepri != nullptr));
+            ctx.last_launches += 1;
+        }
         timed_end(ctx, kKindEvolve, ev);
-        ctx.last_launches += 1;
         CROMA_CUDA(cudaGetLastError());
     }
     return 0;

@@ -163,9 +163,10 @@ int build_tables(Context &ctx)
     }
 
     // ---- caches, FP_Coef.c:77-156 and the grid-only kinematics ----
-    enum { T_P, T_DP, T_E, T_P2, T_CUT, T_2P, T_EXPE, T_SPARE, T_PER };   // per species
+    enum { T_P, T_DP, T_E, T_P2, T_CUT, T_2P, T_EXPE, T_IDX, T_IDXL, T_IDXR, T_PER };   // per species
     const int nspecies_arrays = T_PER * 2;
-    const int n_extra = 5;   // cp_Ep, cp_kin, cp_inv_betap2, sig_eff, ce_beta2
+    // cp_Ep, cp_kin, cp_inv_betap2, sig_eff, ce_beta2, cp_inv2mpkin, ce_inv_beta2
+    const int n_extra = 7;
     const size_t tab_doubles = (size_t)(nspecies_arrays + n_extra) * n + (size_t)n * n;
     std::vector<double> h(tab_doubles, 0.0);
     auto arr = [&](int k) { return h.data() + (size_t)k * n; };
@@ -173,6 +174,7 @@ int build_tables(Context &ctx)
         double *P = arr(s * T_PER + T_P), *DP = arr(s * T_PER + T_DP), *E = arr(s * T_PER + T_E);
         double *P2 = arr(s * T_PER + T_P2), *CUT = arr(s * T_PER + T_CUT);
         double *TWO = arr(s * T_PER + T_2P), *EXPE = arr(s * T_PER + T_EXPE);
+        double *IDX = arr(s * T_PER + T_IDX), *IDXL = arr(s * T_PER + T_IDXL), *IDXR = arr(s * T_PER + T_IDXR);
         for (int j = 0; j < n; j++) {
             P[j] = ctx.h_p[s][j];
             DP[j] = ctx.h_dp[s][j];
@@ -181,11 +183,17 @@ int build_tables(Context &ctx)
             CUT[j] = exp(-1.0 / P[j]);
             TWO[j] = 2.0 / P[j];
             EXPE[j] = (s == 0) ? exp(-E[j] / kEpMax) : 1.0;
+            IDX[j] = 1.0 / DP[j];
+        }
+        for (int j = 0; j < n; j++) {
+            IDXL[j] = (j >= 1) ? 1.0 / (ctx.h_p[s][j] - ctx.h_p[s][j - 1]) : 0.0;
+            IDXR[j] = (j <= n - 2) ? 1.0 / (ctx.h_p[s][j + 1] - ctx.h_p[s][j]) : 0.0;
         }
     }
     double *cpEp = arr(nspecies_arrays + 0), *cpKin = arr(nspecies_arrays + 1);
     double *cpIb = arr(nspecies_arrays + 2), *sigEff = arr(nspecies_arrays + 3);
-    double *ceB2 = arr(nspecies_arrays + 4);
+    double *ceB2 = arr(nspecies_arrays + 4), *cpI2 = arr(nspecies_arrays + 5);
+    double *ceIB2 = arr(nspecies_arrays + 6);
     std::vector<double> sigma(n), sigmoid(n);
     for (int j = 0; j < n; j++) sigma[j] = pp_pion_xsec(2, kMp * ctx.h_p[0][j]);
     int j_pp = 0;
@@ -205,8 +213,10 @@ int build_tables(Context &ctx)
         double sg = (j > j_pp) ? sigma[j] : sigma[j_pp];
         sg *= sigmoid[j];
         sigEff[j] = sg;
+        cpI2[j] = 1.0 / (2.0 * kMp * cpKin[j]);
         const double pe2 = ctx.h_p[1][j] * ctx.h_p[1][j];
         ceB2[j] = pe2 / (1.0 + pe2);
+        ceIB2[j] = 1.0 / ceB2[j];
     }
 
     // ---- device allocation ----
@@ -222,7 +232,9 @@ int build_tables(Context &ctx)
         st.exp_cut = darr(s * T_PER + T_CUT);
         st.two_over_p = darr(s * T_PER + T_2P);
         st.expE = darr(s * T_PER + T_EXPE);
-        st.inv_dx_next = darr(s * T_PER + T_SPARE);
+        st.inv_dx = darr(s * T_PER + T_IDX);
+        st.inv_dxl = darr(s * T_PER + T_IDXL);
+        st.inv_dxr = darr(s * T_PER + T_IDXR);
         st.pm1 = ctx.h_pm1[s];
         st.pp1 = ctx.h_pp1[s];
         st.pm1_p2 = st.pm1 * st.pm1;
@@ -237,6 +249,8 @@ int build_tables(Context &ctx)
     ctx.gt.cp_inv_betap2 = darr(nspecies_arrays + 2);
     ctx.gt.sig_eff = darr(nspecies_arrays + 3);
     ctx.gt.ce_beta2 = darr(nspecies_arrays + 4);
+    ctx.gt.cp_inv2mpkin = darr(nspecies_arrays + 5);
+    ctx.gt.ce_inv_beta2 = darr(nspecies_arrays + 6);
     for (int k = 0; k < 2; k++) {
         const double p = k == 0 ? ctx.h_pm1[0] : ctx.h_pp1[0], p2 = p * p;
         const double gamma = sqrt(1.0 + p2);
