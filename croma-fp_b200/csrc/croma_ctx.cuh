@@ -68,7 +68,9 @@ struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
 
-    // host copies of the grids (p, dp, E per species; pm1/pp1)
+    // host copies of the grids (p, dp, E per species; pm1/pp1); grid_given:
+    // filled by the caller (reference ABI) instead of from pmin/pmax
+    int grid_given = 0;
     std::vector<double> h_p[2], h_dp[2], h_E[2];
     double h_pm1[2] = {0, 0}, h_pp1[2] = {0, 0};
     std::vector<double> h_fqe;        // [nb][nb] transposed [jp][je]

@@ -211,6 +211,10 @@ __device__ __forceinline__ SpeciesTerms make_species_terms(const GridTables &gt,
     return T;
 }
 
+// fused.cu: one caller-defined segment for every tracer (ic_stride 0: one
+// shared IC row; otherwise per-tracer rows, momentum-major [nb][ic_stride]).
+int run_fused_segment(Context &ctx, const SnapArgs &a, const SegInfo &ex, int ic_stride);
+
 // cpu_direct_tacc_value (src/tracer_fp_batch.c:44-62): the direct t_acc of
 // a segment, switched to t_acc_off before t_off.
 __device__ __forceinline__ double segment_tacc(const ModelParams &mp, const SnapArgs &a, const SegInfo &g)

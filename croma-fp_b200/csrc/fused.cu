@@ -44,7 +44,19 @@ struct FusedParams {
     int slot;
     const double *inje;      // [tracer][nb] electron source of the slot, or null
     const int *np_min_qe;    // [nb]
+    // One caller-defined segment shared by every tracer (run_tracer_pipeline):
+    // when set, ex replaces the per-tracer schedule.
+    int explicit_seg;
+    SegInfo ex;
+    // IC rows: shared row (stride 0) or per tracer, momentum-major
+    // [nb][ntracer] (stride = ntracer)
+    int ic_stride;
 };
+
+__device__ __forceinline__ SegInfo segment_of(const FusedParams &P, int t)
+{
+    return P.explicit_seg ? P.ex : seg_info(P.a.sched, t, P.slot, P.a.dt_snap);
+}
 
 __device__ __forceinline__ int swz(int m) { return (m % kR) * 33 + m / kR; }
 __device__ __forceinline__ double sup(double v, int d) { return __shfl_up_sync(kFull, v, d); }
@@ -71,7 +83,8 @@ struct SegTerms {
     double dtT_e;                    // electrons: dt / 1e100
     double dpp_inv, dpp_scale;
     int dpp_fill;
-    const double *ric, *ric_next;
+    const double *ric, *ric_next;   // already offset to this tracer
+    int ric_stride;                 // bin stride of the IC row
     double alpha;
     int interp;
 
@@ -98,7 +111,8 @@ struct SegTerms {
             radp = coul + adiab * p;
             dT = gt->sig_eff[j] * dt_over_tloss_pref;
         } else {
-            const double r = interp ? lerp(ric[j], ric_next[j], alpha) : ric[j];
+            const double r0 = ric[j * ric_stride];
+            const double r = interp ? lerp(r0, ric_next[j * ric_stride], alpha) : r0;
             const double coulomb = coulomb_coeff * (1.0 + log(p * inv_n) * (1.0 / 74.8)) * gt->ce_inv_beta2[j];
             radp = synch_coeff * p2 + r + coulomb + adiab * p;
             dT = dtT_e;
@@ -110,7 +124,8 @@ struct SegTerms {
 
 template <int S>
 __device__ __forceinline__ SegTerms<S> seg_terms(const GridTables &gt, const Bg &bg, int dis,
-                                                 const SnapArgs &a, const SegInfo &g)
+                                                 const SnapArgs &a, const SegInfo &g, int t,
+                                                 int ic_stride)
 {
     SegTerms<S> T;
     T.gt = &gt;
@@ -125,8 +140,9 @@ __device__ __forceinline__ SegTerms<S> seg_terms(const GridTables &gt, const Bg 
     T.dt = g.dt;
     T.dt_over_tloss_pref = g.dt / (1.0 / (0.5 * kC * bg.n_gas) / kGyr);
     T.dtT_e = g.dt / 1.0e+100;
-    T.ric = a.ic_curr;
-    T.ric_next = a.ic_next;
+    T.ric = a.ic_curr + (ic_stride ? t : 0);
+    T.ric_next = a.ic_next + (ic_stride ? t : 0);
+    T.ric_stride = ic_stride ? ic_stride : 1;
     T.alpha = g.alpha;
     T.interp = g.nseg > 1;
     T.dpp_inv = 0.0;
@@ -360,12 +376,12 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) fused_slot_k
     const SnapArgs &a = P.a;
     const int t = blockIdx.x * kWarps + w;
     if (t >= a.ntracer) return;
-    const SegInfo g = seg_info(a.sched, t, P.slot, a.dt_snap);
+    const SegInfo g = segment_of(P, t);
     if (!g.active) return;
     const Bg bg = load_bg(a, t, g);
     const double tacc = segment_tacc(P.mp, a, g);
     const int dis = a.dis ? a.dis[t] : 0;
-    SegTerms<S> T = seg_terms<S>(P.gt, bg, dis, a, g);
+    SegTerms<S> T = seg_terms<S>(P.gt, bg, dis, a, g, t, P.ic_stride);
     const int row0 = lane * kR;
 
     double *Nrow = (S == 0 ? a.crp : a.cre) + (size_t)t * NB + row0;
@@ -457,7 +473,7 @@ __global__ void __launch_bounds__(256) fused_secondary_kernel(FusedParams P, dou
     for (int i = 0; i < 4; i++) {
         const int t = t0 + ty + 16 * i;
         if (t >= a.ntracer) continue;
-        const SegInfo g = seg_info(a.sched, t, P.slot, a.dt_snap);
+        const SegInfo g = segment_of(P, t);
         if (!g.active) continue;
         const double ng = (g.nseg > 1) ? lerp(a.bg_curr[t], a.bg_next[t], g.alpha) : a.bg_curr[t];
 #pragma unroll
@@ -502,6 +518,37 @@ int fused_reserve(Context &ctx, int cap)
     return 0;
 }
 
+// One slot: the secondary source (when both species evolve), then the
+// proton and electron systems.
+static int fused_one_slot(Context &ctx, FusedParams &P)
+{
+    const SnapArgs &a = P.a;
+    const int protons = ctx.mp.species_mask & CROMA_SPECIES_PROTON;
+    const int electrons = ctx.mp.species_mask & CROMA_SPECIES_ELECTRON;
+    cudaEvent_t ev = nullptr;
+    P.inje = nullptr;
+    if (protons && electrons) {
+        dim3 sg((a.ntracer + 63) / 64, (NB + 63) / 64), sb(16, 16);
+        timed_begin(ctx, kKindSecondary, &ev);
+        fused_secondary_kernel<<<sg, sb, 0, ctx.stream>>>(P, ctx.d_inje);
+        timed_end(ctx, kKindSecondary, ev);
+        ctx.last_launches += 1;
+        P.inje = ctx.d_inje;
+    }
+    timed_begin(ctx, kKindEvolve, &ev);
+    if (protons) {
+        CROMA_CUDA(launch_slot<0>(ctx, P, a.qpi != nullptr));
+        ctx.last_launches += 1;
+    }
+    if (electrons) {
+        CROMA_CUDA(launch_slot<1>(ctx, P, P.inje != nullptr || a.qepri != nullptr));
+        ctx.last_launches += 1;
+    }
+    timed_end(ctx, kKindEvolve, ev);
+    CROMA_CUDA(cudaGetLastError());
+    return 0;
+}
+
 int run_fused(Context &ctx, const SnapArgs &a)
 {
     FusedParams P;
@@ -509,34 +556,30 @@ int run_fused(Context &ctx, const SnapArgs &a)
     P.gt = ctx.gt;
     P.mp = ctx.mp;
     P.np_min_qe = ctx.d_np_min_qe;
+    P.explicit_seg = 0;
+    P.ex = SegInfo{};
+    P.ic_stride = 0;
     const int nslots = ctx.mp.interp_max_segments < 1 ? 1 : ctx.mp.interp_max_segments;
-    const int protons = ctx.mp.species_mask & CROMA_SPECIES_PROTON;
-    const int electrons = ctx.mp.species_mask & CROMA_SPECIES_ELECTRON;
     for (int slot = 0; slot < nslots && slot < 64; slot++) {
         P.slot = slot;
-        cudaEvent_t ev = nullptr;
-        P.inje = nullptr;
-        if (protons && electrons) {
-            dim3 sg((a.ntracer + 63) / 64, (NB + 63) / 64), sb(16, 16);
-            timed_begin(ctx, kKindSecondary, &ev);
-            fused_secondary_kernel<<<sg, sb, 0, ctx.stream>>>(P, ctx.d_inje);
-            timed_end(ctx, kKindSecondary, ev);
-            ctx.last_launches += 1;
-            P.inje = ctx.d_inje;
-        }
-        timed_begin(ctx, kKindEvolve, &ev);
-        if (protons) {
-            CROMA_CUDA(launch_slot<0>(ctx, P, a.qpi != nullptr));
-            ctx.last_launches += 1;
-        }
-        if (electrons) {
-            CROMA_CUDA(launch_slot<1>(ctx, P, P.inje != nullptr || a.qepri != nullptr));
-            ctx.last_launches += 1;
-        }
-        timed_end(ctx, kKindEvolve, ev);
-        CROMA_CUDA(cudaGetLastError());
+        int rc = fused_one_slot(ctx, P);
+        if (rc) return rc;
     }
     return 0;
+}
+
+int run_fused_segment(Context &ctx, const SnapArgs &a, const SegInfo &ex, int ic_stride)
+{
+    FusedParams P;
+    P.a = a;
+    P.gt = ctx.gt;
+    P.mp = ctx.mp;
+    P.np_min_qe = ctx.d_np_min_qe;
+    P.slot = 0;
+    P.explicit_seg = 1;
+    P.ex = ex;
+    P.ic_stride = ic_stride;
+    return fused_one_slot(ctx, P);
 }
 
 }  // namespace croma

@@ -1,0 +1,761 @@
+// ref_abi.cu -- the reference-compatible C ABI (include/fp_cuda_backend.h).
+//
+// Each entry point keeps the reference's name, arguments, ownership and
+// return codes (include/fp_cuda_backend.h:92-159 of kosukenishiwaki/croma-fp)
+// and runs on this library's kernels:
+//
+//   run_tracer_pipeline      one (bucket, segment) call of the snapshot driver
+//                            (include/tracer_fp_solve.inc:1341-1463): rows and
+//                            factorisation on chip, fused sub-steps (fused.cu),
+//                            secondary source of the segment
+//   cuda_rank_state_*        rank-global device spectra and sources
+//                            (src/fp_cuda_workspace.cu:440-524)
+//   solve_cc_cuda_batch      one implicit Chang-Cooper step for a batch of
+//                            tridiagonal systems (src/fp_cuda_solver.cu:436-495)
+//   prepare_*_emission_cuda_batch
+//                            synchrotron (pitch-kernel table), hadronic gamma and
+//                            neutrino emissivities (src/fp_cuda_emission.cu)
+//
+// The workspace builds its grid tables from the first call's CRspectrum grids
+// and rebuilds them when the grids change.  Model switches come from CROMA's
+// globals when the library is linked into CROMA (weak references) and from
+// croma_b200_set_model() otherwise.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#define np CROMA_NB
+#define npe CROMA_NB
+#include "../../include/fp_cuda_backend.h"
+#include "croma_segment.cuh"
+
+// CROMA's parameter globals (include/params.h): bound when present.
+extern "C" {
+extern char dpp_mode_spec[] __attribute__((weak));
+extern int ttd_tacc_model __attribute__((weak));
+extern double t_acc_direct_gyr __attribute__((weak));
+extern double eta_dpp_cap __attribute__((weak));
+}
+
+using namespace croma;
+
+struct FpCudaPipelineWorkspace {
+    Context ctx;
+    int ready = 0;
+    double key[6] = {0, 0, 0, 0, 0, 0};
+    // bucket scratch (capacity bcap tracers)
+    int bcap = 0;
+    double *b_bg = nullptr;      // [2][8][ncell]
+    double *b_ric = nullptr;     // [2][nb][ncell]
+    double *b_crp = nullptr, *b_cre = nullptr, *b_qpi = nullptr, *b_qepri = nullptr;   // [ncell][nb]
+    double *b_mass = nullptr;
+    unsigned char *b_dis = nullptr;
+    int *b_idx = nullptr;
+    int b_n = 0, b_has_src = 0;
+    // rank-global state (capacity rcap tracers)
+    int rcap = 0, r_n = 0;
+    double *r_crp = nullptr, *r_cre = nullptr, *r_qpi = nullptr, *r_qepri = nullptr;
+    std::vector<double> h_stage;   // host staging for field packing
+};
+
+namespace {
+
+struct ModelSetter {
+    int dpp_model = kDppOff;
+    int ttd_model = 1;
+    double t_acc_direct = 0.0;
+    double eta_cap = 0.0;
+};
+ModelSetter g_model;
+std::mutex g_mutex;
+
+int resolve_dpp_model()
+{
+    if (&dpp_mode_spec[0] != nullptr) {
+        const char *s = dpp_mode_spec;
+        if (strcmp(s, "asa") == 0) return kDppAsa;
+        if (strcmp(s, "ttd") == 0) return kDppTtd;
+        if (strcmp(s, "direct_tacc") == 0 || strcmp(s, "tacc") == 0 || strcmp(s, "direct") == 0)
+            return kDppDirect;
+        return kDppOff;   // resolve_momentumdiff_model, src/fp_shared_core.c:932-957
+    }
+    return g_model.dpp_model;
+}
+
+void fill_model(ModelParams &mp, double psi, double mach_limit)
+{
+    mp.species_mask = 3;
+    mp.dpp_model = resolve_dpp_model();
+    mp.ttd_brunetti16 = (&ttd_tacc_model != nullptr) ? (ttd_tacc_model == 1) : (g_model.ttd_model == 1);
+    mp.t_acc_direct_gyr = (&t_acc_direct_gyr != nullptr) ? t_acc_direct_gyr : g_model.t_acc_direct;
+    mp.eta_dpp_cap = (&eta_dpp_cap != nullptr) ? eta_dpp_cap : g_model.eta_cap;
+    mp.mach_limit = mach_limit;
+    mp.psi3 = pow(psi, 3.0);
+    mp.t_off_gyr = 0.0;        // the host applies the direct-t_acc schedule per call
+    mp.t_acc_off_gyr = 0.0;
+    mp.window_centred = 1;
+    mp.interp_max_segments = 1;
+    mp.interp_min_steps = 1;
+}
+
+int fail(int code, const char *msg)
+{
+    set_error(msg);
+    return code;
+}
+
+__global__ void gather_rows_kernel(int n, const int *idx, const double *src, double *dst)
+{
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (size_t)n * NB) return;
+    const int i = (int)(k / NB), j = (int)(k % NB);
+    dst[k] = src[(size_t)idx[i] * NB + j];
+}
+
+__global__ void scatter_rows_kernel(int n, const int *idx, const double *src, double *dst)
+{
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (size_t)n * NB) return;
+    const int i = (int)(k / NB), j = (int)(k % NB);
+    dst[(size_t)idx[i] * NB + j] = src[k];
+}
+
+int ensure_bucket(FpCudaPipelineWorkspace *w, int n)
+{
+    if (n <= w->bcap) return 0;
+    Context &c = w->ctx;
+    cudaFree(w->b_bg); cudaFree(w->b_ric); cudaFree(w->b_crp); cudaFree(w->b_cre);
+    cudaFree(w->b_qpi); cudaFree(w->b_qepri); cudaFree(w->b_mass); cudaFree(w->b_dis); cudaFree(w->b_idx);
+    const size_t st = (size_t)n * NB * sizeof(double);
+    CROMA_CUDA(cudaMalloc(&w->b_bg, 2 * (size_t)kNbg * n * sizeof(double)));
+    CROMA_CUDA(cudaMalloc(&w->b_ric, 2 * st));
+    CROMA_CUDA(cudaMalloc(&w->b_crp, st));
+    CROMA_CUDA(cudaMalloc(&w->b_cre, st));
+    CROMA_CUDA(cudaMalloc(&w->b_qpi, st));
+    CROMA_CUDA(cudaMalloc(&w->b_qepri, st));
+    CROMA_CUDA(cudaMalloc(&w->b_mass, (size_t)n * sizeof(double)));
+    CROMA_CUDA(cudaMalloc(&w->b_dis, (size_t)n));
+    CROMA_CUDA(cudaMalloc(&w->b_idx, (size_t)n * sizeof(int)));
+    int rc = fused_reserve(c, n);
+    if (rc) return rc;
+    w->bcap = n;
+    return 0;
+}
+
+int ensure_tables(FpCudaPipelineWorkspace *w, const CRspectrum *crp, const CRspectrum *cre)
+{
+    const double key[6] = {crp->p[0], crp->p[np - 1], crp->pm1, cre->p[0], cre->p[npe - 1], cre->pm1};
+    if (w->ready && memcmp(key, w->key, sizeof key) == 0) return 0;
+    Context &c = w->ctx;
+    c.grid_given = 1;
+    const CRspectrum *g[2] = {crp, cre};
+    for (int s = 0; s < 2; s++) {
+        c.h_p[s].assign(g[s]->p, g[s]->p + NB);
+        c.h_dp[s].assign(g[s]->dp, g[s]->dp + NB);
+        c.h_E[s].assign(g[s]->E, g[s]->E + NB);
+        c.h_pm1[s] = g[s]->pm1;
+        c.h_pp1[s] = g[s]->pp1;
+    }
+    int rc = build_tables(c);
+    if (rc) return rc;
+    memcpy(w->key, key, sizeof key);
+    w->ready = 1;
+    return 0;
+}
+
+// Upload one FpCoeffBatchInput field set (8 background fields) into a
+// field-major [8][n] device block through host staging.
+int upload_bg(FpCudaPipelineWorkspace *w, const double *const f[8], int n, double *dst)
+{
+    w->h_stage.resize((size_t)kNbg * n);
+    for (int k = 0; k < kNbg; k++) {
+        if (f[k]) memcpy(w->h_stage.data() + (size_t)k * n, f[k], (size_t)n * sizeof(double));
+        else memset(w->h_stage.data() + (size_t)k * n, 0, (size_t)n * sizeof(double));
+    }
+    CROMA_CUDA(cudaMemcpyAsync(dst, w->h_stage.data(), (size_t)kNbg * n * sizeof(double),
+                               cudaMemcpyHostToDevice, w->ctx.stream));
+    CROMA_CUDA(cudaStreamSynchronize(w->ctx.stream));
+    return 0;
+}
+
+double elapsed(cudaEvent_t a, cudaEvent_t b)
+{
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+
+// ---- one implicit Chang-Cooper step per system: fp_thomas_solve_ws with the
+// RHS of solve_cc_batch_cpu_timed (src/fp_shared_core.c:226-257, 564-615).
+// cprime is the kernel's scratch, [nsys][nrow].
+__global__ void cc_thomas_kernel(int nsys, int nrow, double dt, const double *a, const double *b,
+                                 const double *c, const double *src, const double *x_in,
+                                 double *x_out, double *cprime, unsigned *err)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    const size_t o = (size_t)s * nrow;
+    double *cp = cprime + o;
+    double *x = x_out + o;
+    if (fabs(b[o]) <= 1.0e-300) { atomicOr(err, kErrSingular); return; }
+    cp[0] = -c[o] / b[o];
+    x[0] = (dt * src[o] + x_in[o]) / b[o];
+    for (int i = 1; i < nrow; i++) {
+        const double den = b[o + i] + a[o + i] * cp[i - 1];
+        if (fabs(den) <= 1.0e-300) { atomicOr(err, kErrSingular); return; }
+        cp[i] = (i == nrow - 1) ? 0.0 : -c[o + i] / den;
+        x[i] = ((dt * src[o + i] + x_in[o + i]) + a[o + i] * x[i - 1]) / den;
+    }
+    for (int i = nrow - 2; i >= 0; i--) x[i] -= cp[i] * x[i + 1];
+}
+
+// ---- emission kernels ----
+// Q_one (src/EMISSION.c:297-308) times E n_gas, one thread per (cell, bin).
+__global__ void hadronic_emission_kernel(int ncell, int nbins, const double *crp, const double *n_gas,
+                                         const double *beta_p, const double *dp, const double *kern,
+                                         const double *E, double *out)
+{
+    const int ng = blockIdx.y * blockDim.y + threadIdx.y;
+    const int icell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (icell >= ncell || ng >= nbins) return;
+    const double *N = crp + (size_t)icell * NB;
+    const double *f = kern + (size_t)ng * NB;
+    double fpre = beta_p[0] * N[0] * f[0], integral = 0.0;
+    for (int i = 1; i < NB; i++) {
+        const double fn = beta_p[i] * N[i] * f[i];
+        integral += (fpre + fn) * dp[i];
+        fpre = fn;
+    }
+    out[(size_t)icell * nbins + ng] = E[ng] * (integral * 0.5) * n_gas[icell];
+}
+
+// prepare_synch_emission_cell_major, pitch-kernel-table branch
+// (src/fp_shared_core.c:2070-2112 with tracer_fp_interp_synch_kernel_logk :2054-2068).
+__global__ void synch_table_kernel(int ncell, int nfreq, int nlogb, double logb_min, double inv_dlogb,
+                                   double a0, double den1, double den2, const double *table,
+                                   const double *b_dyn, const double *logb, const double *cre,
+                                   const double *dp, double *out)
+{
+    const int nf = blockIdx.y * blockDim.y + threadIdx.y;
+    const int icell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (icell >= ncell || nf >= nfreq) return;
+    const double *N = cre + (size_t)icell * NB;
+    const double A = a0 * b_dyn[icell] / den1 / den2;
+    const double u = (logb[icell] - logb_min) * inv_dlogb;
+    int ib = (int)floor(u);
+    if (ib < 0) ib = 0;
+    if (ib > nlogb - 2) ib = nlogb - 2;
+    double t = u - (double)ib;
+    if (t < 0.0) t = 0.0;
+    if (t > 1.0) t = 1.0;
+    const double *k0 = table + ((size_t)ib * nfreq + nf) * NB;
+    const double *k1 = table + ((size_t)(ib + 1) * nfreq + nf) * NB;
+    double integral = 0.0;
+    for (int je = 2; je < NB - 1 && N[je + 1] > 0.0; je++) {
+        const double a = k0[je], b = k1[je];
+        double K;
+        if (t <= 0.0) K = a;
+        else if (t >= 1.0) K = b;
+        else if (a > 0.0 && b > 0.0) K = exp((1.0 - t) * log(a) + t * log(b));
+        else K = (1.0 - t) * a + t * b;
+        integral += N[je] * K * dp[je];
+    }
+    out[(size_t)icell * nfreq + nf] = A * integral;
+}
+
+// One-shot device buffers of the stateless entry points (grow-only, guarded).
+struct Scratch {
+    std::vector<void *> ptrs;
+    ~Scratch() { release(); }
+    void release()
+    {
+        for (void *p : ptrs) cudaFree(p);
+        ptrs.clear();
+    }
+    cudaError_t get(void **out, size_t bytes)
+    {
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes ? bytes : 8);
+        if (e == cudaSuccess) ptrs.push_back(p);
+        *out = p;
+        return e;
+    }
+};
+
+int emission_hadronic(int ncell, int nbins, double emin, double emax, const double *crp_batch,
+                      const double *n_gas, const double *beta_p, const double *kern,
+                      const CRspectrum *grid, double *out, double *elapsed_ms)
+{
+    if (ncell <= 0 || nbins <= 0 || !crp_batch || !n_gas || !beta_p || !kern || !grid || !out)
+        return fail(-1, "invalid emission arguments");
+    // E grid as the reference accumulates it (fp_shared_core.c:2178-2188)
+    std::vector<double> E(nbins);
+    const double d = (emax - emin) / (double)nbins;
+    double a = emin - d;
+    for (int i = 0; i < nbins; i++) {
+        a += d;
+        E[i] = pow(10.0, a);
+    }
+    Scratch s;
+    double *d_crp, *d_n, *d_bp, *d_dp, *d_k, *d_E, *d_out;
+    CROMA_CUDA(s.get((void **)&d_crp, (size_t)ncell * NB * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_n, (size_t)ncell * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_bp, NB * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_dp, NB * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_k, (size_t)nbins * NB * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_E, (size_t)nbins * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_out, (size_t)ncell * nbins * sizeof(double)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    CROMA_CUDA(cudaMemcpy(d_crp, crp_batch, (size_t)ncell * NB * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_n, n_gas, (size_t)ncell * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_bp, beta_p, NB * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_dp, grid->dp, NB * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_k, kern, (size_t)nbins * NB * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_E, E.data(), (size_t)nbins * sizeof(double), cudaMemcpyHostToDevice));
+    dim3 blk(32, 4), grd((ncell + 31) / 32, (nbins + 3) / 4);
+    hadronic_emission_kernel<<<grd, blk>>>(ncell, nbins, d_crp, d_n, d_bp, d_dp, d_k, d_E, d_out);
+    CROMA_CUDA(cudaGetLastError());
+    CROMA_CUDA(cudaMemcpy(out, d_out, (size_t)ncell * nbins * sizeof(double), cudaMemcpyDeviceToHost));
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    if (elapsed_ms) *elapsed_ms = elapsed(e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int croma_b200_set_model(int dpp_model, int ttd_model, double t_acc_direct, double eta_cap)
+{
+    if (dpp_model < 1 || dpp_model > 4) return fail(-1, "unknown dpp model");
+    std::lock_guard<std::mutex> lk(g_mutex);
+    g_model.dpp_model = dpp_model;
+    g_model.ttd_model = ttd_model;
+    g_model.t_acc_direct = t_acc_direct;
+    g_model.eta_cap = eta_cap;
+    return 0;
+}
+
+int cuda_pipeline_is_available(void)
+{
+    int n = 0;
+    return (cudaGetDeviceCount(&n) == cudaSuccess && n > 0) ? 1 : 0;
+}
+
+int cuda_bind_local_rank(int local_rank, int *device_out)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return fail(-1, "no CUDA device available");
+    if (local_rank < 0) return fail(-1, "negative local rank");
+    const int dev = local_rank % n;
+    CROMA_CUDA(cudaSetDevice(dev));
+    if (device_out) *device_out = dev;
+    return 0;
+}
+
+int cuda_get_binding_state(int *device_count_out, int *current_device_out)
+{
+    int n = 0, cur = -1;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+    if (n > 0) cudaGetDevice(&cur);
+    if (device_count_out) *device_count_out = n;
+    if (current_device_out) *current_device_out = cur;
+    return n > 0 ? 0 : -1;
+}
+
+int cuda_get_current_device_id(char *out, int len)
+{
+    if (!out || len <= 0) return fail(-1, "invalid buffer");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return fail(-1, "no current device");
+    CROMA_CUDA(cudaDeviceGetPCIBusId(out, len, dev));
+    return 0;
+}
+
+int fp_cuda_tridiag_uses_pcr(int nrow)
+{
+    (void)nrow;
+    return 0;
+}
+
+const char *fp_cuda_tridiag_solver_name(int nrow)
+{
+    (void)nrow;
+    return "Thomas (warp-scan LU, factor once per segment)";
+}
+
+int solve_cc_cuda_batch(const FpChangCooperSolveBatchInput *in, const double *state_init,
+                        double *state_out, double *elapsed_ms, int *used_pcr_out)
+{
+    if (!in || !state_init || !state_out || in->nsys <= 0 || in->nrow <= 1 || !in->a_batch ||
+        !in->b_batch || !in->c_batch || !in->source_batch)
+        return fail(-1, "invalid solve_cc_cuda_batch arguments");
+    const size_t n = (size_t)in->nsys * in->nrow, bytes = n * sizeof(double);
+    Scratch s;
+    double *d[7];
+    for (int k = 0; k < 7; k++) CROMA_CUDA(s.get((void **)&d[k], bytes));
+    unsigned *d_err = nullptr;
+    CROMA_CUDA(s.get((void **)&d_err, sizeof(unsigned)));
+    CROMA_CUDA(cudaMemset(d_err, 0, sizeof(unsigned)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    const double *h[5] = {in->a_batch, in->b_batch, in->c_batch, in->source_batch, state_init};
+    for (int k = 0; k < 5; k++) CROMA_CUDA(cudaMemcpy(d[k], h[k], bytes, cudaMemcpyHostToDevice));
+    cc_thomas_kernel<<<(in->nsys + 127) / 128, 128>>>(in->nsys, in->nrow, in->dt, d[0], d[1], d[2], d[3],
+                                                      d[4], d[5], d[6], d_err);
+    CROMA_CUDA(cudaGetLastError());
+    CROMA_CUDA(cudaMemcpy(state_out, d[5], bytes, cudaMemcpyDeviceToHost));
+    unsigned err = 0;
+    CROMA_CUDA(cudaMemcpy(&err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    if (elapsed_ms) *elapsed_ms = elapsed(e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (used_pcr_out) *used_pcr_out = 0;
+    if (err) return fail(-2, "singular tridiagonal pivot in solve_cc_cuda_batch");
+    return 0;
+}
+
+FpCudaPipelineWorkspace *cuda_pipeline_workspace_create(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        set_error("no CUDA device available");
+        return nullptr;
+    }
+    auto *w = new (std::nothrow) FpCudaPipelineWorkspace();
+    if (!w) return nullptr;
+    Context &c = w->ctx;
+    cudaGetDevice(&c.device);
+    c.cfg.nb = NB;
+    c.cfg.species_mask = 3;
+    c.cfg.path = CROMA_PATH_FUSED;
+    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&c.d_err, sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(c.d_err, 0, sizeof(unsigned)) != cudaSuccess) {
+        set_error("workspace creation failed");
+        cuda_pipeline_workspace_destroy(w);
+        return nullptr;
+    }
+    return w;
+}
+
+void cuda_pipeline_workspace_destroy(FpCudaPipelineWorkspace *w)
+{
+    if (!w) return;
+    Context &c = w->ctx;
+    cudaSetDevice(c.device);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    cudaFree(w->b_bg); cudaFree(w->b_ric); cudaFree(w->b_crp); cudaFree(w->b_cre);
+    cudaFree(w->b_qpi); cudaFree(w->b_qepri); cudaFree(w->b_mass); cudaFree(w->b_dis); cudaFree(w->b_idx);
+    cudaFree(w->r_crp); cudaFree(w->r_cre); cudaFree(w->r_qpi); cudaFree(w->r_qepri);
+    cudaFree(c.d_inje);
+    cudaFree(c.d_tables);
+    cudaFree(c.d_np_min_qe);
+    cudaFree(c.d_err);
+    for (auto &t : c.timed) { cudaEventDestroy(t.start); cudaEventDestroy(t.stop); }
+    for (auto e : c.event_pool) cudaEventDestroy(e);
+    if (c.stream) cudaStreamDestroy(c.stream);
+    delete w;
+}
+
+int cuda_rank_state_upload(FpCudaPipelineWorkspace *w, int ncell, const double *qpi, const double *qepri,
+                           const double *crp, const double *cre, double *elapsed_ms)
+{
+    if (!w || ncell <= 0) return fail(-1, "invalid rank state upload");
+    Context &c = w->ctx;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    const size_t st = (size_t)ncell * NB * sizeof(double);
+    if (ncell > w->rcap) {
+        cudaFree(w->r_crp); cudaFree(w->r_cre); cudaFree(w->r_qpi); cudaFree(w->r_qepri);
+        CROMA_CUDA(cudaMalloc(&w->r_crp, st));
+        CROMA_CUDA(cudaMalloc(&w->r_cre, st));
+        CROMA_CUDA(cudaMalloc(&w->r_qpi, st));
+        CROMA_CUDA(cudaMalloc(&w->r_qepri, st));
+        w->rcap = ncell;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, c.stream);
+    const double *h[4] = {crp, cre, qpi, qepri};
+    double *d[4] = {w->r_crp, w->r_cre, w->r_qpi, w->r_qepri};
+    for (int k = 0; k < 4; k++) {
+        if (h[k]) CROMA_CUDA(cudaMemcpyAsync(d[k], h[k], st, cudaMemcpyHostToDevice, c.stream));
+        else CROMA_CUDA(cudaMemsetAsync(d[k], 0, st, c.stream));
+    }
+    cudaEventRecord(e1, c.stream);
+    CROMA_CUDA(cudaEventSynchronize(e1));
+    if (elapsed_ms) *elapsed_ms = elapsed(e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    w->r_n = ncell;
+    return 0;
+}
+
+int cuda_rank_state_download(FpCudaPipelineWorkspace *w, int ncell, double *crp, double *cre,
+                             double *elapsed_ms)
+{
+    if (!w || ncell <= 0 || ncell > w->r_n) return fail(-1, "invalid rank state download");
+    Context &c = w->ctx;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    const size_t st = (size_t)ncell * NB * sizeof(double);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, c.stream);
+    if (crp) CROMA_CUDA(cudaMemcpyAsync(crp, w->r_crp, st, cudaMemcpyDeviceToHost, c.stream));
+    if (cre) CROMA_CUDA(cudaMemcpyAsync(cre, w->r_cre, st, cudaMemcpyDeviceToHost, c.stream));
+    cudaEventRecord(e1, c.stream);
+    CROMA_CUDA(cudaEventSynchronize(e1));
+    if (elapsed_ms) *elapsed_ms = elapsed(e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return 0;
+}
+
+int run_tracer_pipeline(const FpCudaPipelineInput *in, const FpCudaOutputSchedule *schedule,
+                        double *crp_state_out, double *cre_state_out, double *eps_syn_out,
+                        double *eps_gamma_out, double *eps_nu_out, FpCudaPipelineTimes *times)
+{
+    (void)eps_syn_out;
+    (void)eps_gamma_out;
+    (void)eps_nu_out;
+    if (!in || !in->crp_grid || !in->cre_grid || !in->coeff_in || in->ncell <= 0 || in->nstep < 0)
+        return fail(-1, "invalid run_tracer_pipeline arguments");
+    if (schedule && (schedule->emit_all_steps || schedule->emit_final_only || schedule->nselected_steps > 0))
+        return fail(-1, "in-pipeline emission is not supported; use prepare_*_emission_cuda_batch");
+    FpCudaPipelineWorkspace *w = in->workspace;
+    if (!w) return fail(-1, "run_tracer_pipeline needs a workspace");
+    Context &c = w->ctx;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    const FpCoeffBatchInput *ci = in->coeff_in;
+    const int n = in->ncell;
+    cudaEvent_t e0, e1, e2, e3;
+    cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3);
+    cudaEventRecord(e0, c.stream);
+    int rc = ensure_tables(w, in->crp_grid, in->cre_grid);
+    if (!rc) rc = ensure_bucket(w, n);
+    if (rc) return rc;
+    fill_model(c.mp, in->psi_value, in->mach_limit_value);
+    c.cfg.species_mask = 3;
+
+    // ---- spectra and sources of the bucket ----
+    const size_t st = (size_t)n * NB * sizeof(double);
+    if (in->gather_rank_state) {
+        if (!in->rank_state_indices || !w->r_crp) return fail(-1, "rank state gather without state");
+        CROMA_CUDA(cudaMemcpyAsync(w->b_idx, in->rank_state_indices, n * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+        const int blocks = (int)(((size_t)n * NB + 255) / 256);
+        gather_rows_kernel<<<blocks, 256, 0, c.stream>>>(n, w->b_idx, w->r_crp, w->b_crp);
+        gather_rows_kernel<<<blocks, 256, 0, c.stream>>>(n, w->b_idx, w->r_cre, w->b_cre);
+        gather_rows_kernel<<<blocks, 256, 0, c.stream>>>(n, w->b_idx, w->r_qpi, w->b_qpi);
+        gather_rows_kernel<<<blocks, 256, 0, c.stream>>>(n, w->b_idx, w->r_qepri, w->b_qepri);
+        w->b_has_src = 1;
+        w->b_n = n;
+    } else if (in->crp_init || in->cre_init) {
+        if (in->crp_init) CROMA_CUDA(cudaMemcpyAsync(w->b_crp, in->crp_init, st, cudaMemcpyHostToDevice, c.stream));
+        else CROMA_CUDA(cudaMemsetAsync(w->b_crp, 0, st, c.stream));
+        if (in->cre_init) CROMA_CUDA(cudaMemcpyAsync(w->b_cre, in->cre_init, st, cudaMemcpyHostToDevice, c.stream));
+        else CROMA_CUDA(cudaMemsetAsync(w->b_cre, 0, st, c.stream));
+        if (in->qpi_batch) CROMA_CUDA(cudaMemcpyAsync(w->b_qpi, in->qpi_batch, st, cudaMemcpyHostToDevice, c.stream));
+        else CROMA_CUDA(cudaMemsetAsync(w->b_qpi, 0, st, c.stream));
+        if (in->qepri_batch) CROMA_CUDA(cudaMemcpyAsync(w->b_qepri, in->qepri_batch, st, cudaMemcpyHostToDevice, c.stream));
+        else CROMA_CUDA(cudaMemsetAsync(w->b_qepri, 0, st, c.stream));
+        w->b_has_src = (in->qpi_batch || in->qepri_batch) ? 1 : 0;
+        w->b_n = n;
+    } else if (w->b_n != n) {
+        return fail(-1, "no bucket state: pass crp_init/cre_init or gather the rank state");
+    }
+
+    // ---- background of the segment (device interpolation when requested) ----
+    const int interp = ci->device_interp_background ? 1 : 0;
+    {
+        const double *cur[8] = {ci->n_gas, ci->kbt, ci->b_field, ci->divv_gyr,
+                                ci->l_turb_mpc, ci->dv_imc, ci->cs, ci->beta_pl};
+        if (!ci->n_gas || !ci->kbt || !ci->b_field || !ci->divv_gyr || !ci->rad_ic_batch)
+            return fail(-1, "incomplete coefficient input");
+        if ((rc = upload_bg(w, cur, n, w->b_bg))) return rc;
+        CROMA_CUDA(cudaMemcpyAsync(w->b_ric, ci->rad_ic_batch, st, cudaMemcpyHostToDevice, c.stream));
+        if (interp) {
+            const double *nxt[8] = {ci->n_gas_next, ci->kbt_next, ci->b_field_next, ci->divv_gyr_next,
+                                    ci->l_turb_mpc_next, ci->dv_imc_next, ci->cs_next, ci->beta_pl_next};
+            if ((rc = upload_bg(w, nxt, n, w->b_bg + (size_t)kNbg * n))) return rc;
+            if (ci->rad_ic_batch_next)
+                CROMA_CUDA(cudaMemcpyAsync(w->b_ric + (size_t)NB * n, ci->rad_ic_batch_next, st,
+                                           cudaMemcpyHostToDevice, c.stream));
+            else
+                CROMA_CUDA(cudaMemcpyAsync(w->b_ric + (size_t)NB * n, w->b_ric, st, cudaMemcpyDeviceToDevice, c.stream));
+        }
+        if (ci->tracer_mass_msun)
+            CROMA_CUDA(cudaMemcpyAsync(w->b_mass, ci->tracer_mass_msun, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+        else
+            CROMA_CUDA(cudaMemsetAsync(w->b_mass, 0, n * sizeof(double), c.stream));
+        if (ci->disable_adiabatic)
+            CROMA_CUDA(cudaMemcpyAsync(w->b_dis, ci->disable_adiabatic, n, cudaMemcpyHostToDevice, c.stream));
+        else
+            CROMA_CUDA(cudaMemsetAsync(w->b_dis, 0, n, c.stream));
+    }
+    cudaEventRecord(e1, c.stream);
+
+    // ---- coefficients, secondary source and sub-steps ----
+    if (in->nstep > 0) {
+        SnapArgs a{};
+        a.ntracer = n;
+        a.bg_curr = w->b_bg;
+        a.bg_next = interp ? w->b_bg + (size_t)kNbg * n : w->b_bg;
+        a.ic_curr = w->b_ric;
+        a.ic_next = interp ? w->b_ric + (size_t)NB * n : w->b_ric;
+        a.allow_interp = interp;
+        a.dt_snap = in->dt * in->nstep;
+        a.elapsed = 0.0;
+        a.crp = w->b_crp;
+        a.cre = w->b_cre;
+        a.qpi = w->b_has_src ? w->b_qpi : nullptr;
+        a.qepri = w->b_has_src ? w->b_qepri : nullptr;
+        a.mass = w->b_mass;
+        a.dis = w->b_dis;
+        a.err = c.d_err;
+        SegInfo ex{};
+        ex.active = 1;
+        ex.nsub = in->nstep;
+        ex.nseg = interp ? 2 : 1;
+        ex.b = 0;
+        ex.e = in->nstep;
+        ex.steps = in->nstep;
+        ex.windowed = in->use_windowed_reacc ? 1 : 0;
+        ex.sl = in->on_start_step;
+        ex.el = in->on_end_step;
+        ex.alpha = interp ? ci->interp_alpha : 0.0;
+        ex.dt = in->dt;
+        if ((rc = run_fused_segment(c, a, ex, n))) return rc;
+    }
+    cudaEventRecord(e2, c.stream);
+
+    // ---- outputs ----
+    if (in->scatter_rank_state) {
+        if (!in->rank_state_indices || !w->r_crp) return fail(-1, "rank state scatter without state");
+        if (!in->gather_rank_state)
+            CROMA_CUDA(cudaMemcpyAsync(w->b_idx, in->rank_state_indices, n * sizeof(int), cudaMemcpyHostToDevice, c.stream));
+        const int blocks = (int)(((size_t)n * NB + 255) / 256);
+        scatter_rows_kernel<<<blocks, 256, 0, c.stream>>>(n, w->b_idx, w->b_crp, w->r_crp);
+        scatter_rows_kernel<<<blocks, 256, 0, c.stream>>>(n, w->b_idx, w->b_cre, w->r_cre);
+    }
+    double *crp_out = crp_state_out ? crp_state_out : in->crp_state_out;
+    double *cre_out = cre_state_out ? cre_state_out : in->cre_state_out;
+    if (crp_out) CROMA_CUDA(cudaMemcpyAsync(crp_out, w->b_crp, st, cudaMemcpyDeviceToHost, c.stream));
+    if (cre_out) CROMA_CUDA(cudaMemcpyAsync(cre_out, w->b_cre, st, cudaMemcpyDeviceToHost, c.stream));
+    cudaEventRecord(e3, c.stream);
+    CROMA_CUDA(cudaEventSynchronize(e3));
+    unsigned err = 0;
+    CROMA_CUDA(cudaMemcpy(&err, c.d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (times) {
+        memset(times, 0, sizeof(*times));
+        times->h2d_ms = elapsed(e0, e1);
+        times->solve_ms = elapsed(e1, e2);
+        times->d2h_ms = elapsed(e2, e3);
+        times->total_ms = elapsed(e0, e3);
+    }
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
+    if (err) {
+        cudaMemset(c.d_err, 0, sizeof(unsigned));
+        return fail(-2, "kernel reported a numerical failure (singular pivot or NaN CC row)");
+    }
+    return 0;
+}
+
+int run_pipeline_cuda(const FpCudaPipelineInput *in, const FpCudaOutputSchedule *schedule,
+                      double *crp_state_out, double *cre_state_out, double *eps_syn_out,
+                      double *eps_gamma_out, double *eps_nu_out, FpCudaPipelineTimes *times)
+{
+    return run_tracer_pipeline(in, schedule, crp_state_out, cre_state_out, eps_syn_out, eps_gamma_out,
+                               eps_nu_out, times);
+}
+
+int run_tracer_pipeline_group(const FpCudaPipelineInput *inputs, int ninput,
+                              const FpCudaOutputSchedule *schedule, FpCudaPipelineTimes *times)
+{
+    if (!inputs || ninput <= 0) return fail(-1, "invalid pipeline group");
+    FpCudaPipelineTimes acc{}, one{};
+    for (int i = 0; i < ninput; i++) {
+        int rc = run_tracer_pipeline(&inputs[i], schedule, inputs[i].crp_state_out, inputs[i].cre_state_out,
+                                     inputs[i].eps_syn_out, inputs[i].eps_gamma_out, inputs[i].eps_nu_out, &one);
+        if (rc) return rc;
+        acc.h2d_ms += one.h2d_ms;
+        acc.solve_ms += one.solve_ms;
+        acc.d2h_ms += one.d2h_ms;
+        acc.total_ms += one.total_ms;
+    }
+    if (times) *times = acc;
+    return 0;
+}
+
+int prepare_gamma_emission_cuda_batch(const FpGammaEmissionBatchInput *in, const CRspectrum *crp_grid,
+                                      double *eps_gamma_out, double *elapsed_ms)
+{
+    if (!in) return fail(-1, "null gamma input");
+    return emission_hadronic(in->ncell, in->nbins, in->egamma_min, in->egamma_max, in->crp_batch,
+                             in->n_gas, in->beta_p, in->fga_flat, crp_grid, eps_gamma_out, elapsed_ms);
+}
+
+int prepare_neutrino_emission_cuda_batch(const FpNeutrinoEmissionBatchInput *in, const CRspectrum *crp_grid,
+                                         double *eps_nu_out, double *elapsed_ms)
+{
+    if (!in) return fail(-1, "null neutrino input");
+    return emission_hadronic(in->ncell, in->nbins, in->enu_min, in->enu_max, in->crp_batch,
+                             in->n_gas, in->beta_p, in->fnu_flat, crp_grid, eps_nu_out, elapsed_ms);
+}
+
+int prepare_synch_emission_cuda_batch(const FpSynchEmissionBatchInput *in, const CRspectrum *cre_grid,
+                                      double *eps_syn_out, double *elapsed_ms)
+{
+    if (!in || !cre_grid || !eps_syn_out || in->ncell <= 0 || in->nfreq <= 0)
+        return fail(-1, "invalid synchrotron input");
+    if (!in->pitch_kernel_table || in->nlogb <= 1 || !(in->inv_dlogb > 0.0))
+        return fail(-1, "synchrotron emission needs the pitch-kernel table");
+    if (!in->b_dyn || !in->logb || !in->cre_batch) return fail(-1, "incomplete synchrotron input");
+    const int ncell = in->ncell, nfreq = in->nfreq, nlogb = in->nlogb;
+    Scratch s;
+    double *d_tab, *d_b, *d_lb, *d_cre, *d_dp, *d_out;
+    const size_t tab = (size_t)nlogb * nfreq * NB;
+    CROMA_CUDA(s.get((void **)&d_tab, tab * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_b, ncell * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_lb, ncell * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_cre, (size_t)ncell * NB * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_dp, NB * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_out, (size_t)ncell * nfreq * sizeof(double)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    CROMA_CUDA(cudaMemcpy(d_tab, in->pitch_kernel_table, tab * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_b, in->b_dyn, ncell * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_lb, in->logb, ncell * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_cre, in->cre_batch, (size_t)ncell * NB * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_dp, cre_grid->dp, NB * sizeof(double), cudaMemcpyHostToDevice));
+    const double a0 = sqrt(3.0) * pow(4.8e-10, 3.0);
+    const double den1 = 2.0 * 9.11e-28 * kC * kC, den2 = 4.0 * kPi;
+    dim3 blk(32, 4), grd((ncell + 31) / 32, (nfreq + 3) / 4);
+    synch_table_kernel<<<grd, blk>>>(ncell, nfreq, nlogb, in->logb_min, in->inv_dlogb, a0, den1, den2,
+                                     d_tab, d_b, d_lb, d_cre, d_dp, d_out);
+    CROMA_CUDA(cudaGetLastError());
+    CROMA_CUDA(cudaMemcpy(eps_syn_out, d_out, (size_t)ncell * nfreq * sizeof(double), cudaMemcpyDeviceToHost));
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    if (elapsed_ms) *elapsed_ms = elapsed(e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return 0;
+}
+
+}  // extern "C"

@@ -123,14 +123,16 @@ int build_tables(Context &ctx)
 {
     const CromaB200Config &c = ctx.cfg;
     const int n = NB;
-    // ---- momentum grids: momentum_bin, FP_Coef.c:291-330 ----
-    for (int s = 0; s < 2; s++) {
-        ctx.h_p[s].assign(n, 0.0);
-        ctx.h_dp[s].assign(n, 0.0);
-        ctx.h_E[s].assign(n, 0.0);
-    }
     std::vector<double> beta_p(n);
-    {
+    if (ctx.grid_given) {
+        for (int j = 0; j < n; j++) beta_p[j] = ctx.h_p[0][j] / sqrt(1.0 + ctx.h_p[0][j] * ctx.h_p[0][j]);
+    } else {
+        // ---- momentum grids: momentum_bin, FP_Coef.c:291-330 ----
+        for (int s = 0; s < 2; s++) {
+            ctx.h_p[s].assign(n, 0.0);
+            ctx.h_dp[s].assign(n, 0.0);
+            ctx.h_E[s].assign(n, 0.0);
+        }
         double da = (c.pmax - c.pmin) / (double)n, a = c.pmin - da;
         ctx.h_pm1[0] = pow(10.0, a);
         for (int j = 0; j < n; j++) {
@@ -220,6 +222,10 @@ int build_tables(Context &ctx)
     }
 
     // ---- device allocation ----
+    if (ctx.d_tables) cudaFree(ctx.d_tables);
+    if (ctx.d_np_min_qe) cudaFree(ctx.d_np_min_qe);
+    ctx.d_tables = nullptr;
+    ctx.d_np_min_qe = nullptr;
     CROMA_CUDA(cudaMalloc(&ctx.d_tables, tab_doubles * sizeof(double)));
     double *d = ctx.d_tables;
     auto darr = [&](int k) { return d + (size_t)k * n; };
