@@ -252,6 +252,24 @@ int solve_cc_cuda_batch(const FpChangCooperSolveBatchInput *in,             /* :
                         double *elapsed_ms,
                         int *used_pcr_out);
 
+/* No counterpart in the reference.  The same implicit Chang-Cooper step as
+ * solve_cc_cuda_batch for callers that must not allocate device memory (a
+ * host whose device memory already belongs to its own pool allocator, or a
+ * time step that cannot afford cudaMalloc/cudaFree synchronising the device):
+ * every pointer is a device pointer owned by the caller, layout
+ * [nsys][nrow] as in FpChangCooperSolveBatchInput, stream is a cudaStream_t
+ * (0 for the default stream).  The only scratch is a fixed array inside the
+ * library, so nsys * nrow may not exceed 524288 (larger batches return -1);
+ * every GPU that loads the library keeps that 4 MiB array until exit.  All
+ * calls on a device share it: calls that overlap on the GPU race and must be
+ * serialised.  The first call on a device looks the array up and should come
+ * before any stream capture.  The call waits for its stream and returns -2
+ * on a singular pivot. */
+int solve_cc_cuda_batch_noalloc(int nsys, int nrow, double dt,
+                                const double *a, const double *b, const double *c,
+                                const double *source, const double *state_in,
+                                double *state_out, void *stream);
+
 int fp_cuda_tridiag_uses_pcr(int nrow);                                      /* :118 */
 const char *fp_cuda_tridiag_solver_name(int nrow);                           /* :119 */
 
