@@ -36,6 +36,10 @@ NSNAP_TIMELINE = 100
 SEED = 20261203
 METRIC = "tracer-snapshot updates/s at <=1e-6 rel err vs FP64, chosen vs plain; p50/p99 latency"
 UNIT = "tracer-snapshot updates/s"
+# DRAM bytes (read + write) of one fused slot (proton + electron launches) per
+# tracer, from an ncu capture of this workload at 65,536 tracers
+# (profiles/fused_slot_kernel_batching_e_p_256.txt).
+NCU_DRAM_BYTES_PER_TRACER_SLOT = (143.05e6 + 83.32e6 + 278.07e6 + 103.90e6) / 65536
 
 
 def load_package():
@@ -312,8 +316,33 @@ def run_gpu_arm(args):
                     "alg_bytes_per_launch": per_launch,
                     "alg_bytes_rule": "per tracer-snapshot: nsub x 2 species x nb x 6 doubles"}
     else:
-        roofline = {"bound": "hbm", "achieved": None, "peak": None, "unit": "GB/s", "frac": None,
-                    "traffic": None}
+        # The fused evolve keeps every row on chip, so its DRAM traffic is only the
+        # compulsory state, source and background; the bound is the FP64 pipe.
+        # Algorithmic flops are the reference's Thomas step per row per sub-step
+        # (RHS FMA, denominator FMA, back-substitution FMA, 2 divides: 9 flops +
+        # 2 divides, counted 11), summed over both species and every sub-step of
+        # the schedule.  Per-segment coefficient work is not counted.
+        flops_per_snapshot = float(np.sum(nsub)) * nspecies * nb * 11.0
+        per_launch = flops_per_snapshot * args.steps / max(1, evolve_n)
+        avg_launch_ms = evolve_ms / max(1, evolve_n)
+        achieved = per_launch / (avg_launch_ms / 1e3) / 1e12
+        peak = native.fp64_peak(cfg.nb)
+        # compulsory bytes of one slot launch pair: both species' N read and
+        # written, the electron source row read, both backgrounds read
+        comp_bytes = nt * (nspecies * nb * 16 + nb * 8 + 2 * 8 * 8)
+        traffic = NCU_DRAM_BYTES_PER_TRACER_SLOT * nt if args.tracers == NTRACER else None
+        roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": traffic,
+                    "peak_source": "measured live: croma_b200_fp64_peak (FMA chains on every SM)",
+                    "kernel": "fused_slot_kernel (proton + electron launches of one slot)",
+                    "launches": evolve_n, "kernel_ms_total": evolve_ms,
+                    "share_of_step": evolve_ms / ms if ms > 0 else None,
+                    "alg_flops_per_launch": per_launch,
+                    "alg_flops_rule": "per tracer-snapshot: nsub x 2 species x nb x 11 (reference Thomas)",
+                    "hbm_view": {"compulsory_bytes_per_launch": comp_bytes,
+                                 "achieved_gbs": comp_bytes / (avg_launch_ms / 1e3) / 1e9,
+                                 "peak_gbs": float(peaks.get("hbm_gbs", 6650.0)),
+                                 "peak_source": peak_kind}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -60,8 +60,8 @@ void free_state(Context &c)
     cudaFree(c.d_mass); cudaFree(c.d_dis); cudaFree(c.d_bg); cudaFree(c.d_layout_tmp);
     c.d_crp = c.d_cre = c.d_qpi = c.d_qepri = c.d_mass = c.d_bg = c.d_layout_tmp = nullptr;
     c.d_dis = nullptr;
-    cudaFree(c.d_coef); cudaFree(c.d_inje); cudaFree(c.d_seg_ngas);
-    c.d_coef = c.d_inje = c.d_seg_ngas = nullptr;
+    cudaFree(c.d_coef); cudaFree(c.d_inje); cudaFree(c.d_seg_ngas); cudaFree(c.d_eta_scale);
+    c.d_coef = c.d_inje = c.d_seg_ngas = c.d_eta_scale = nullptr;
     cudaFree(c.d_sched_int); cudaFree(c.d_capped); cudaFree(c.d_cub_tmp);
     cudaFree(c.d_keys); cudaFree(c.d_vals);
     c.d_sched_int = nullptr; c.d_capped = nullptr; c.d_cub_tmp = nullptr;
@@ -424,6 +424,57 @@ int croma_b200_reset_kernel_stats(CromaB200Context *h)
     double ms;
     croma_b200_kernel_stats(h, 0, &ms, nullptr);
     for (int k = 0; k < 4; k++) { c.kernel_ms[k] = 0.0; c.kernel_launches[k] = 0; }
+    return 0;
+}
+
+}  // extern "C"
+
+namespace croma_probe {
+// 8 independent FMA chains per thread; the result is written so the work is kept.
+__global__ void fp64_fma_probe(int iters, double seed, double *out)
+{
+    double x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = seed + threadIdx.x * 1e-9 + k * 1e-7;
+    const double m = 0.999999999, a = 1e-12;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) x[k] = fma(x[k], m, a);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += x[k];
+    if (s == 12345.678) out[blockIdx.x] = s;
+}
+}  // namespace croma_probe
+
+extern "C" {
+
+int croma_b200_fp64_peak(double *tflops)
+{
+    if (!tflops) { set_error("null argument"); return -1; }
+    int dev = 0, nsm = 0;
+    CROMA_CUDA(cudaGetDevice(&dev));
+    CROMA_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    double *out = nullptr;
+    CROMA_CUDA(cudaMalloc(&out, (size_t)nsm * 16 * sizeof(double)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = nsm * 16, threads = 256, iters = 4096;
+    croma_probe::fp64_fma_probe<<<blocks, threads>>>(64, 1.0, out);   // warm-up
+    cudaEventRecord(e0);
+    croma_probe::fp64_fma_probe<<<blocks, threads>>>(iters, 1.0, out);
+    cudaEventRecord(e1);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (e != cudaSuccess) return cuda_fail(e, "fp64 probe");
+    const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
+    *tflops = flops / (ms * 1e-3) / 1e12;
     return 0;
 }
 

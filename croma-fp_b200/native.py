@@ -70,12 +70,22 @@ def load_library(nb: int) -> C.CDLL:
     L.croma_b200_set_kernel_timing.argtypes = [_vp, _i]
     L.croma_b200_kernel_stats.argtypes = [_vp, _i, P(_d), P(C.c_longlong)]
     L.croma_b200_reset_kernel_stats.argtypes = [_vp]
+    L.croma_b200_fp64_peak.argtypes = [P(_d)]
     _LIBS[nb] = L
     return L
 
 
 class CromaError(RuntimeError):
     pass
+
+
+def fp64_peak(nb: int = 256) -> float:
+    """FP64 FMA throughput of the current device in TFLOP/s (measured live)."""
+    L = load_library(nb)
+    t = _d()
+    if L.croma_b200_fp64_peak(C.byref(t)) != 0:
+        raise CromaError(L.croma_b200_last_error().decode())
+    return t.value
 
 
 def _p(a):

@@ -131,6 +131,11 @@ int croma_b200_set_kernel_timing(CromaB200Context *ctx, int enable);
 int croma_b200_kernel_stats(CromaB200Context *ctx, int kind, double *total_ms, long long *launches);
 int croma_b200_reset_kernel_stats(CromaB200Context *ctx);
 
+/* FP64 FMA throughput of the current device, measured by a kernel of
+ * independent fused multiply-add chains on every SM (TFLOP/s, FMA = 2 flops);
+ * the denominator of the fused evolve's roofline. */
+int croma_b200_fp64_peak(double *tflops);
+
 #ifdef __cplusplus
 }
 #endif
