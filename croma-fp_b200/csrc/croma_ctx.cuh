@@ -109,6 +109,7 @@ struct Context {
     double *d_coef = nullptr;         // [2 sets][2 species][3][nb][cap]
     double *d_inje = nullptr;         // [nb][cap]
     double *d_seg_ngas = nullptr;     // [cap]
+    double *d_eta_scale = nullptr;    // [cap] Dpp eta-cap scale of the current slot
     double *d_layout_tmp = nullptr;   // [nb][cap] transpose staging
 
     unsigned *d_err = nullptr;

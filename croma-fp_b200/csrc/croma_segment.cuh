@@ -101,6 +101,31 @@ __device__ inline DppForm dpp_form(const ModelParams &mp, int model, const Bg &b
 
 // fp_apply_eta_dpp_cap_cell (fp_shared_core.c:1032-1081): the factor by
 // which the "on" Dpp is scaled (1 when the cap does not act).
+// The cap from a given CR energy sum ecr (erg): the tail of the routine below.
+__device__ inline double eta_cap_scale_from_ecr(const ModelParams &mp, const Bg &bg, double mass,
+                                                double tacc_direct, double ecr)
+{
+    if (!(mp.eta_dpp_cap > 0.0) || !isfinite(mp.eta_dpp_cap)) return 1.0;
+    if (!(mass > 0.0) || !(bg.lturb > 0.0) || !(bg.dv > 0.0)) return 1.0;
+    double tacc = 0.0;
+    if (bg.lturb > 0.0 && bg.cs > 0.0) {
+        double mach = bg.dv / bg.cs;
+        if (mach < 0.0) mach = 0.0;
+        if (mp.mach_limit > 0.0 && mach > mp.mach_limit) mach = mp.mach_limit;
+        if (mach > 0.0) {
+            if (mp.dpp_model == kDppAsa) tacc = (bg.beta > 0.0) ? tacc_asa(mp.psi3, bg.lturb * kMpc, bg.cs, mach, bg.beta) : 0.0;
+            else if (mp.dpp_model == kDppTtd) tacc = tacc_ttd(mp.ttd_brunetti16, bg.lturb * kMpc, bg.cs, mach, bg.dv);
+            else if (mp.dpp_model == kDppDirect) tacc = (tacc_direct > 0.0 && isfinite(tacc_direct)) ? tacc_direct : 0.0;
+        }
+    }
+    if (!(tacc > 0.0) || !isfinite(tacc)) return 1.0;
+    const double qturb = 0.5 * mass * kMsun * bg.dv * bg.dv * bg.dv / (bg.lturb * kMpc);
+    if (!(ecr > 0.0) || !(qturb > 0.0) || !isfinite(ecr) || !isfinite(qturb)) return 1.0;
+    const double eta = ecr / (qturb * tacc * kGyr);
+    if (!(eta > mp.eta_dpp_cap) || !isfinite(eta)) return 1.0;
+    return mp.eta_dpp_cap / eta;
+}
+
 __device__ inline double eta_cap_scale(const ModelParams &mp, const GridTables &gt, const Bg &bg,
                                 double mass, double tacc_direct, const double *crp,
                                 const double *cre, size_t stride)

@@ -43,6 +43,7 @@ struct FusedParams {
     ModelParams mp;
     int slot;
     const double *inje;      // [tracer][nb] electron source of the slot, or null
+    const double *eta_scale; // [tracer] Dpp eta-cap scale of the slot, or null (no cap)
     const int *np_min_qe;    // [nb]
     // One caller-defined segment shared by every tracer (run_tracer_pipeline):
     // when set, ex replaces the per-tracer schedule.
@@ -400,10 +401,7 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) fused_slot_k
     }
 
     const DppForm on = dpp_form(P.mp, P.mp.dpp_model, bg, tacc);
-    const double on_scale = (P.mp.dpp_model != kDppOff)
-        ? eta_cap_scale(P.mp, P.gt, bg, a.mass ? a.mass[t] : 0.0, tacc, a.crp + (size_t)t * NB,
-                        a.cre + (size_t)t * NB, 1)
-        : 1.0;
+    const double on_scale = (P.mp.dpp_model != kDppOff && P.eta_scale) ? P.eta_scale[t] : 1.0;
 
     Factor<SRC> F;
     int cur = -1;
@@ -424,6 +422,35 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) fused_slot_k
 #pragma unroll
     for (int r = 0; r < kR; r += 2)
         *reinterpret_cast<double2 *>(Nrow + r) = make_double2(N[r], N[r + 1]);
+}
+
+// Dpp eta-cap scale of every tracer with a segment in this slot, from the
+// spectra at the start of the segment (prepare_momentumdiff_cell_major,
+// src/fp_shared_core.c:1032-1081, runs before either species evolves), one
+// warp per tracer.  The energy sum is split over the lanes and combined by a
+// shuffle tree, so it agrees with the reference's sequential sum to rounding.
+__global__ void __launch_bounds__(128) eta_scale_kernel(FusedParams P, double *eta)
+{
+    const int lane = threadIdx.x & 31;
+    const int t = blockIdx.x * 4 + (threadIdx.x >> 5);
+    const SnapArgs &a = P.a;
+    if (t >= a.ntracer) return;
+    const SegInfo g = segment_of(P, t);
+    if (!g.active) return;
+    const Bg bg = load_bg(a, t, g);
+    const double tacc_direct = segment_tacc(P.mp, a, g);
+    const double mass = a.mass ? a.mass[t] : 0.0;
+    const double *crp = a.crp + (size_t)t * NB, *cre = a.cre + (size_t)t * NB;
+    double ecr = 0.0;
+    for (int j = 2 + lane; j < NB - 2; j += 32) {
+        const double ekp = P.gt.s[0].E[j] - kMp, vp = crp[j];
+        if (ekp > 0.0 && isfinite(vp)) ecr += ekp * kGeV * vp * P.gt.s[0].dp[j];
+        const double eke = P.gt.s[1].E[j] - kMe, ve = cre[j];
+        if (eke > 0.0 && isfinite(ve)) ecr += eke * kGeV * ve * P.gt.s[1].dp[j];
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) ecr += __shfl_xor_sync(kFull, ecr, off);
+    if (lane == 0) eta[t] = eta_cap_scale_from_ecr(P.mp, bg, mass, tacc_direct, ecr);
 }
 
 // Secondary source of the slot, cell-major:
@@ -513,8 +540,10 @@ cudaError_t launch_slot(Context &ctx, const FusedParams &P, bool src)
 int fused_reserve(Context &ctx, int cap)
 {
     cudaFree(ctx.d_inje);
-    ctx.d_inje = nullptr;
+    cudaFree(ctx.d_eta_scale);
+    ctx.d_inje = ctx.d_eta_scale = nullptr;
     CROMA_CUDA(cudaMalloc(&ctx.d_inje, (size_t)NB * cap * sizeof(double)));
+    CROMA_CUDA(cudaMalloc(&ctx.d_eta_scale, (size_t)cap * sizeof(double)));
     return 0;
 }
 
@@ -527,6 +556,14 @@ static int fused_one_slot(Context &ctx, FusedParams &P)
     const int electrons = ctx.mp.species_mask & CROMA_SPECIES_ELECTRON;
     cudaEvent_t ev = nullptr;
     P.inje = nullptr;
+    P.eta_scale = nullptr;
+    if (ctx.mp.eta_dpp_cap > 0.0 && isfinite(ctx.mp.eta_dpp_cap) && ctx.mp.dpp_model != kDppOff) {
+        timed_begin(ctx, kKindCoeff, &ev);
+        eta_scale_kernel<<<(a.ntracer + 3) / 4, 128, 0, ctx.stream>>>(P, ctx.d_eta_scale);
+        timed_end(ctx, kKindCoeff, ev);
+        ctx.last_launches += 1;
+        P.eta_scale = ctx.d_eta_scale;
+    }
     if (protons && electrons) {
         dim3 sg((a.ntracer + 63) / 64, (NB + 63) / 64), sb(16, 16);
         timed_begin(ctx, kKindSecondary, &ev);

@@ -461,6 +461,7 @@ void cuda_pipeline_workspace_destroy(FpCudaPipelineWorkspace *w)
     cudaFree(w->b_qpi); cudaFree(w->b_qepri); cudaFree(w->b_mass); cudaFree(w->b_dis); cudaFree(w->b_idx);
     cudaFree(w->r_crp); cudaFree(w->r_cre); cudaFree(w->r_qpi); cudaFree(w->r_qepri);
     cudaFree(c.d_inje);
+    cudaFree(c.d_eta_scale);
     cudaFree(c.d_tables);
     cudaFree(c.d_np_min_qe);
     cudaFree(c.d_err);

@@ -45,6 +45,8 @@ CASES = {
     "c1_narrow_window": (("config1", dict(nb=128, pmin=0.0, pmax=3.0, pemin=1.0, pemax=3.0,
                                           reacc_window_mode=1, f_eddy=0.002)), 32, 50, 2, 110, 100),
     "c4_asa512": (("config4", dict()), 3, 60, 1, 108, 100),
+    # eta cap binding for most tracers, with protons and electrons evolving
+    "c1_etacap": (("config1", dict(nb=128, eta_dpp_cap=1.0)), 8, 30, 2, 111, 100),
 }
 
 
