@@ -86,6 +86,11 @@ struct Context {
     double ic_z[2] = {0, 0};
     int ic_valid[2] = {0, 0};
     int ic_slot_curr = 0;
+    // pinned staging of the IC outer abscissae: two slots, each reused only
+    // after the copy that last read it has completed (its event)
+    double *h_ic_stage = nullptr;
+    cudaEvent_t ic_stage_ev[2] = {nullptr, nullptr};
+    int ic_stage_next = 0;
 
     // resident state (momentum-major [nb][cap])
     int cap = 0, ntracer = 0;
@@ -110,6 +115,13 @@ struct Context {
     double *d_inje = nullptr;         // [nb][cap]
     double *d_seg_ngas = nullptr;     // [cap]
     double *d_eta_scale = nullptr;    // [cap] Dpp eta-cap scale of the current slot
+
+    // fused-path workspace, per tracer chunk: factored matrices of every
+    // segment [2 species][nseg][sets][chunk][3][nb], proton spectra at the
+    // segment starts and the electron source per segment [nseg][chunk][nb]
+    double *d_fac = nullptr;
+    double *d_np_seg = nullptr;
+    int fused_chunk = 0, fused_nseg = 0, fused_sets = 0;
     double *d_layout_tmp = nullptr;   // [nb][cap] transpose staging
 
     unsigned *d_err = nullptr;
@@ -142,6 +154,7 @@ int cuda_fail(cudaError_t e, const char *what);
 
 // tables.cu
 int build_tables(Context &ctx);
+void free_ic_stage(Context &ctx);
 int ic_rows(Context &ctx, double z, double *d_out);
 // schedule.cu
 int schedule_reserve(Context &ctx, int cap);

@@ -1,31 +1,39 @@
-// fused.cu -- the fused FP64 evolve: one warp per (tracer, species)
-// system, the spectrum held in registers across a coefficient segment.
+// fused.cu -- the on-chip FP64 evolve: the segment matrices of a tracer
+// chunk are built and factored by one kernel, and a second kernel runs every
+// sub-step of every segment with the spectrum held in registers.
 //
-// Per segment slot and system the warp
-//   1. evaluates the loss / diffusion terms of every bin and the Chang-Cooper
-//      face weights in rolled, lane-strided loops into the warp's slice of
-//      shared memory (losses / Dpp / CC assembly of
-//      src/fp_shared_core.c:729-842, 1241-1317, 2358-2431 and
-//      src/Chang_Cooper.c:22-184);
-//   2. assembles its rows a, b, c in registers -- lane l owns rows
-//      [l*R, (l+1)*R), R = nb/32 -- and factors the tridiagonal matrix once,
-//      since it is constant over the segment's sub-steps: the Thomas pivots
-//      d_i = b_i - a_i c_{i-1}/d_{i-1} are a chain of Moebius maps, composed
-//      per lane as 2x2 matrices and combined across lanes by a warp scan; each
-//      lane then re-runs the exact recurrence on its rows from the scanned
-//      incoming pivot;
-//   3. runs every sub-step as the two first-order linear recurrences of
-//      fp_thomas_solve_ws (src/fp_shared_core.c:226-257), each an affine warp
-//      scan: a local pass per lane, five shuffle levels, a second local pass.
+// Per chunk of tracers (sized to the workspace budget) and species:
+//   1. factor_kernel, one warp per (segment, tracer[, on/off set]): the loss /
+//      diffusion terms of every bin and the Chang-Cooper face weights in
+//      rolled lane-strided loops into the warp's slice of shared memory
+//      (losses / Dpp / CC assembly of src/fp_shared_core.c:729-842,
+//      1241-1317, 2358-2431 and src/Chang_Cooper.c:22-184); rows a, b, c in
+//      registers -- lane l owns rows [l*R, (l+1)*R), R = nb/32 -- and the
+//      Thomas pivots d_i = b_i - a_i c_{i-1}/d_{i-1}, a chain of Moebius maps
+//      composed per lane as 2x2 matrices and combined by a warp scan, after
+//      which each lane re-runs the exact recurrence on its rows from the
+//      scanned incoming pivot.  It stores 1/d, a/d and c/d per row.
+//      Nothing here depends on the evolving spectra (the eta cap aside, which
+//      then runs the chunk one segment at a time), so every segment of the
+//      snapshot is factored by one launch with full occupancy.
+//   2. steps_kernel, one warp per tracer: for each segment it loads the
+//      factored rows (and the segment's source), and runs each sub-step as
+//      the two first-order linear recurrences of fp_thomas_solve_ws
+//      (src/fp_shared_core.c:226-257), each an affine warp scan: a local pass
+//      per lane, five shuffle levels, a second local pass.  The proton kernel
+//      records the spectrum at each segment start for the secondaries.
+//   3. secondary_kernel: the electron source of every segment from those
+//      proton spectra (prepare_secondary_sources_cell_major,
+//      src/fp_shared_core.c:1591-1672), a tiled [segments*tracers x nb] .
+//      [nb x nb] product, between the proton and the electron steps.
 //
 // Shared-memory rows are stored at (m % R) * 33 + m / R, so the blocked reads
-// of step 2 (lane l, row l*R + r and its neighbours) hit 32 distinct banks.
+// of step 1 (lane l, row l*R + r and its neighbours) hit 32 distinct banks.
 // Divisions by grid quantities use reciprocals tabulated on the host; the
 // results agree with the reference's divisions to an ulp per operation.
-// The secondary-electron source of each segment (a dense [tracers x nb] .
-// [nb x nb] product, prepare_secondary_sources_cell_major,
-// src/fp_shared_core.c:1591-1672) runs as a tiled kernel before the slot.
 // Spectra are cell-major [tracer][nb] so that a warp's rows are contiguous.
+#include <cstdlib>
+
 #include "croma_segment.cuh"
 
 namespace croma {
@@ -34,17 +42,23 @@ namespace {
 
 constexpr int kR = NB / 32;          // rows per lane
 constexpr int kSw = 33 * kR;         // swizzled row-array length
-constexpr int kWarps = 4;            // warps (systems) per block
+constexpr int kWarps = 4;            // warps per block
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kFacDoubles = 3 * NB;  // 1/d, a/d, c/d of one system
+constexpr int kFacWarps = 8;         // warps per factor-kernel block
+
+// Grid tables of one species staged in shared memory by the factor kernel.
+// X0..X4: protons expE, cp_Ep, cp_inv2mpkin, cp_inv_betap2, sig_eff;
+// electrons ce_inv_beta2, ce_logp and the shared IC rows of z_curr, z_next.
+enum { TB_P, TB_P2, TB_CUT, TB_2P, TB_DXF, TB_X0, TB_X1, TB_X2, TB_X3, TB_X4, kTab };
 
 struct FusedParams {
     SnapArgs a;              // spectra and sources cell-major [tracer][nb]
     GridTables gt;
     ModelParams mp;
-    int slot;
-    const double *inje;      // [tracer][nb] electron source of the slot, or null
-    const double *eta_scale; // [tracer] Dpp eta-cap scale of the slot, or null (no cap)
-    const int *np_min_qe;    // [nb]
+    int g0, g1;              // segment slots of this launch
+    int t0, nt;              // tracer chunk [t0, t0 + nt)
+    int sets;                // factor sets per segment: 1 (on) or 2 (on, off)
     // One caller-defined segment shared by every tracer (run_tracer_pipeline):
     // when set, ex replaces the per-tracer schedule.
     int explicit_seg;
@@ -52,11 +66,30 @@ struct FusedParams {
     // IC rows: shared row (stride 0) or per tracer, momentum-major
     // [nb][ntracer] (stride = ntracer)
     int ic_stride;
+    const double *eta_scale; // [ntracer] Dpp eta-cap scale of slot g0, or null (no cap)
+    double *fac;             // [2 species][g1 - g0][sets][nt][3][nb]
+    double *np_seg;          // [g1 - g0][nt][nb] proton spectra at segment starts, or null
+    double *inje;            // [g1 - g0][nt][nb] electron source per segment, or null
+    const int *np_min_qe;    // [nb]
 };
 
-__device__ __forceinline__ SegInfo segment_of(const FusedParams &P, int t)
+__device__ __forceinline__ SegInfo segment_of(const FusedParams &P, int t, int slot)
 {
-    return P.explicit_seg ? P.ex : seg_info(P.a.sched, t, P.slot, P.a.dt_snap);
+    return P.explicit_seg ? P.ex : seg_info(P.a.sched, t, slot, P.a.dt_snap);
+}
+
+__device__ __forceinline__ double *fac_ptr(const FusedParams &P, int S, int gi, int set, int tl)
+{
+    return P.fac + ((((size_t)S * (P.g1 - P.g0) + gi) * P.sets + set) * P.nt + tl) * kFacDoubles;
+}
+
+// Which factor sets a segment needs: 0 = Dpp on, 1 = off (windowed segments).
+// The window is clamped to the segment's sub-steps as the steps kernel runs it.
+__device__ __forceinline__ bool needs_set(const SegInfo &g, int set)
+{
+    if (!g.windowed) return set == 0;
+    const int sl = min(max(g.sl, 0), g.steps), el = min(max(g.el, sl), g.steps);
+    return (set == 0) ? el > sl : (sl > 0 || el < g.steps);
 }
 
 __device__ __forceinline__ int swz(int m) { return (m % kR) * 33 + m / kR; }
@@ -78,47 +111,57 @@ __device__ __forceinline__ void rescale2(double &m00, double &m01, double &m10, 
 template <int S>
 struct SegTerms {
     const GridTables *gt;
-    double n_gas, kbt, inv_kbt, inv_n, adiab;
+    double n_gas, kbt, inv_kbt, log_n, adiab;
     double synch_coeff, coulomb_coeff;
     double dt, dt_over_tloss_pref;   // protons: dt / T = sig_eff * dt_over_tloss_pref
     double dtT_e;                    // electrons: dt / 1e100
     double dpp_inv, dpp_scale;
     int dpp_fill;
     const double *ric, *ric_next;   // already offset to this tracer
-    int ric_stride;                 // bin stride of the IC row
+    int ric_stride;                 // bin stride of the IC row; 0: the shared row, staged
     double alpha;
     int interp;
 
-    // B = radp - 2 Dpp / p, C = Dpp, dT = dt / tloss at bin j
-    __device__ __forceinline__ void at(int j, double &B, double &C, double &dT) const
+    // B = radp - 2 Dpp / p, C = Dpp, dT = dt / tloss at bin j, from the grid
+    // tables staged in shared memory (tab, kTab arrays of nb)
+    __device__ __forceinline__ void at(const double *tab, int j, double &B, double &C, double &dT) const
     {
-        const SpeciesTables &st = gt->s[S];
-        const double p = st.p[j];
-        const double p2 = st.p2[j];
+        const double p = tab[TB_P * NB + j];
+        const double p2 = tab[TB_P2 * NB + j];
+        const double cut = tab[TB_CUT * NB + j];
         double D;
         if (!dpp_fill) D = p2 * (1.0 / (4.0 * 1.0e+5));
-        else if (S == 0) D = p2 * dpp_inv * st.expE[j] * st.exp_cut[j];
-        else D = p2 * dpp_inv * st.exp_cut[j];
+        else if (S == 0) D = p2 * dpp_inv * tab[TB_X0 * NB + j] * cut;
+        else D = p2 * dpp_inv * cut;
         D *= dpp_scale;
         double radp;
         if (S == 0) {
-            const double xp = gt->cp_Ep[j] * inv_kbt;
+            const double xp = tab[TB_X1 * NB + j] * inv_kbt;
             const double xe = xp * (kMe / kMp);
             const double sum = coulomb_kernel_fast(xe) + coulomb_kernel_fast(xp) * (kMe / kMp);
-            const double thermal = 1.0 - kbt * gt->cp_inv2mpkin[j];
+            const double thermal = 1.0 - kbt * tab[TB_X2 * NB + j];
             const double coul = (thermal < 0.0)
                 ? 0.0
-                : kGyr * kC / (kMp * kGeV) * sum * n_gas * gt->cp_inv_betap2[j] * thermal * 3.5e-29;
+                : kGyr * kC / (kMp * kGeV) * sum * n_gas * tab[TB_X3 * NB + j] * thermal * 3.5e-29;
             radp = coul + adiab * p;
-            dT = gt->sig_eff[j] * dt_over_tloss_pref;
+            dT = tab[TB_X4 * NB + j] * dt_over_tloss_pref;
         } else {
-            const double r0 = ric[j * ric_stride];
-            const double r = interp ? lerp(r0, ric_next[j * ric_stride], alpha) : r0;
-            const double coulomb = coulomb_coeff * (1.0 + log(p * inv_n) * (1.0 / 74.8)) * gt->ce_inv_beta2[j];
+            double r0, r1;
+            if (ric_stride == 0) {
+                r0 = tab[TB_X2 * NB + j];
+                r1 = tab[TB_X3 * NB + j];
+            } else {
+                r0 = ric[j * ric_stride];
+                r1 = ric_next[j * ric_stride];
+            }
+            const double r = interp ? lerp(r0, r1, alpha) : r0;
+            // log(p / n) as log p - log n: the per-bin logarithm is tabulated
+            const double coulomb = coulomb_coeff * (1.0 + (tab[TB_X1 * NB + j] - log_n) * (1.0 / 74.8)) *
+                                   tab[TB_X0 * NB + j];
             radp = synch_coeff * p2 + r + coulomb + adiab * p;
             dT = dtT_e;
         }
-        B = radp - st.two_over_p[j] * D;
+        B = radp - tab[TB_2P * NB + j] * D;
         C = D;
     }
 };
@@ -133,7 +176,7 @@ __device__ __forceinline__ SegTerms<S> seg_terms(const GridTables &gt, const Bg 
     T.n_gas = bg.n_gas;
     T.kbt = bg.kbt;
     T.inv_kbt = 1.0 / bg.kbt;
-    T.inv_n = 1.0 / bg.n_gas;
+    T.log_n = log(bg.n_gas);
     T.adiab = 1.0 / 3.0 * (dis ? 0.0 : bg.divv);
     const double b_ratio = bg.b_field * 1.0e+6 / 3.2;
     T.synch_coeff = 4.8e-4 * b_ratio * b_ratio * 9.11e-28 * 3.0e+10 * 3.1536e+16;
@@ -143,7 +186,7 @@ __device__ __forceinline__ SegTerms<S> seg_terms(const GridTables &gt, const Bg 
     T.dtT_e = g.dt / 1.0e+100;
     T.ric = a.ic_curr + (ic_stride ? t : 0);
     T.ric_next = a.ic_next + (ic_stride ? t : 0);
-    T.ric_stride = ic_stride ? ic_stride : 1;
+    T.ric_stride = ic_stride;
     T.alpha = g.alpha;
     T.interp = g.nseg > 1;
     T.dpp_inv = 0.0;
@@ -156,38 +199,29 @@ struct WarpSmem {
     double B[kSw], C[kSw], D[kSw], Wp[kSw], Wm[kSw];
 };
 
-// The factored matrix of one system, distributed over the warp.
-template <bool SRC>
-struct Factor {
-    double inv[kR];      // 1 / d_i
-    double h[kR];        // a_i / d_i      (forward recurrence)
-    double q[kR];        // c_i / d_i      (back substitution)
-    double sd[SRC ? kR : 1];  // dt * source_i / d_i
-    double hk[5], qk[5]; // warp-scan multipliers per level
-};
 
-// Terms, faces, rows and the factorisation of one system.
-template <int S, bool SRC>
-__device__ unsigned factorize(const SegTerms<S> &T, const double *sdt, int lane, WarpSmem &sm,
-                              Factor<SRC> &F)
+// Terms, faces, rows and the factorisation of one system, stored to out.
+template <int S>
+__device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int lane, WarpSmem &sm,
+                                 double *out)
 {
     const SpeciesTables &st = T.gt->s[S];
     const double *x = st.p;
     unsigned err = 0;
 
     // terms, lane-strided
-#pragma unroll 1
+#pragma unroll 2
     for (int k = 0; k < kR; k++) {
         const int j = k * 32 + lane;
         double B, C, D;
-        T.at(j, B, C, D);
+        T.at(tab, j, B, C, D);
         sm.B[swz(j)] = B;
         sm.C[swz(j)] = C;
         sm.D[swz(j)] = D;
     }
     __syncwarp();
     // faces j (between bins j and j+1), lane-strided
-#pragma unroll 1
+#pragma unroll 2
     for (int k = 0; k < kR; k++) {
         const int j = k * 32 + lane;
         double wp = 0.0, wm = 0.0;
@@ -195,8 +229,8 @@ __device__ unsigned factorize(const SegTerms<S> &T, const double *sdt, int lane,
             const double cl = sm.C[swz(j)];
             if (fabs(cl) > 1.0e-200) {
                 const double w = (sm.B[swz(j)] + sm.B[swz(j + 1)]) / (cl + sm.C[swz(j + 1)]) *
-                                 (x[j + 1] - x[j]);
-                face_weights(w, wp, wm);
+                                 tab[TB_DXF * NB + j];
+                face_weights_fast(w, wp, wm);
             }
         }
         sm.Wp[swz(j)] = wp;
@@ -296,14 +330,122 @@ __device__ unsigned factorize(const SegTerms<S> &T, const double *sdt, int lane,
         const double den = Bd[r] + A[r] * cp_prev;
         if (fabs(den) <= 1.0e-300) err |= kErrSingular;
         const double inv = 1.0 / den;
-        F.inv[r] = inv;
-        F.h[r] = A[r] * inv;
-        F.q[r] = (m == NB - 1) ? 0.0 : Cc[r] * inv;
-        if (SRC) F.sd[r] = sdt[r] * inv;
-        cp_prev = -Cc[r] * inv;
+        const double cr = Cc[r];
+        Bd[r] = inv;
+        A[r] = A[r] * inv;
+        Cc[r] = (m == NB - 1) ? 0.0 : cr * inv;
+        cp_prev = -cr * inv;
     }
+    // inv, h = a / d, q = c / d of this lane's rows: 64 contiguous bytes per
+    // array per lane, 2 KB per array per warp
+#pragma unroll
+    for (int r = 0; r < kR; r += 2) {
+        __stcg(reinterpret_cast<double2 *>(out + row0 + r), make_double2(Bd[r], Bd[r + 1]));
+        __stcg(reinterpret_cast<double2 *>(out + NB + row0 + r), make_double2(A[r], A[r + 1]));
+        __stcg(reinterpret_cast<double2 *>(out + 2 * NB + row0 + r), make_double2(Cc[r], Cc[r + 1]));
+    }
+    (void)vp;
+    return err;
+}
 
-    // ---- warp-scan multipliers of the two linear recurrences ----
+
+// Factor kernel, persistent: each block stages the species' grid tables in
+// shared memory once, then its warps take work items u -> (segment gi, set,
+// tracer tl), tl fastest, strided by the grid.
+template <int S>
+__global__ void __launch_bounds__(kFacWarps * 32, (NB <= 256 ? 2 : 1)) factor_kernel(FusedParams P)
+{
+    extern __shared__ double4 smem_raw[];
+    double *tab = reinterpret_cast<double *>(smem_raw);
+    WarpSmem *smem = reinterpret_cast<WarpSmem *>(tab + kTab * NB);
+    const int w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const SnapArgs &a = P.a;
+    const SpeciesTables &st = P.gt.s[S];
+    for (int i = threadIdx.x; i < NB; i += blockDim.x) {
+        tab[TB_P * NB + i] = st.p[i];
+        tab[TB_P2 * NB + i] = st.p2[i];
+        tab[TB_CUT * NB + i] = st.exp_cut[i];
+        tab[TB_2P * NB + i] = st.two_over_p[i];
+        tab[TB_DXF * NB + i] = st.dxf[i];
+        if (S == 0) {
+            tab[TB_X0 * NB + i] = st.expE[i];
+            tab[TB_X1 * NB + i] = P.gt.cp_Ep[i];
+            tab[TB_X2 * NB + i] = P.gt.cp_inv2mpkin[i];
+            tab[TB_X3 * NB + i] = P.gt.cp_inv_betap2[i];
+            tab[TB_X4 * NB + i] = P.gt.sig_eff[i];
+        } else {
+            tab[TB_X0 * NB + i] = P.gt.ce_inv_beta2[i];
+            tab[TB_X1 * NB + i] = P.gt.ce_logp[i];
+            tab[TB_X2 * NB + i] = (P.ic_stride == 0) ? a.ic_curr[i] : 0.0;
+            tab[TB_X3 * NB + i] = (P.ic_stride == 0) ? a.ic_next[i] : 0.0;
+            tab[TB_X4 * NB + i] = 0.0;
+        }
+    }
+    __syncthreads();
+    const long long total = (long long)(P.g1 - P.g0) * P.sets * P.nt;
+    const long long stride = (long long)gridDim.x * kFacWarps;
+#pragma unroll 1
+    for (long long u = (long long)blockIdx.x * kFacWarps + w; u < total; u += stride) {
+        const int tl = (int)(u % P.nt);
+        const int rest = (int)(u / P.nt);
+        const int set = rest % P.sets, gi = rest / P.sets;
+        const int t = P.t0 + tl;
+        const SegInfo g = segment_of(P, t, P.g0 + gi);
+        if (!g.active || !needs_set(g, set)) continue;
+        if (needs_set(g, 1) && P.sets < 2) {   // checked on the host; never write past the sets
+            if (lane == 0) atomicOr(a.err, kErrBadInput);
+            continue;
+        }
+        const Bg bg = load_bg(a, t, g);
+        const int dis = a.dis ? a.dis[t] : 0;
+        SegTerms<S> T = seg_terms<S>(P.gt, bg, dis, a, g, t, P.ic_stride);
+        if (set == 0) {
+            const double tacc = segment_tacc(P.mp, a, g);
+            const DppForm on = dpp_form(P.mp, P.mp.dpp_model, bg, tacc);
+            T.dpp_fill = on.fill;
+            T.dpp_inv = on.inv;
+            T.dpp_scale = (P.mp.dpp_model != kDppOff && P.eta_scale) ? P.eta_scale[t] : 1.0;
+        }
+        const unsigned err = factor_store<S>(T, tab, lane, smem[w], fac_ptr(P, S, gi, set, tl));
+        if (err && lane == 0) atomicOr(a.err, err);
+        __syncwarp();
+    }
+}
+
+// The factored rows of one segment as a lane holds them for its sub-steps,
+// with the warp-scan multipliers.  hk[lv] / qk[lv] are zero on the lanes a
+// scan level does not combine, and lane 0's a/d of row 0 and lane 31's c/d of
+// the last row are zero, so the scans need no lane predicates.
+template <bool SRC>
+struct Coef {
+    double inv[kR];      // 1 / d_i
+    double h[kR];        // a_i / d_i      (forward recurrence)
+    double q[kR];        // c_i / d_i      (back substitution)
+    double sd[SRC ? kR : 1];  // dt * source_i / d_i
+    double hk[5], qk[5];
+};
+
+template <bool SRC>
+__device__ __forceinline__ void load_coef(Coef<SRC> &F, const double *fac, const double *src, double dt,
+                                          int lane)
+{
+    const int row0 = lane * kR;
+#pragma unroll
+    for (int r = 0; r < kR; r += 2) {
+        const double2 vi = __ldcg(reinterpret_cast<const double2 *>(fac + row0 + r));
+        const double2 vh = __ldcg(reinterpret_cast<const double2 *>(fac + NB + row0 + r));
+        const double2 vq = __ldcg(reinterpret_cast<const double2 *>(fac + 2 * NB + row0 + r));
+        F.inv[r] = vi.x; F.inv[r + 1] = vi.y;
+        F.h[r] = vh.x; F.h[r + 1] = vh.y;
+        F.q[r] = vq.x; F.q[r + 1] = vq.y;
+    }
+    if (lane == 0) F.h[0] = 0.0;
+    if (lane == 31) F.q[kR - 1] = 0.0;
+    if (SRC) {
+#pragma unroll
+        for (int r = 0; r < kR; r++) F.sd[r] = (dt * src[row0 + r]) * F.inv[r];
+    }
     double H = 1.0, Q = 1.0;
 #pragma unroll
     for (int r = 0; r < kR; r++) {
@@ -313,78 +455,59 @@ __device__ unsigned factorize(const SegTerms<S> &T, const double *sdt, int lane,
 #pragma unroll
     for (int lv = 0; lv < 5; lv++) {
         const int off = 1 << lv;
-        F.hk[lv] = H;
-        F.qk[lv] = Q;
+        F.hk[lv] = (lane >= off) ? H : 0.0;
+        F.qk[lv] = (lane + off < 32) ? Q : 0.0;
         const double Hu = sup(H, off), Qd = sdn(Q, off);
         if (lane >= off) H *= Hu;
         if (lane + off < 32) Q *= Qd;
     }
-    (void)vp;
-    return err;
 }
 
 // One implicit sub-step: N <- M^{-1} (N + dt src) with the factored M.
+// A shuffle from a lane outside the warp returns the caller's own (finite)
+// value, which the zero multipliers discard exactly.
 template <bool SRC>
-__device__ __forceinline__ void substep(const Factor<SRC> &F, int lane, double N[kR])
+__device__ __forceinline__ void substep(const Coef<SRC> &F, double N[kR])
 {
-    double y[kR];
     double acc = 0.0;
 #pragma unroll
     for (int r = 0; r < kR; r++) {
-        y[r] = SRC ? fma(N[r], F.inv[r], F.sd[r]) : N[r] * F.inv[r];
-        acc = fma(F.h[r], acc, y[r]);
+        N[r] = SRC ? fma(N[r], F.inv[r], F.sd[r]) : N[r] * F.inv[r];
+        acc = fma(F.h[r], acc, N[r]);
     }
 #pragma unroll
-    for (int lv = 0; lv < 5; lv++) {
-        const int off = 1 << lv;
-        const double o = sup(acc, off);
-        if (lane >= off) acc = fma(F.hk[lv], o, acc);
-    }
+    for (int lv = 0; lv < 5; lv++) acc = fma(F.hk[lv], sup(acc, 1 << lv), acc);
     double prev = sup(acc, 1);
-    if (lane == 0) prev = 0.0;
 #pragma unroll
     for (int r = 0; r < kR; r++) {
-        prev = fma(F.h[r], prev, y[r]);
-        y[r] = prev;
+        prev = fma(F.h[r], prev, N[r]);
+        N[r] = prev;
     }
     acc = 0.0;
 #pragma unroll
-    for (int r = kR - 1; r >= 0; r--) acc = fma(F.q[r], acc, y[r]);
+    for (int r = kR - 1; r >= 0; r--) acc = fma(F.q[r], acc, N[r]);
 #pragma unroll
-    for (int lv = 0; lv < 5; lv++) {
-        const int off = 1 << lv;
-        const double o = sdn(acc, off);
-        if (lane + off < 32) acc = fma(F.qk[lv], o, acc);
-    }
+    for (int lv = 0; lv < 5; lv++) acc = fma(F.qk[lv], sdn(acc, 1 << lv), acc);
     prev = sdn(acc, 1);
-    if (lane == 31) prev = 0.0;
 #pragma unroll
     for (int r = kR - 1; r >= 0; r--) {
-        prev = fma(F.q[r], prev, y[r]);
+        prev = fma(F.q[r], prev, N[r]);
         N[r] = prev;
     }
 }
 
-// Systems of species S for tracers with a segment in this slot: warp w of
-// block b handles tracer b * kWarps + w.
+// Steps kernel: warp w of block b runs every segment [g0, g1) of tracer
+// t0 + b * kWarps + w for species S.
 template <int S, bool SRC>
-__global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) fused_slot_kernel(FusedParams P)
+__global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) steps_kernel(FusedParams P)
 {
-    extern __shared__ double4 smem_raw[];
-    WarpSmem *smem = reinterpret_cast<WarpSmem *>(smem_raw);
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
+    const int tl = blockIdx.x * kWarps + w;
+    if (tl >= P.nt) return;
+    const int t = P.t0 + tl;
     const SnapArgs &a = P.a;
-    const int t = blockIdx.x * kWarps + w;
-    if (t >= a.ntracer) return;
-    const SegInfo g = segment_of(P, t);
-    if (!g.active) return;
-    const Bg bg = load_bg(a, t, g);
-    const double tacc = segment_tacc(P.mp, a, g);
-    const int dis = a.dis ? a.dis[t] : 0;
-    SegTerms<S> T = seg_terms<S>(P.gt, bg, dis, a, g, t, P.ic_stride);
     const int row0 = lane * kR;
-
     double *Nrow = (S == 0 ? a.crp : a.cre) + (size_t)t * NB + row0;
     double N[kR];
 #pragma unroll
@@ -393,49 +516,63 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) fused_slot_k
         N[r] = v.x;
         N[r + 1] = v.y;
     }
-    double sdt[SRC ? kR : 1];
-    if (SRC) {
-        const double *src = (S == 0) ? a.qpi : (P.inje ? P.inje : a.qepri);
-#pragma unroll
-        for (int r = 0; r < kR; r++) sdt[r] = g.dt * src[(size_t)t * NB + row0 + r];
-    }
-
-    const DppForm on = dpp_form(P.mp, P.mp.dpp_model, bg, tacc);
-    const double on_scale = (P.mp.dpp_model != kDppOff && P.eta_scale) ? P.eta_scale[t] : 1.0;
-
-    Factor<SRC> F;
-    int cur = -1;
-    unsigned err = 0;
+    const double *qsrc = (S == 0) ? a.qpi : a.qepri;
+    Coef<SRC> F;
 #pragma unroll 1
-    for (int istep = 0; istep < g.steps; istep++) {
-        const int want = (!g.windowed || (istep >= g.sl && istep < g.el)) ? 0 : 1;
-        if (want != cur) {
-            T.dpp_fill = want == 0 ? on.fill : 0;
-            T.dpp_inv = want == 0 ? on.inv : 0.0;
-            T.dpp_scale = want == 0 ? on_scale : 1.0;
-            err |= factorize<S, SRC>(T, sdt, lane, smem[w], F);
-            cur = want;
+    for (int gi = 0; gi < P.g1 - P.g0; gi++) {
+        const SegInfo g = segment_of(P, t, P.g0 + gi);
+        if (!g.active) continue;
+        if (S == 0 && P.np_seg) {
+            double *o = P.np_seg + ((size_t)gi * P.nt + tl) * NB + row0;
+#pragma unroll
+            for (int r = 0; r < kR; r += 2)
+                __stcg(reinterpret_cast<double2 *>(o + r), make_double2(N[r], N[r + 1]));
         }
-        substep<SRC>(F, lane, N);
+        const double *src = nullptr;
+        if (SRC) {
+            src = (S == 1 && P.inje) ? P.inje + ((size_t)gi * P.nt + tl) * NB
+                                     : qsrc + (size_t)t * NB;
+        }
+        // runs of sub-steps with one coefficient set: Dpp off before the
+        // window, on inside it, off after it (all on when not windowed)
+        const int sl = g.windowed ? min(max(g.sl, 0), g.steps) : 0;
+        const int el = g.windowed ? min(max(g.el, sl), g.steps) : g.steps;
+        const int run_n[3] = {sl, el - sl, g.steps - el};
+        int cur = -1;
+#pragma unroll 1
+        for (int k = 0; k < 3; k++) {
+            const int want = (k == 1) ? 0 : 1;
+            if (run_n[k] <= 0) continue;
+            if (want >= P.sets) {   // no off set in the workspace: report, leave N as it was
+                if (lane == 0) atomicOr(a.err, kErrBadInput);
+                return;
+            }
+            if (want != cur) {
+                load_coef<SRC>(F, fac_ptr(P, S, gi, want, tl), src, g.dt, lane);
+                cur = want;
+            }
+#pragma unroll 1
+            for (int istep = 0; istep < run_n[k]; istep++) substep<SRC>(F, N);
+        }
     }
-    if (err && lane == 0) atomicOr(a.err, err);
 #pragma unroll
     for (int r = 0; r < kR; r += 2)
         *reinterpret_cast<double2 *>(Nrow + r) = make_double2(N[r], N[r + 1]);
 }
 
-// Dpp eta-cap scale of every tracer with a segment in this slot, from the
-// spectra at the start of the segment (prepare_momentumdiff_cell_major,
+// Dpp eta-cap scale of every tracer of the chunk with a segment in slot g0,
+// from the spectra at the start of the segment (prepare_momentumdiff_cell_major,
 // src/fp_shared_core.c:1032-1081, runs before either species evolves), one
 // warp per tracer.  The energy sum is split over the lanes and combined by a
 // shuffle tree, so it agrees with the reference's sequential sum to rounding.
 __global__ void __launch_bounds__(128) eta_scale_kernel(FusedParams P, double *eta)
 {
     const int lane = threadIdx.x & 31;
-    const int t = blockIdx.x * 4 + (threadIdx.x >> 5);
+    const int tl = blockIdx.x * 4 + (threadIdx.x >> 5);
     const SnapArgs &a = P.a;
-    if (t >= a.ntracer) return;
-    const SegInfo g = segment_of(P, t);
+    if (tl >= P.nt) return;
+    const int t = P.t0 + tl;
+    const SegInfo g = segment_of(P, t, P.g0);
     if (!g.active) return;
     const Bg bg = load_bg(a, t, g);
     const double tacc_direct = segment_tacc(P.mp, a, g);
@@ -453,17 +590,21 @@ __global__ void __launch_bounds__(128) eta_scale_kernel(FusedParams P, double *e
     if (lane == 0) eta[t] = eta_cap_scale_from_ecr(P.mp, bg, mass, tacc_direct, ecr);
 }
 
-// Secondary source of the slot, cell-major:
-// inje[t][je] = Gyr n_gas(t) sum_{jp} N_p[t][jp] fqe[jp][je] + qepri[t][je].
-// 64 x 64 output tile, 16 x 16 threads, 4 x 4 outputs each; the proton
-// index runs upward from the first bin with a nonzero weight in the tile.
-__global__ void __launch_bounds__(256) fused_secondary_kernel(FusedParams P, double *inje)
+// Secondary source of every segment of the chunk, cell-major:
+// inje[gi][tl][je] = Gyr n_gas(t, segment) sum_{jp} N_p[gi][tl][jp] fqe[jp][je]
+//                    + qepri[t][je],
+// over the rows m = gi * nt + tl.  64 x 64 output tile, 16 x 16 threads,
+// 4 x 4 outputs each; the proton index runs upward from the first bin with a
+// nonzero weight in the tile.
+__global__ void __launch_bounds__(256) secondary_kernel(FusedParams P)
 {
     __shared__ double sN[64][17];
     __shared__ double sF[16][64];
     const SnapArgs &a = P.a;
+    const long long nrows = (long long)(P.g1 - P.g0) * P.nt;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 16 + tx;
-    const int t0 = blockIdx.x * 64, je0 = blockIdx.y * 64;
+    const long long m0 = (long long)blockIdx.x * 64;
+    const int je0 = blockIdx.y * 64;
     int jstart = NB;
     for (int i = 0; i < 64 && je0 + i < NB; i++) jstart = min(jstart, P.np_min_qe[je0 + i]);
     jstart = max(jstart, P.gt.fqe_jp0);
@@ -475,8 +616,9 @@ __global__ void __launch_bounds__(256) fused_secondary_kernel(FusedParams P, dou
     for (int k0 = jstart; k0 < NB; k0 += 16) {
         for (int q = tid; q < 64 * 16; q += 256) {
             const int tt = q / 16, kk = q % 16;
-            const int t = t0 + tt, jp = k0 + kk;
-            sN[tt][kk] = (t < a.ntracer && jp < NB) ? a.crp[(size_t)t * NB + jp] : 0.0;
+            const long long m = m0 + tt;
+            const int jp = k0 + kk;
+            sN[tt][kk] = (m < nrows && jp < NB) ? P.np_seg[(size_t)m * NB + jp] : 0.0;
             const int r = q / 64, col = q % 64;
             const int jp2 = k0 + r;
             sF[r][col] = (jp2 < NB && je0 + col < NB) ? P.gt.fqe[(size_t)jp2 * NB + je0 + col] : 0.0;
@@ -498,9 +640,11 @@ __global__ void __launch_bounds__(256) fused_secondary_kernel(FusedParams P, dou
     }
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        const int t = t0 + ty + 16 * i;
-        if (t >= a.ntracer) continue;
-        const SegInfo g = segment_of(P, t);
+        const long long m = m0 + ty + 16 * i;
+        if (m >= nrows) continue;
+        const int gi = (int)(m / P.nt), tl = (int)(m % P.nt);
+        const int t = P.t0 + tl;
+        const SegInfo g = segment_of(P, t, P.g0 + gi);
         if (!g.active) continue;
         const double ng = (g.nseg > 1) ? lerp(a.bg_curr[t], a.bg_next[t], g.alpha) : a.bg_curr[t];
 #pragma unroll
@@ -508,87 +652,180 @@ __global__ void __launch_bounds__(256) fused_secondary_kernel(FusedParams P, dou
             const int je = je0 + tx + 16 * j;
             if (je >= NB) continue;
             const double q = a.qepri ? a.qepri[(size_t)t * NB + je] : 0.0;
-            inje[(size_t)t * NB + je] = acc[i][j] * kGyr * ng + q;
+            P.inje[(size_t)m * NB + je] = acc[i][j] * kGyr * ng + q;
         }
     }
 }
 
-template <int S, bool SRC>
-cudaError_t launch_one(Context &ctx, const FusedParams &P)
+template <int S>
+cudaError_t launch_factor(Context &ctx, const FusedParams &P)
 {
-    constexpr size_t smem = kWarps * sizeof(WarpSmem);
-    static bool configured = false;   // per instantiation; set before the first launch
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(fused_slot_kernel<S, SRC>,
+    constexpr size_t smem = (size_t)kTab * NB * sizeof(double) + kFacWarps * sizeof(WarpSmem);
+    static int resident = 0;   // blocks per SM, per instantiation; found before the first launch
+    if (!resident) {
+        cudaError_t e = cudaFuncSetAttribute(factor_kernel<S>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, factor_kernel<S>, kFacWarps * 32, smem);
+        if (e != cudaSuccess) return e;
+        if (resident < 1) return cudaErrorInvalidConfiguration;
     }
-    const int blocks = (P.a.ntracer + kWarps - 1) / kWarps;
-    fused_slot_kernel<S, SRC><<<blocks, kWarps * 32, smem, ctx.stream>>>(P);
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long warps = (long long)(P.g1 - P.g0) * P.sets * P.nt;
+    long long blocks = (warps + kFacWarps - 1) / kFacWarps;
+    const long long full = (long long)nsm * resident;
+    if (blocks > full) blocks = full;
+    if (blocks < 1) return cudaSuccess;
+    factor_kernel<S><<<(unsigned)blocks, kFacWarps * 32, smem, ctx.stream>>>(P);
     return cudaGetLastError();
 }
 
 template <int S>
-cudaError_t launch_slot(Context &ctx, const FusedParams &P, bool src)
+cudaError_t launch_steps(Context &ctx, const FusedParams &P, bool src)
 {
-    return src ? launch_one<S, true>(ctx, P) : launch_one<S, false>(ctx, P);
+    const int blocks = (P.nt + kWarps - 1) / kWarps;
+    if (src) steps_kernel<S, true><<<blocks, kWarps * 32, 0, ctx.stream>>>(P);
+    else steps_kernel<S, false><<<blocks, kWarps * 32, 0, ctx.stream>>>(P);
+    return cudaGetLastError();
+}
+
+// Workspace budget of the fused path (factored matrices, segment-start
+// proton spectra, segment sources); CROMA_B200_WORKSPACE_GB overrides it.
+double workspace_budget_bytes()
+{
+    const char *s = getenv("CROMA_B200_WORKSPACE_GB");
+    double gb = s ? atof(s) : 0.0;
+    if (!(gb > 0.0)) gb = 24.0;
+    return gb * 1e9;
 }
 
 }  // namespace
 
 int fused_reserve(Context &ctx, int cap)
 {
+    const int nseg = ctx.mp.interp_max_segments < 1 ? 1
+                   : (ctx.mp.interp_max_segments > 64 ? 64 : ctx.mp.interp_max_segments);
+    const int sets = ctx.mp.window_centred ? 2 : 1;
+    const double per_tracer = 8.0 * NB * ((double)2 * nseg * sets * 3 + 2.0 * nseg);
+    long long chunk = (long long)(workspace_budget_bytes() / per_tracer);
+    if (chunk < 1) chunk = 1;
+    if (chunk > cap) chunk = cap;
     cudaFree(ctx.d_inje);
     cudaFree(ctx.d_eta_scale);
-    ctx.d_inje = ctx.d_eta_scale = nullptr;
-    CROMA_CUDA(cudaMalloc(&ctx.d_inje, (size_t)NB * cap * sizeof(double)));
+    cudaFree(ctx.d_fac);
+    cudaFree(ctx.d_np_seg);
+    ctx.d_inje = ctx.d_eta_scale = ctx.d_fac = ctx.d_np_seg = nullptr;
+    ctx.fused_chunk = ctx.fused_nseg = ctx.fused_sets = 0;
+    const size_t rows = (size_t)nseg * chunk * NB;
+    CROMA_CUDA(cudaMalloc(&ctx.d_fac, (size_t)2 * sets * rows * 3 * sizeof(double)));
+    CROMA_CUDA(cudaMalloc(&ctx.d_np_seg, rows * sizeof(double)));
+    CROMA_CUDA(cudaMalloc(&ctx.d_inje, rows * sizeof(double)));
     CROMA_CUDA(cudaMalloc(&ctx.d_eta_scale, (size_t)cap * sizeof(double)));
+    ctx.fused_chunk = (int)chunk;
+    ctx.fused_nseg = nseg;
+    ctx.fused_sets = sets;
     return 0;
 }
 
-// One slot: the secondary source (when both species evolve), then the
-// proton and electron systems.
-static int fused_one_slot(Context &ctx, FusedParams &P)
+// Segments [g0, g1) of one tracer chunk: the eta-cap scales (if the cap is
+// on), the factored matrices of both species, the proton steps, the
+// secondary source, the electron steps.
+static int fused_range(Context &ctx, FusedParams &P, int g0, int g1)
 {
     const SnapArgs &a = P.a;
     const int protons = ctx.mp.species_mask & CROMA_SPECIES_PROTON;
     const int electrons = ctx.mp.species_mask & CROMA_SPECIES_ELECTRON;
-    cudaEvent_t ev = nullptr;
-    P.inje = nullptr;
+    const bool secondaries = protons && electrons;
+    const bool cap = ctx.mp.eta_dpp_cap > 0.0 && isfinite(ctx.mp.eta_dpp_cap) && ctx.mp.dpp_model != kDppOff;
+    if (cap && g1 != g0 + 1) {
+        set_error("internal: the eta cap needs one segment per launch");
+        return -1;
+    }
+    P.g0 = g0;
+    P.g1 = g1;
     P.eta_scale = nullptr;
-    if (ctx.mp.eta_dpp_cap > 0.0 && isfinite(ctx.mp.eta_dpp_cap) && ctx.mp.dpp_model != kDppOff) {
-        timed_begin(ctx, kKindCoeff, &ev);
-        eta_scale_kernel<<<(a.ntracer + 3) / 4, 128, 0, ctx.stream>>>(P, ctx.d_eta_scale);
-        timed_end(ctx, kKindCoeff, ev);
+    P.np_seg = secondaries ? ctx.d_np_seg : nullptr;
+    P.inje = secondaries ? ctx.d_inje : nullptr;
+    cudaEvent_t ev = nullptr;
+    timed_begin(ctx, kKindCoeff, &ev);
+    if (cap) {
+        eta_scale_kernel<<<(P.nt + 3) / 4, 128, 0, ctx.stream>>>(P, ctx.d_eta_scale);
         ctx.last_launches += 1;
         P.eta_scale = ctx.d_eta_scale;
     }
-    if (protons && electrons) {
-        dim3 sg((a.ntracer + 63) / 64, (NB + 63) / 64), sb(16, 16);
-        timed_begin(ctx, kKindSecondary, &ev);
-        fused_secondary_kernel<<<sg, sb, 0, ctx.stream>>>(P, ctx.d_inje);
-        timed_end(ctx, kKindSecondary, ev);
-        ctx.last_launches += 1;
-        P.inje = ctx.d_inje;
-    }
-    timed_begin(ctx, kKindEvolve, &ev);
     if (protons) {
-        CROMA_CUDA(launch_slot<0>(ctx, P, a.qpi != nullptr));
+        CROMA_CUDA(launch_factor<0>(ctx, P));
         ctx.last_launches += 1;
     }
     if (electrons) {
-        CROMA_CUDA(launch_slot<1>(ctx, P, P.inje != nullptr || a.qepri != nullptr));
+        CROMA_CUDA(launch_factor<1>(ctx, P));
         ctx.last_launches += 1;
     }
-    timed_end(ctx, kKindEvolve, ev);
+    timed_end(ctx, kKindCoeff, ev);
+    if (protons) {
+        timed_begin(ctx, kKindEvolve, &ev);
+        CROMA_CUDA(launch_steps<0>(ctx, P, a.qpi != nullptr));
+        timed_end(ctx, kKindEvolve, ev);
+        ctx.last_launches += 1;
+    }
+    if (secondaries) {
+        const long long rows = (long long)(g1 - g0) * P.nt;
+        dim3 sg((unsigned)((rows + 63) / 64), (NB + 63) / 64), sb(16, 16);
+        timed_begin(ctx, kKindSecondary, &ev);
+        secondary_kernel<<<sg, sb, 0, ctx.stream>>>(P);
+        timed_end(ctx, kKindSecondary, ev);
+        ctx.last_launches += 1;
+    }
+    if (electrons) {
+        timed_begin(ctx, kKindEvolve, &ev);
+        CROMA_CUDA(launch_steps<1>(ctx, P, secondaries || a.qepri != nullptr));
+        timed_end(ctx, kKindEvolve, ev);
+        ctx.last_launches += 1;
+    }
     CROMA_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// Every segment slot of every tracer chunk.
+static int fused_chunks(Context &ctx, FusedParams &P, int nslots)
+{
+    if (ctx.fused_chunk <= 0 || !ctx.d_fac) {
+        set_error("fused workspace not reserved");
+        return -1;
+    }
+    if (nslots > ctx.fused_nseg) {
+        set_error("internal: more segment slots than the fused workspace holds");
+        return -1;
+    }
+    const bool windows = P.explicit_seg ? P.ex.windowed != 0 : ctx.mp.window_centred != 0;
+    if (windows && ctx.fused_sets < 2) {
+        set_error("internal: windowed segments without an off-coefficient workspace");
+        return -1;
+    }
+    const bool cap = ctx.mp.eta_dpp_cap > 0.0 && isfinite(ctx.mp.eta_dpp_cap) && ctx.mp.dpp_model != kDppOff;
+    P.sets = ctx.fused_sets;
+    P.fac = ctx.d_fac;
+    for (int t0 = 0; t0 < P.a.ntracer; t0 += ctx.fused_chunk) {
+        P.t0 = t0;
+        P.nt = P.a.ntracer - t0 < ctx.fused_chunk ? P.a.ntracer - t0 : ctx.fused_chunk;
+        if (!cap) {
+            const int rc = fused_range(ctx, P, 0, nslots);
+            if (rc) return rc;
+        } else {
+            for (int g = 0; g < nslots; g++) {
+                const int rc = fused_range(ctx, P, g, g + 1);
+                if (rc) return rc;
+            }
+        }
+    }
     return 0;
 }
 
 int run_fused(Context &ctx, const SnapArgs &a)
 {
-    FusedParams P;
+    FusedParams P{};
     P.a = a;
     P.gt = ctx.gt;
     P.mp = ctx.mp;
@@ -596,27 +833,22 @@ int run_fused(Context &ctx, const SnapArgs &a)
     P.explicit_seg = 0;
     P.ex = SegInfo{};
     P.ic_stride = 0;
-    const int nslots = ctx.mp.interp_max_segments < 1 ? 1 : ctx.mp.interp_max_segments;
-    for (int slot = 0; slot < nslots && slot < 64; slot++) {
-        P.slot = slot;
-        int rc = fused_one_slot(ctx, P);
-        if (rc) return rc;
-    }
-    return 0;
+    const int nslots = ctx.mp.interp_max_segments < 1 ? 1
+                     : (ctx.mp.interp_max_segments > 64 ? 64 : ctx.mp.interp_max_segments);
+    return fused_chunks(ctx, P, nslots);
 }
 
 int run_fused_segment(Context &ctx, const SnapArgs &a, const SegInfo &ex, int ic_stride)
 {
-    FusedParams P;
+    FusedParams P{};
     P.a = a;
     P.gt = ctx.gt;
     P.mp = ctx.mp;
     P.np_min_qe = ctx.d_np_min_qe;
-    P.slot = 0;
     P.explicit_seg = 1;
     P.ex = ex;
     P.ic_stride = ic_stride;
-    return fused_one_slot(ctx, P);
+    return fused_chunks(ctx, P, 1);
 }
 
 }  // namespace croma

@@ -462,6 +462,8 @@ void cuda_pipeline_workspace_destroy(FpCudaPipelineWorkspace *w)
     cudaFree(w->r_crp); cudaFree(w->r_cre); cudaFree(w->r_qpi); cudaFree(w->r_qepri);
     cudaFree(c.d_inje);
     cudaFree(c.d_eta_scale);
+    cudaFree(c.d_fac);
+    cudaFree(c.d_np_seg);
     cudaFree(c.d_tables);
     cudaFree(c.d_np_min_qe);
     cudaFree(c.d_err);
@@ -543,14 +545,15 @@ int run_tracer_pipeline(const FpCudaPipelineInput *in, const FpCudaOutputSchedul
     CROMA_CUDA(cudaSetDevice(c.device));
     const FpCoeffBatchInput *ci = in->coeff_in;
     const int n = in->ncell;
-    cudaEvent_t e0, e1, e2, e3;
-    cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3);
-    cudaEventRecord(e0, c.stream);
+    // the model first: the bucket workspace is sized by it (on/off factor sets)
+    fill_model(c.mp, in->psi_value, in->mach_limit_value);
+    c.cfg.species_mask = 3;
     int rc = ensure_tables(w, in->crp_grid, in->cre_grid);
     if (!rc) rc = ensure_bucket(w, n);
     if (rc) return rc;
-    fill_model(c.mp, in->psi_value, in->mach_limit_value);
-    c.cfg.species_mask = 3;
+    cudaEvent_t e0, e1, e2, e3;
+    cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3);
+    cudaEventRecord(e0, c.stream);
 
     // ---- spectra and sources of the bucket ----
     const size_t st = (size_t)n * NB * sizeof(double);

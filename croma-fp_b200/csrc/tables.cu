@@ -165,10 +165,10 @@ int build_tables(Context &ctx)
     }
 
     // ---- caches, FP_Coef.c:77-156 and the grid-only kinematics ----
-    enum { T_P, T_DP, T_E, T_P2, T_CUT, T_2P, T_EXPE, T_IDX, T_IDXL, T_IDXR, T_PER };   // per species
+    enum { T_P, T_DP, T_E, T_P2, T_CUT, T_2P, T_EXPE, T_IDX, T_IDXL, T_IDXR, T_DXF, T_PER };   // per species
     const int nspecies_arrays = T_PER * 2;
-    // cp_Ep, cp_kin, cp_inv_betap2, sig_eff, ce_beta2, cp_inv2mpkin, ce_inv_beta2
-    const int n_extra = 7;
+    // cp_Ep, cp_kin, cp_inv_betap2, sig_eff, ce_beta2, cp_inv2mpkin, ce_inv_beta2, ce_logp
+    const int n_extra = 8;
     const size_t tab_doubles = (size_t)(nspecies_arrays + n_extra) * n + (size_t)n * n;
     std::vector<double> h(tab_doubles, 0.0);
     auto arr = [&](int k) { return h.data() + (size_t)k * n; };
@@ -177,6 +177,7 @@ int build_tables(Context &ctx)
         double *P2 = arr(s * T_PER + T_P2), *CUT = arr(s * T_PER + T_CUT);
         double *TWO = arr(s * T_PER + T_2P), *EXPE = arr(s * T_PER + T_EXPE);
         double *IDX = arr(s * T_PER + T_IDX), *IDXL = arr(s * T_PER + T_IDXL), *IDXR = arr(s * T_PER + T_IDXR);
+        double *DXF = arr(s * T_PER + T_DXF);
         for (int j = 0; j < n; j++) {
             P[j] = ctx.h_p[s][j];
             DP[j] = ctx.h_dp[s][j];
@@ -190,12 +191,14 @@ int build_tables(Context &ctx)
         for (int j = 0; j < n; j++) {
             IDXL[j] = (j >= 1) ? 1.0 / (ctx.h_p[s][j] - ctx.h_p[s][j - 1]) : 0.0;
             IDXR[j] = (j <= n - 2) ? 1.0 / (ctx.h_p[s][j + 1] - ctx.h_p[s][j]) : 0.0;
+            DXF[j] = (j <= n - 2) ? ctx.h_p[s][j + 1] - ctx.h_p[s][j] : 0.0;
         }
     }
     double *cpEp = arr(nspecies_arrays + 0), *cpKin = arr(nspecies_arrays + 1);
     double *cpIb = arr(nspecies_arrays + 2), *sigEff = arr(nspecies_arrays + 3);
     double *ceB2 = arr(nspecies_arrays + 4), *cpI2 = arr(nspecies_arrays + 5);
     double *ceIB2 = arr(nspecies_arrays + 6);
+    double *ceLogp = arr(nspecies_arrays + 7);
     std::vector<double> sigma(n), sigmoid(n);
     for (int j = 0; j < n; j++) sigma[j] = pp_pion_xsec(2, kMp * ctx.h_p[0][j]);
     int j_pp = 0;
@@ -219,6 +222,7 @@ int build_tables(Context &ctx)
         const double pe2 = ctx.h_p[1][j] * ctx.h_p[1][j];
         ceB2[j] = pe2 / (1.0 + pe2);
         ceIB2[j] = 1.0 / ceB2[j];
+        ceLogp[j] = log(ctx.h_p[1][j]);
     }
 
     // ---- device allocation ----
@@ -241,6 +245,7 @@ int build_tables(Context &ctx)
         st.inv_dx = darr(s * T_PER + T_IDX);
         st.inv_dxl = darr(s * T_PER + T_IDXL);
         st.inv_dxr = darr(s * T_PER + T_IDXR);
+        st.dxf = darr(s * T_PER + T_DXF);
         st.pm1 = ctx.h_pm1[s];
         st.pp1 = ctx.h_pp1[s];
         st.pm1_p2 = st.pm1 * st.pm1;
@@ -257,6 +262,7 @@ int build_tables(Context &ctx)
     ctx.gt.ce_beta2 = darr(nspecies_arrays + 4);
     ctx.gt.cp_inv2mpkin = darr(nspecies_arrays + 5);
     ctx.gt.ce_inv_beta2 = darr(nspecies_arrays + 6);
+    ctx.gt.ce_logp = darr(nspecies_arrays + 7);
     for (int k = 0; k < 2; k++) {
         const double p = k == 0 ? ctx.h_pm1[0] : ctx.h_pp1[0], p2 = p * p;
         const double gamma = sqrt(1.0 + p2);
@@ -333,7 +339,15 @@ int ic_rows(Context &ctx, double z, double *d_out)
         set_error("IC outer grid out of range");
         return -2;
     }
-    std::vector<double> outer(N + 1);
+    if (!ctx.h_ic_stage) {
+        CROMA_CUDA(cudaMallocHost(&ctx.h_ic_stage, 2 * (size_t)(kIcMaxOuter + 1) * sizeof(double)));
+        for (int k = 0; k < 2; k++)
+            CROMA_CUDA(cudaEventCreateWithFlags(&ctx.ic_stage_ev[k], cudaEventDisableTiming));
+    }
+    const int k = ctx.ic_stage_next;
+    ctx.ic_stage_next ^= 1;
+    CROMA_CUDA(cudaEventSynchronize(ctx.ic_stage_ev[k]));   // the copy that last read this slot
+    double *outer = ctx.h_ic_stage + (size_t)k * (kIcMaxOuter + 1);
     double a = log10(emin);
     outer[0] = emin;
     for (int i = 1; i <= N; i++) {
@@ -341,14 +355,23 @@ int ic_rows(Context &ctx, double z, double *d_out)
         outer[i] = pow(10.0, a);
     }
     double *d_outer = d_out + NB + 2;   // scratch tail reserved after the row
-    CROMA_CUDA(cudaMemcpyAsync(d_outer, outer.data(), (N + 1) * sizeof(double),
-                               cudaMemcpyHostToDevice, ctx.stream));
+    CROMA_CUDA(cudaMemcpyAsync(d_outer, outer, (N + 1) * sizeof(double), cudaMemcpyHostToDevice,
+                               ctx.stream));
+    CROMA_CUDA(cudaEventRecord(ctx.ic_stage_ev[k], ctx.stream));
     ic_row_kernel<<<NB + 2, 128, 0, ctx.stream>>>(ctx.icc, ctx.gt.s[1].p, ctx.h_pm1[1], ctx.h_pp1[1],
                                                   d_outer, N, z, d_out);
     CROMA_CUDA(cudaGetLastError());
-    // outer[] must stay alive until the copy is done
-    CROMA_CUDA(cudaStreamSynchronize(ctx.stream));
     return 0;
+}
+
+void free_ic_stage(Context &ctx)
+{
+    for (int k = 0; k < 2; k++) {
+        if (ctx.ic_stage_ev[k]) cudaEventDestroy(ctx.ic_stage_ev[k]);
+        ctx.ic_stage_ev[k] = nullptr;
+    }
+    if (ctx.h_ic_stage) cudaFreeHost(ctx.h_ic_stage);
+    ctx.h_ic_stage = nullptr;
 }
 
 }  // namespace croma
