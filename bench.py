@@ -36,10 +36,11 @@ NSNAP_TIMELINE = 100
 SEED = 20261203
 METRIC = "tracer-snapshot updates/s at <=1e-6 rel err vs FP64, chosen vs plain; p50/p99 latency"
 UNIT = "tracer-snapshot updates/s"
-# DRAM bytes (read + write) of one fused slot (proton + electron launches) per
-# tracer, from an ncu capture of this workload at 65,536 tracers
-# (profiles/fused_slot_kernel_batching_e_p_256.txt).
-NCU_DRAM_BYTES_PER_TRACER_SLOT = (143.05e6 + 83.32e6 + 278.07e6 + 103.90e6) / 65536
+# DRAM bytes (read + write) of one steps_kernel launch per tracer, mean of the
+# proton and electron launches of an ncu capture of this workload at 32,768
+# tracers (profiles/steps_factor_secondary_batching_e_p_256.txt); traffic
+# scales with the tracer count (every tracer moves its own rows).
+NCU_DRAM_BYTES_PER_TRACER_STEPS_LAUNCH = (3.289135e9 + 1.119739e9 + 4.397054e9 + 0.114189e9) / 2 / 32768
 
 
 def load_package():
@@ -84,7 +85,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -190,6 +191,21 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------- GPU arm
+def coeff_segments(cfg, nsub, allow=True):
+    """Coefficient segments of a tracer (largest power of two within the
+    segment cap and nsub / min_steps), as the schedule kernel derives them."""
+    if not allow or nsub <= 1 or cfg.coeff_interp_min_steps <= 0:
+        return 1
+    max_seg = max(1, cfg.coeff_interp_max_segments)
+    max_allowed = nsub // cfg.coeff_interp_min_steps
+    if max_allowed < 1:
+        return 1
+    seg = 1
+    while seg * 2 <= max_seg and seg * 2 <= max_allowed:
+        seg *= 2
+    return min(seg, nsub)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -316,33 +332,48 @@ def run_gpu_arm(args):
                     "alg_bytes_per_launch": per_launch,
                     "alg_bytes_rule": "per tracer-snapshot: nsub x 2 species x nb x 6 doubles"}
     else:
-        # The fused evolve keeps every row on chip, so its DRAM traffic is only the
-        # compulsory state, source and background; the bound is the FP64 pipe.
-        # Algorithmic flops are the reference's Thomas step per row per sub-step
-        # (RHS FMA, denominator FMA, back-substitution FMA, 2 divides: 9 flops +
-        # 2 divides, counted 11), summed over both species and every sub-step of
-        # the schedule.  Per-segment coefficient work is not counted.
+        # The steps kernel runs every sub-step with the spectrum and the factored
+        # rows in registers: the bound is the FP64 pipe.  Algorithmic flops are
+        # the reference's Thomas step per row per sub-step (RHS FMA, denominator
+        # FMA, back-substitution FMA, 2 divides: 9 flops + 2 divides, counted 11)
+        # over both species and every sub-step of the schedule.  Its DRAM traffic
+        # is the factored rows of each segment (written by the factor kernel),
+        # the spectra and the segment-start proton spectra.
         flops_per_snapshot = float(np.sum(nsub)) * nspecies * nb * 11.0
         per_launch = flops_per_snapshot * args.steps / max(1, evolve_n)
         avg_launch_ms = evolve_ms / max(1, evolve_n)
         achieved = per_launch / (avg_launch_ms / 1e3) / 1e12
         peak = native.fp64_peak(cfg.nb)
-        # compulsory bytes of one slot launch pair: both species' N read and
-        # written, the electron source row read, both backgrounds read
-        comp_bytes = nt * (nspecies * nb * 16 + nb * 8 + 2 * 8 * 8)
-        traffic = NCU_DRAM_BYTES_PER_TRACER_SLOT * nt if args.tracers == NTRACER else None
+        nseg = np.array([coeff_segments(cfg, int(n)) for n in sched["nsub"]], dtype=np.float64)
+        # bytes the steps launches must move: factored rows (3 x nb doubles per
+        # segment), N in and out, segment-start proton spectra (proton launch)
+        alg_bytes_launch = (float(np.sum(nseg)) * (3 * nb * 8) * nspecies + nt * nb * 16 * nspecies
+                            + float(np.sum(nseg)) * nb * 8) / nspecies
+        traffic = (NCU_DRAM_BYTES_PER_TRACER_STEPS_LAUNCH * nt
+                   if NCU_DRAM_BYTES_PER_TRACER_STEPS_LAUNCH and args.tracers == NTRACER else None)
+        _, npmin = fp.secondary_kernel()
+        sec_flops = float(np.sum(nseg)) * 2.0 * float(np.sum(nb - np.asarray(npmin))) * args.steps
         roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "traffic": traffic,
                     "peak_source": "measured live: croma_b200_fp64_peak (FMA chains on every SM)",
-                    "kernel": "fused_slot_kernel (proton + electron launches of one slot)",
+                    "kernel": "steps_kernel (one proton and one electron launch per snapshot)",
                     "launches": evolve_n, "kernel_ms_total": evolve_ms,
                     "share_of_step": evolve_ms / ms if ms > 0 else None,
                     "alg_flops_per_launch": per_launch,
                     "alg_flops_rule": "per tracer-snapshot: nsub x 2 species x nb x 11 (reference Thomas)",
-                    "hbm_view": {"compulsory_bytes_per_launch": comp_bytes,
-                                 "achieved_gbs": comp_bytes / (avg_launch_ms / 1e3) / 1e9,
+                    "hbm_view": {"alg_bytes_per_launch": alg_bytes_launch,
+                                 "achieved_gbs": alg_bytes_launch / (avg_launch_ms / 1e3) / 1e9,
                                  "peak_gbs": float(peaks.get("hbm_gbs", 6650.0)),
-                                 "peak_source": peak_kind}}
+                                 "peak_source": peak_kind},
+                    "other_kernels": {
+                        "factor_kernel": {"ms_total": coeff_ms, "launches": coeff_n,
+                                          "share_of_step": coeff_ms / ms if ms > 0 else None},
+                        "secondary_kernel": {"ms_total": sec_ms, "launches": sec_n,
+                                             "share_of_step": sec_ms / ms if ms > 0 else None,
+                                             "achieved_tflops": sec_flops / (sec_ms / 1e3) / 1e12
+                                             if sec_ms > 0 else None,
+                                             "frac": (sec_flops / (sec_ms / 1e3) / 1e12) / peak
+                                             if sec_ms > 0 else None}}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -28,8 +28,9 @@ __device__ __forceinline__ SegInfo seg_info(const Schedule &s, int t, int slot, 
     if (slot >= g.nseg) return g;
     g.nsub = s.nsub[t];
     const int non = s.non[t];
-    g.b = (int)(((long long)slot * g.nsub) / g.nseg);
-    g.e = (int)(((long long)(slot + 1) * g.nsub) / g.nseg);
+    // slot < 64 and nsub <= 1e6 (the sub-step ceiling), so 32-bit products suffice
+    g.b = (slot * g.nsub) / g.nseg;
+    g.e = ((slot + 1) * g.nsub) / g.nseg;
     g.steps = g.e - g.b;
     if (g.steps <= 0) return g;
     g.active = 1;

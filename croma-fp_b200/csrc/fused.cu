@@ -50,7 +50,10 @@ constexpr int kFacWarps = 8;         // warps per factor-kernel block
 // Grid tables of one species staged in shared memory by the factor kernel.
 // X0..X4: protons expE, cp_Ep, cp_inv2mpkin, cp_inv_betap2, sig_eff;
 // electrons ce_inv_beta2, ce_logp and the shared IC rows of z_curr, z_next.
-enum { TB_P, TB_P2, TB_CUT, TB_2P, TB_DXF, TB_X0, TB_X1, TB_X2, TB_X3, TB_X4, kTab };
+enum { TB_P, TB_P2, TB_CUT, TB_2P, TB_DXF, TB_X0, TB_X1, TB_X2, TB_X3, TB_X4,
+       TB_IDX, TB_IDXL, TB_IDXR,   // 1/dp, 1/(p[m]-p[m-1]), 1/(p[m+1]-p[m]) in swizzled order
+       kTab };
+constexpr int kTabStride = (NB > kSw ? NB : kSw);   // doubles per staged table
 
 struct FusedParams {
     SnapArgs a;              // spectra and sources cell-major [tracer][nb]
@@ -126,42 +129,42 @@ struct SegTerms {
     // tables staged in shared memory (tab, kTab arrays of nb)
     __device__ __forceinline__ void at(const double *tab, int j, double &B, double &C, double &dT) const
     {
-        const double p = tab[TB_P * NB + j];
-        const double p2 = tab[TB_P2 * NB + j];
-        const double cut = tab[TB_CUT * NB + j];
+        const double p = tab[TB_P * kTabStride + j];
+        const double p2 = tab[TB_P2 * kTabStride + j];
+        const double cut = tab[TB_CUT * kTabStride + j];
         double D;
         if (!dpp_fill) D = p2 * (1.0 / (4.0 * 1.0e+5));
-        else if (S == 0) D = p2 * dpp_inv * tab[TB_X0 * NB + j] * cut;
+        else if (S == 0) D = p2 * dpp_inv * tab[TB_X0 * kTabStride + j] * cut;
         else D = p2 * dpp_inv * cut;
         D *= dpp_scale;
         double radp;
         if (S == 0) {
-            const double xp = tab[TB_X1 * NB + j] * inv_kbt;
+            const double xp = tab[TB_X1 * kTabStride + j] * inv_kbt;
             const double xe = xp * (kMe / kMp);
             const double sum = coulomb_kernel_fast(xe) + coulomb_kernel_fast(xp) * (kMe / kMp);
-            const double thermal = 1.0 - kbt * tab[TB_X2 * NB + j];
+            const double thermal = 1.0 - kbt * tab[TB_X2 * kTabStride + j];
             const double coul = (thermal < 0.0)
                 ? 0.0
-                : kGyr * kC / (kMp * kGeV) * sum * n_gas * tab[TB_X3 * NB + j] * thermal * 3.5e-29;
+                : kGyr * kC / (kMp * kGeV) * sum * n_gas * tab[TB_X3 * kTabStride + j] * thermal * 3.5e-29;
             radp = coul + adiab * p;
-            dT = tab[TB_X4 * NB + j] * dt_over_tloss_pref;
+            dT = tab[TB_X4 * kTabStride + j] * dt_over_tloss_pref;
         } else {
             double r0, r1;
             if (ric_stride == 0) {
-                r0 = tab[TB_X2 * NB + j];
-                r1 = tab[TB_X3 * NB + j];
+                r0 = tab[TB_X2 * kTabStride + j];
+                r1 = tab[TB_X3 * kTabStride + j];
             } else {
                 r0 = ric[j * ric_stride];
                 r1 = ric_next[j * ric_stride];
             }
             const double r = interp ? lerp(r0, r1, alpha) : r0;
             // log(p / n) as log p - log n: the per-bin logarithm is tabulated
-            const double coulomb = coulomb_coeff * (1.0 + (tab[TB_X1 * NB + j] - log_n) * (1.0 / 74.8)) *
-                                   tab[TB_X0 * NB + j];
+            const double coulomb = coulomb_coeff * (1.0 + (tab[TB_X1 * kTabStride + j] - log_n) * (1.0 / 74.8)) *
+                                   tab[TB_X0 * kTabStride + j];
             radp = synch_coeff * p2 + r + coulomb + adiab * p;
             dT = dtT_e;
         }
-        B = radp - tab[TB_2P * NB + j] * D;
+        B = radp - tab[TB_2P * kTabStride + j] * D;
         C = D;
     }
 };
@@ -229,7 +232,7 @@ __device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int la
             const double cl = sm.C[swz(j)];
             if (fabs(cl) > 1.0e-200) {
                 const double w = (sm.B[swz(j)] + sm.B[swz(j + 1)]) / (cl + sm.C[swz(j + 1)]) *
-                                 tab[TB_DXF * NB + j];
+                                 tab[TB_DXF * kTabStride + j];
                 face_weights_fast(w, wp, wm);
             }
         }
@@ -244,13 +247,13 @@ __device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int la
 #pragma unroll
     for (int r = 0; r < kR; r++) {
         const int m = row0 + r;
-        const double k = T.dt * st.inv_dx[m];
+        const double k = T.dt * tab[TB_IDX * kTabStride + r * 33 + lane];
         const double Cm = sm.C[r * 33 + lane], Bm = sm.B[r * 33 + lane], Dm = sm.D[r * 33 + lane];
         double av = 0.0, bv, cv = 0.0;
         if (m == 0) {
             const double nC = sm.C[swz(1)], nB = sm.B[swz(1)];
             if (fabs(Cm) > 1.0e-200) {
-                const double cm12 = 0.5 * (Cm + nC) * st.inv_dxr[0];
+                const double cm12 = 0.5 * (Cm + nC) * tab[TB_IDXR * kTabStride + r * 33 + lane];
                 bv = 1.0 + k * (0.0 + cm12 * sm.Wm[swz(0)]) + Dm;
                 cv = k * cm12 * sm.Wp[swz(0)];
             } else {
@@ -262,7 +265,7 @@ __device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int la
             const double wpm = sm.Wp[swz(m - 1)], wmm = sm.Wm[swz(m - 1)];
             if (m == NB - 1) {
                 if (fabs(Cm) > 1.0e-200) {
-                    const double cm_12 = 0.5 * (Cm + pC) * st.inv_dxl[m];
+                    const double cm_12 = 0.5 * (Cm + pC) * tab[TB_IDXL * kTabStride + r * 33 + lane];
                     av = k * cm_12 * wmm;
                     bv = 1.0 + k * (cm_12 * wpm) + Dm;
                     if (isnan(av)) err |= kErrCcNan;
@@ -276,8 +279,8 @@ __device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int la
             } else {
                 const double nC = sm.C[swz(m + 1)], nB = sm.B[swz(m + 1)];
                 if (fabs(Cm) > 1.0e-200) {
-                    const double cm_12 = 0.5 * (Cm + pC) * st.inv_dxl[m];
-                    const double cm12 = 0.5 * (Cm + nC) * st.inv_dxr[m];
+                    const double cm_12 = 0.5 * (Cm + pC) * tab[TB_IDXL * kTabStride + r * 33 + lane];
+                    const double cm12 = 0.5 * (Cm + nC) * tab[TB_IDXR * kTabStride + r * 33 + lane];
                     av = k * cm_12 * wmm;
                     bv = 1.0 + k * (cm_12 * wpm + cm12 * sm.Wm[swz(m)]) + Dm;
                     cv = k * cm12 * sm.Wp[swz(m)];
@@ -357,38 +360,41 @@ __global__ void __launch_bounds__(kFacWarps * 32, (NB <= 256 ? 2 : 1)) factor_ke
 {
     extern __shared__ double4 smem_raw[];
     double *tab = reinterpret_cast<double *>(smem_raw);
-    WarpSmem *smem = reinterpret_cast<WarpSmem *>(tab + kTab * NB);
+    WarpSmem *smem = reinterpret_cast<WarpSmem *>(tab + kTab * kTabStride);
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const SnapArgs &a = P.a;
     const SpeciesTables &st = P.gt.s[S];
     for (int i = threadIdx.x; i < NB; i += blockDim.x) {
-        tab[TB_P * NB + i] = st.p[i];
-        tab[TB_P2 * NB + i] = st.p2[i];
-        tab[TB_CUT * NB + i] = st.exp_cut[i];
-        tab[TB_2P * NB + i] = st.two_over_p[i];
-        tab[TB_DXF * NB + i] = st.dxf[i];
+        tab[TB_P * kTabStride + i] = st.p[i];
+        tab[TB_P2 * kTabStride + i] = st.p2[i];
+        tab[TB_CUT * kTabStride + i] = st.exp_cut[i];
+        tab[TB_2P * kTabStride + i] = st.two_over_p[i];
+        tab[TB_DXF * kTabStride + i] = st.dxf[i];
         if (S == 0) {
-            tab[TB_X0 * NB + i] = st.expE[i];
-            tab[TB_X1 * NB + i] = P.gt.cp_Ep[i];
-            tab[TB_X2 * NB + i] = P.gt.cp_inv2mpkin[i];
-            tab[TB_X3 * NB + i] = P.gt.cp_inv_betap2[i];
-            tab[TB_X4 * NB + i] = P.gt.sig_eff[i];
+            tab[TB_X0 * kTabStride + i] = st.expE[i];
+            tab[TB_X1 * kTabStride + i] = P.gt.cp_Ep[i];
+            tab[TB_X2 * kTabStride + i] = P.gt.cp_inv2mpkin[i];
+            tab[TB_X3 * kTabStride + i] = P.gt.cp_inv_betap2[i];
+            tab[TB_X4 * kTabStride + i] = P.gt.sig_eff[i];
         } else {
-            tab[TB_X0 * NB + i] = P.gt.ce_inv_beta2[i];
-            tab[TB_X1 * NB + i] = P.gt.ce_logp[i];
-            tab[TB_X2 * NB + i] = (P.ic_stride == 0) ? a.ic_curr[i] : 0.0;
-            tab[TB_X3 * NB + i] = (P.ic_stride == 0) ? a.ic_next[i] : 0.0;
-            tab[TB_X4 * NB + i] = 0.0;
+            tab[TB_X0 * kTabStride + i] = P.gt.ce_inv_beta2[i];
+            tab[TB_X1 * kTabStride + i] = P.gt.ce_logp[i];
+            tab[TB_X2 * kTabStride + i] = (P.ic_stride == 0) ? a.ic_curr[i] : 0.0;
+            tab[TB_X3 * kTabStride + i] = (P.ic_stride == 0) ? a.ic_next[i] : 0.0;
+            tab[TB_X4 * kTabStride + i] = 0.0;
         }
+        tab[TB_IDX * kTabStride + swz(i)] = st.inv_dx[i];
+        tab[TB_IDXL * kTabStride + swz(i)] = st.inv_dxl[i];
+        tab[TB_IDXR * kTabStride + swz(i)] = st.inv_dxr[i];
     }
     __syncthreads();
-    const long long total = (long long)(P.g1 - P.g0) * P.sets * P.nt;
-    const long long stride = (long long)gridDim.x * kFacWarps;
+    const int total = (P.g1 - P.g0) * P.sets * P.nt;   // < 2^31, checked on the host
+    const int stride = gridDim.x * kFacWarps;
 #pragma unroll 1
-    for (long long u = (long long)blockIdx.x * kFacWarps + w; u < total; u += stride) {
-        const int tl = (int)(u % P.nt);
-        const int rest = (int)(u / P.nt);
+    for (int u = blockIdx.x * kFacWarps + w; u < total; u += stride) {
+        const int tl = u % P.nt;
+        const int rest = u / P.nt;
         const int set = rest % P.sets, gi = rest / P.sets;
         const int t = P.t0 + tl;
         const SegInfo g = segment_of(P, t, P.g0 + gi);
@@ -424,6 +430,9 @@ struct Coef {
     double q[kR];        // c_i / d_i      (back substitution)
     double sd[SRC ? kR : 1];  // dt * source_i / d_i
     double hk[5], qk[5];
+    // products of h over the lower and upper half of the lane's rows, and of
+    // q likewise: the local passes run as two half-length chains
+    double hlo, hhi, qlo, qhi;
 };
 
 template <bool SRC>
@@ -446,12 +455,19 @@ __device__ __forceinline__ void load_coef(Coef<SRC> &F, const double *fac, const
 #pragma unroll
         for (int r = 0; r < kR; r++) F.sd[r] = (dt * src[row0 + r]) * F.inv[r];
     }
-    double H = 1.0, Q = 1.0;
+    double hlo = 1.0, hhi = 1.0, qlo = 1.0, qhi = 1.0;
 #pragma unroll
-    for (int r = 0; r < kR; r++) {
-        H *= F.h[r];
-        Q *= F.q[r];
+    for (int r = 0; r < kR / 2; r++) {
+        hlo *= F.h[r];
+        qlo *= F.q[r];
+        hhi *= F.h[r + kR / 2];
+        qhi *= F.q[r + kR / 2];
     }
+    F.hlo = hlo;
+    F.hhi = hhi;
+    F.qlo = qlo;
+    F.qhi = qhi;
+    double H = hlo * hhi, Q = qlo * qhi;
 #pragma unroll
     for (int lv = 0; lv < 5; lv++) {
         const int off = 1 << lv;
@@ -465,34 +481,55 @@ __device__ __forceinline__ void load_coef(Coef<SRC> &F, const double *fac, const
 
 // One implicit sub-step: N <- M^{-1} (N + dt src) with the factored M.
 // A shuffle from a lane outside the warp returns the caller's own (finite)
-// value, which the zero multipliers discard exactly.
+// value, which the zero multipliers discard exactly.  Each local pass runs
+// as two independent half-length chains joined by one multiply-add, and the
+// second pass seeds its upper (lower) half from the scanned carry directly,
+// so no dependent chain is longer than half the lane's rows plus one.
 template <bool SRC>
 __device__ __forceinline__ void substep(const Coef<SRC> &F, double N[kR])
 {
-    double acc = 0.0;
+    constexpr int H2 = kR / 2;
+    // forward: z_i = y_i + h_i z_{i-1}, y = N / d + dt src / d
+    double alo = 0.0, ahi = 0.0;
 #pragma unroll
-    for (int r = 0; r < kR; r++) {
+    for (int r = 0; r < H2; r++) {
         N[r] = SRC ? fma(N[r], F.inv[r], F.sd[r]) : N[r] * F.inv[r];
-        acc = fma(F.h[r], acc, N[r]);
+        N[r + H2] = SRC ? fma(N[r + H2], F.inv[r + H2], F.sd[r + H2]) : N[r + H2] * F.inv[r + H2];
+        alo = fma(F.h[r], alo, N[r]);
+        ahi = fma(F.h[r + H2], ahi, N[r + H2]);
     }
+    double acc = fma(F.hhi, alo, ahi);
 #pragma unroll
     for (int lv = 0; lv < 5; lv++) acc = fma(F.hk[lv], sup(acc, 1 << lv), acc);
-    double prev = sup(acc, 1);
+    const double cin = sup(acc, 1);
+    double plo = cin, phi = fma(F.hlo, cin, alo);
 #pragma unroll
-    for (int r = 0; r < kR; r++) {
-        prev = fma(F.h[r], prev, N[r]);
-        N[r] = prev;
+    for (int r = 0; r < H2; r++) {
+        plo = fma(F.h[r], plo, N[r]);
+        phi = fma(F.h[r + H2], phi, N[r + H2]);
+        N[r] = plo;
+        N[r + H2] = phi;
     }
-    acc = 0.0;
+    // back substitution: x_i = z_i + q_i x_{i+1}
+    alo = 0.0;
+    ahi = 0.0;
 #pragma unroll
-    for (int r = kR - 1; r >= 0; r--) acc = fma(F.q[r], acc, N[r]);
+    for (int r = H2 - 1; r >= 0; r--) {
+        alo = fma(F.q[r], alo, N[r]);
+        ahi = fma(F.q[r + H2], ahi, N[r + H2]);
+    }
+    acc = fma(F.qlo, ahi, alo);
 #pragma unroll
     for (int lv = 0; lv < 5; lv++) acc = fma(F.qk[lv], sdn(acc, 1 << lv), acc);
-    prev = sdn(acc, 1);
+    const double cout = sdn(acc, 1);
+    phi = cout;
+    plo = fma(F.qhi, cout, ahi);
 #pragma unroll
-    for (int r = kR - 1; r >= 0; r--) {
-        prev = fma(F.q[r], prev, N[r]);
-        N[r] = prev;
+    for (int r = H2 - 1; r >= 0; r--) {
+        phi = fma(F.q[r + H2], phi, N[r + H2]);
+        plo = fma(F.q[r], plo, N[r]);
+        N[r + H2] = phi;
+        N[r] = plo;
     }
 }
 
@@ -591,76 +628,151 @@ __global__ void __launch_bounds__(128) eta_scale_kernel(FusedParams P, double *e
 }
 
 // Secondary source of every segment of the chunk, cell-major:
-// inje[gi][tl][je] = Gyr n_gas(t, segment) sum_{jp} N_p[gi][tl][jp] fqe[jp][je]
-//                    + qepri[t][je],
-// over the rows m = gi * nt + tl.  64 x 64 output tile, 16 x 16 threads,
-// 4 x 4 outputs each; the proton index runs upward from the first bin with a
-// nonzero weight in the tile.
-__global__ void __launch_bounds__(256) secondary_kernel(FusedParams P)
+// inje[m][je] = Gyr n_gas(t, segment) sum_{jp} N_p[m][jp] fqe[jp][je] + qepri[t][je]
+// over the rows m = gi * nt + tl of np_seg.  An FP64 GEMM on the CUDA cores:
+// 128 x 64 output tile per 256-thread block, 8 x 4 outputs per thread,
+// k-tiles of 16 double-buffered in shared memory with the next tile
+// prefetched into registers.  The proton index starts at the first k-tile
+// holding a nonzero weight for the block's columns; fqe is zero below
+// np_min_qe[je] (prepare_secondary_kernel_flat, src/fp_shared_core.c:1453-1506),
+// so the rounded-down start adds exact zeros only.
+constexpr int kGM = 128, kGN = 64, kGK = 16, kGPad = 4;
+
+struct GemmSmem {
+    double A[2][kGK][kGM + kGPad];   // transposed: [k][m]
+    double B[2][kGK][kGN];
+};
+
+__global__ void __launch_bounds__(256, 2) secondary_kernel(FusedParams P)
 {
-    __shared__ double sN[64][17];
-    __shared__ double sF[16][64];
+    extern __shared__ double4 smem_raw[];
+    GemmSmem &sm = *reinterpret_cast<GemmSmem *>(smem_raw);
     const SnapArgs &a = P.a;
-    const long long nrows = (long long)(P.g1 - P.g0) * P.nt;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 16 + tx;
-    const long long m0 = (long long)blockIdx.x * 64;
-    const int je0 = blockIdx.y * 64;
+    const int nrows = (P.g1 - P.g0) * P.nt;   // < 2^31, checked on the host
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    // column tile fastest, so the NB / kGN blocks of one row tile run together
+    // and read their A tile from L2
+    const int n0 = (int)(blockIdx.x % (NB / kGN)) * kGN;
+    const int m0 = (int)(blockIdx.x / (NB / kGN)) * kGM;
     int jstart = NB;
-    for (int i = 0; i < 64 && je0 + i < NB; i++) jstart = min(jstart, P.np_min_qe[je0 + i]);
+    for (int i = 0; i < kGN && n0 + i < NB; i++) jstart = min(jstart, P.np_min_qe[n0 + i]);
     jstart = max(jstart, P.gt.fqe_jp0);
-    double acc[4][4];
+    const int kbeg = (jstart / kGK) * kGK;
+
+    // loader roles: A row lm, k-half lh (8 doubles); B row lk, 4 columns ln
+    const int lm = tid >> 1, lh = tid & 1;
+    const int lk = tid >> 4, ln = (tid & 15) * 4;
+    const bool arow = (m0 + lm) < nrows;
+    const double *Arow = P.np_seg + (size_t)(m0 + lm) * NB + lh * 8;
+    const double *Bp = P.gt.fqe + n0 + ln;
+    double ra[8], rb[4];
+    auto fetch = [&](int k0) {
+        if (arow) {
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+            for (int i = 0; i < 8; i += 2) {
+                const double2 v = __ldcs(reinterpret_cast<const double2 *>(Arow + k0 + i));
+                ra[i] = v.x;
+                ra[i + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; i++) ra[i] = 0.0;
+        }
+        const double2 b0 = __ldg(reinterpret_cast<const double2 *>(Bp + (size_t)(k0 + lk) * NB));
+        const double2 b1 = __ldg(reinterpret_cast<const double2 *>(Bp + (size_t)(k0 + lk) * NB + 2));
+        rb[0] = b0.x; rb[1] = b0.y; rb[2] = b1.x; rb[3] = b1.y;
+    };
+    auto stash = [&](int buf) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) sm.A[buf][lh * 8 + i][lm] = ra[i];
+        *reinterpret_cast<double2 *>(&sm.B[buf][lk][ln]) = make_double2(rb[0], rb[1]);
+        *reinterpret_cast<double2 *>(&sm.B[buf][lk][ln + 2]) = make_double2(rb[2], rb[3]);
+    };
+
+    double acc[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-    for (int k0 = jstart; k0 < NB; k0 += 16) {
-        for (int q = tid; q < 64 * 16; q += 256) {
-            const int tt = q / 16, kk = q % 16;
-            const long long m = m0 + tt;
-            const int jp = k0 + kk;
-            sN[tt][kk] = (m < nrows && jp < NB) ? P.np_seg[(size_t)m * NB + jp] : 0.0;
-            const int r = q / 64, col = q % 64;
-            const int jp2 = k0 + r;
-            sF[r][col] = (jp2 < NB && je0 + col < NB) ? P.gt.fqe[(size_t)jp2 * NB + je0 + col] : 0.0;
-        }
-        __syncthreads();
-        const int kmax = min(16, NB - k0);
-        for (int kk = 0; kk < kmax; kk++) {
-            double n[4], f[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) n[i] = sN[ty + 16 * i][kk];
-#pragma unroll
-            for (int j = 0; j < 4; j++) f[j] = sF[kk][tx + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] = fma(n[i], f[j], acc[i][j]);
-        }
-        __syncthreads();
+
+    int buf = 0;
+    if (kbeg < NB) {
+        fetch(kbeg);
+        stash(0);
     }
+    __syncthreads();
+#pragma unroll 1
+    for (int k0 = kbeg; k0 < NB; k0 += kGK) {
+        const bool more = k0 + kGK < NB;
+        if (more) fetch(k0 + kGK);
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const long long m = m0 + ty + 16 * i;
+        for (int kk = 0; kk < kGK; kk++) {
+            double av[8], bv[4];
+#pragma unroll
+            for (int i = 0; i < 8; i += 2) {
+                const double2 v = *reinterpret_cast<const double2 *>(&sm.A[buf][kk][ty * 8 + i]);
+                av[i] = v.x;
+                av[i + 1] = v.y;
+            }
+            const double2 b0 = *reinterpret_cast<const double2 *>(&sm.B[buf][kk][tx * 4]);
+            const double2 b1 = *reinterpret_cast<const double2 *>(&sm.B[buf][kk][tx * 4 + 2]);
+            bv[0] = b0.x; bv[1] = b0.y; bv[2] = b1.x; bv[3] = b1.y;
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        }
+        if (more) stash(buf ^ 1);
+        __syncthreads();
+        buf ^= 1;
+    }
+
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int m = m0 + ty * 8 + i;
         if (m >= nrows) continue;
-        const int gi = (int)(m / P.nt), tl = (int)(m % P.nt);
+        const int gi = m / P.nt, tl = m - gi * P.nt;
         const int t = P.t0 + tl;
         const SegInfo g = segment_of(P, t, P.g0 + gi);
         if (!g.active) continue;
         const double ng = (g.nseg > 1) ? lerp(a.bg_curr[t], a.bg_next[t], g.alpha) : a.bg_curr[t];
+        const int je = n0 + tx * 4;
+        double q[4] = {0.0, 0.0, 0.0, 0.0};
+        if (a.qepri) {
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int je = je0 + tx + 16 * j;
-            if (je >= NB) continue;
-            const double q = a.qepri ? a.qepri[(size_t)t * NB + je] : 0.0;
-            P.inje[(size_t)m * NB + je] = acc[i][j] * kGyr * ng + q;
+            for (int j = 0; j < 4; j++) q[j] = a.qepri[(size_t)t * NB + je + j];
         }
+        double *o = P.inje + (size_t)m * NB + je;
+        *reinterpret_cast<double2 *>(o) =
+            make_double2(acc[i][0] * kGyr * ng + q[0], acc[i][1] * kGyr * ng + q[1]);
+        *reinterpret_cast<double2 *>(o + 2) =
+            make_double2(acc[i][2] * kGyr * ng + q[2], acc[i][3] * kGyr * ng + q[3]);
     }
+}
+
+cudaError_t launch_secondary(Context &ctx, const FusedParams &P)
+{
+    constexpr size_t smem = sizeof(GemmSmem);
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(secondary_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    const long long rows = (long long)(P.g1 - P.g0) * P.nt;
+    if (rows > 0x7fffffffLL) return cudaErrorInvalidValue;
+    const long long blocks = (rows + kGM - 1) / kGM * (NB / kGN);
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+    secondary_kernel<<<(unsigned)blocks, 256, smem, ctx.stream>>>(P);
+    return cudaGetLastError();
 }
 
 template <int S>
 cudaError_t launch_factor(Context &ctx, const FusedParams &P)
 {
-    constexpr size_t smem = (size_t)kTab * NB * sizeof(double) + kFacWarps * sizeof(WarpSmem);
+    constexpr size_t smem = (size_t)kTab * kTabStride * sizeof(double) + kFacWarps * sizeof(WarpSmem);
     static int resident = 0;   // blocks per SM, per instantiation; found before the first launch
     if (!resident) {
         cudaError_t e = cudaFuncSetAttribute(factor_kernel<S>,
@@ -674,6 +786,7 @@ cudaError_t launch_factor(Context &ctx, const FusedParams &P)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const long long warps = (long long)(P.g1 - P.g0) * P.sets * P.nt;
+    if (warps > 0x7fffffffLL) return cudaErrorInvalidValue;
     long long blocks = (warps + kFacWarps - 1) / kFacWarps;
     const long long full = (long long)nsm * resident;
     if (blocks > full) blocks = full;
@@ -771,10 +884,8 @@ static int fused_range(Context &ctx, FusedParams &P, int g0, int g1)
         ctx.last_launches += 1;
     }
     if (secondaries) {
-        const long long rows = (long long)(g1 - g0) * P.nt;
-        dim3 sg((unsigned)((rows + 63) / 64), (NB + 63) / 64), sb(16, 16);
         timed_begin(ctx, kKindSecondary, &ev);
-        secondary_kernel<<<sg, sb, 0, ctx.stream>>>(P);
+        CROMA_CUDA(launch_secondary(ctx, P));
         timed_end(ctx, kKindSecondary, ev);
         ctx.last_launches += 1;
     }
