@@ -80,3 +80,32 @@ def config4(**kw) -> RunConfig:
                 pemin=-1.0, pemax=6.0, dpp_mode="asa", nsub_max=500)
     base.update(kw)
     return RunConfig(**base)
+
+
+DSA_MODELS = ("KR07", "KR07r", "KR13", "KR13r", "CS14", "CS14r", "Ryu19", "Ryu19r")
+DSA_MODE = {"off": 0, "tracer_state": 1, "tracer_source": 2}
+DSA_REACC = {"off": 0, "positive_delta": 1, "drury83": 2}
+
+
+@dataclasses.dataclass
+class DsaParams:
+    """DSA injection parameters, mirroring the reference's globals
+    (src/params.c:96-113, mu_mol :127) and the DSA grid bounds of
+    src/tracer_fp.c:841 (dsa_init_grid(..., -3.0, -3.0)).  Efficiency models
+    are indices into DSA_MODELS (the DSAModelID order)."""
+    eta_model_initial: int = 6        # Ryu19
+    eta_model_reacc: int = 7          # Ryu19r
+    chi_p: float = 3.5
+    chi_e: float = 3.5
+    k_ep: float = 1.0e-2
+    pmax_p_mc: float = 1.0e6
+    pmax_e_mc: float = 1.0e5
+    min_mach: float = 1.5
+    gamma_gas: float = 5.0 / 3.0
+    xcr_pmin_pmc: float = 1.0
+    reacc_eta_cap: float = 0.0
+    mu_mol: float = 0.59
+    pmin_dsa_p_log10: float = -3.0
+    pmin_dsa_e_log10: float = -3.0
+    inject_species: int = 0           # 0 both, 1 electrons, 2 protons
+

@@ -86,6 +86,29 @@ def background(ntracer: int, snapshot: int, seed: int, mach_limit: float = 0.5) 
     return out
 
 
+def shocks(bg: np.ndarray, snapshot: int, seed: int, fraction: float = 0.05,
+           merged: bool = False) -> dict:
+    """Seeded shock fields for one snapshot: each tracer is shocked with
+    probability `fraction` (Bernoulli per tracer-snapshot) with Mach number
+    U[2, 5]; the upstream temperature and density are the tracer's own
+    background (kbt, n_gas), density_unit = 1.  `merged` gives the merged-DSA
+    form (trigger, Mach, pre-shock density, kinetic energy flux 0.5 rho u^3 at
+    u = M cs) instead of (mach, prestemp, presden, side code)."""
+    n = bg.shape[1]
+    rng = _rng(seed ^ 0x5A5A5A5A, snapshot)
+    hit = rng.uniform(size=n) < fraction
+    mach = np.where(hit, rng.uniform(2.0, 5.0, n), 0.0)
+    temp = bg[1] * 1.0e9 / KB_EV
+    rho = bg[0] * (1.6e-24 * MU_MOL)
+    if merged:
+        u = mach * bg[6]
+        return {"has_dsa": 1, "dsa_trigger": hit.astype(np.float64), "dsa_mach": mach,
+                "dsa_pre_density": rho, "dsa_flux_cgs": 0.5 * rho * u * u * u,
+                "shock_side_code": np.where(hit, 1.0, 99.0)}
+    return {"has_dsa": 0, "mach": mach, "prestemp": temp, "presden": rho,
+            "shock_side_code": np.where(hit, 1.0, 99.0)}
+
+
 def _cosmic_time_gyr(z: float, h0: float = 70.0, om: float = 0.3) -> float:
     """Age of a flat LCDM universe at redshift z, in Gyr."""
     ol = 1.0 - om

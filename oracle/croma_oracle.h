@@ -109,6 +109,36 @@ int or_snapshot_with_ic(const OrCtx *ctx, int ntracer, const double *bg_curr,
 
 void or_set_threads(int n);
 
+/* ---- DSA injection (croma_oracle_dsa.c) ---- */
+enum { OR_DSA_OFF = 0, OR_DSA_STATE = 1, OR_DSA_SOURCE = 2 };          /* TracerDsaInjectionMode */
+enum { OR_REACC_OFF = 0, OR_REACC_POSITIVE = 1, OR_REACC_DRURY83 = 2 }; /* TracerDsaReaccMode */
+
+/* The DSA run parameters (src/params.c:96-113 and mu_mol, :127); model ids
+ * follow DSAModelID: 0 KR07, 1 KR07r, 2 KR13, 3 KR13r, 4 CS14, 5 CS14r,
+ * 6 Ryu19, 7 Ryu19r.  inject_species: 0 both, 1 electrons, 2 protons. */
+typedef struct {
+    int eta_model_initial, eta_model_reacc;
+    double chi_p, chi_e, k_ep, pmax_p_mc, pmax_e_mc;
+    double min_mach, gamma_gas, xcr_pmin_pmc, reacc_eta_cap, mu_mol;
+    double pmin_dsa_p_log10, pmin_dsa_e_log10;   /* dsa_init_grid bounds */
+    int inject_species;
+} OrDsaParams;
+
+/* Per-tracer shock fields [ntracer] (TracerFpRawBackgroundSlot,
+ * include/tracer_fp_types.h:292-313); optional arrays may be NULL. */
+typedef struct {
+    const double *mach, *prestemp, *presden, *pre_density_cgs, *upstream_speed_cgs, *shock_side_code;
+    const double *dsa_trigger, *dsa_mach, *dsa_pre_density, *dsa_flux_cgs;
+    int has_dsa;
+} OrShockFields;
+
+/* tracer_fp_apply_dsa_tracer_injection_snapshot on cell-major state. */
+int or_dsa_inject(const OrDsaParams *prm, int nb, const double *p_p, const double *dp_p,
+                  const double *p_e, const double *dp_e, const OrShockFields *sh, int ntracer,
+                  const double *mass_msun, double density_unit, double dt_gyr, int mode,
+                  int reacc_mode, double *crp, double *cre, double *qpi, double *qepri,
+                  unsigned char *dis, int *ninjected);
+
 #ifdef __cplusplus
 }
 #endif

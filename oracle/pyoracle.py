@@ -45,6 +45,39 @@ class _RefConfig(C.Structure):
                 ("t_acc_off_gyr", _d), ("nthreads", _i)]
 
 
+class _DsaParams(C.Structure):
+    _fields_ = [("eta_model_initial", _i), ("eta_model_reacc", _i), ("chi_p", _d), ("chi_e", _d),
+                ("k_ep", _d), ("pmax_p_mc", _d), ("pmax_e_mc", _d), ("min_mach", _d),
+                ("gamma_gas", _d), ("xcr_pmin_pmc", _d), ("reacc_eta_cap", _d), ("mu_mol", _d),
+                ("pmin_dsa_p_log10", _d), ("pmin_dsa_e_log10", _d), ("inject_species", _i)]
+
+
+SHOCK_FIELDS = ("mach", "prestemp", "presden", "pre_density_cgs", "upstream_speed_cgs",
+                "shock_side_code", "dsa_trigger", "dsa_mach", "dsa_pre_density", "dsa_flux_cgs")
+
+
+class _ShockFields(C.Structure):
+    _fields_ = [(n, _vp) for n in SHOCK_FIELDS] + [("has_dsa", _i)]
+
+
+def _dsa_structs(params, shocks):
+    """ctypes structs for DSA parameters (an object with the _DsaParams
+    field names) and shock fields (dict of [ntracer] arrays, missing = NULL,
+    plus 'has_dsa'); the arrays are kept alive in the returned tuple."""
+    prm = _DsaParams()
+    for name, _ in _DsaParams._fields_:
+        setattr(prm, name, getattr(params, name))
+    keep = {}
+    sh = _ShockFields()
+    for n in SHOCK_FIELDS:
+        a = shocks.get(n)
+        if a is not None:
+            keep[n] = np.ascontiguousarray(a, dtype=np.float64)
+            setattr(sh, n, keep[n].ctypes.data)
+    sh.has_dsa = int(shocks.get("has_dsa", 0))
+    return prm, sh, keep
+
+
 def _fill(struct, cfg, extra=None):
     s = struct()
     for name, _ in struct._fields_:
@@ -100,6 +133,20 @@ class _Common:
             raise RuntimeError(f"nsub failed: {err}")
         return nsub, tgt, non, cap
 
+    def dsa_inject(self, params, shocks, mass, density_unit, dt_gyr, mode, reacc_mode, crp, cre,
+                   qpi=None, qepri=None, dis=None):
+        """tracer_fp_apply_dsa_tracer_injection_snapshot on cell-major arrays
+        (modified in place).  Returns the number of tracers injected."""
+        prm, sh, keep = _dsa_structs(params, shocks)
+        n = crp.shape[0]
+        nin = _i()
+        rc = self._dsa(C.byref(prm), C.byref(sh), n, _ptr(_as_d(mass)), float(density_unit),
+                       float(dt_gyr), int(mode), int(reacc_mode), _ptr(crp), _ptr(cre), _ptr(qpi),
+                       _ptr(qepri), _ptr(dis), C.byref(nin))
+        if rc != 0:
+            raise RuntimeError(f"dsa_inject failed: {rc}")
+        return nin.value
+
     def buckets(self, nsub: np.ndarray, non: np.ndarray):
         n = nsub.size
         bid = np.empty(n, np.int32); idx = np.empty(n, np.int32)
@@ -140,6 +187,8 @@ class Oracle(_Common):
         L.or_snapshot_with_ic.argtypes = [_vp, _i, _D, _D, _D, _D, _i, _d, _d, _D, _D, _vp, _vp,
                                           _D, _D, _I, _I, _I, C.POINTER(_i)]
         L.or_set_threads.argtypes = [_i]
+        L.or_dsa_inject.argtypes = [_vp, _i, _vp, _vp, _vp, _vp, _vp, _i, _vp, _d, _d, _i, _i,
+                                    _vp, _vp, _vp, _vp, _vp, _vp]
         self.cfg = cfg
         self.nb = cfg.nb
         p = _fill(_Params, cfg)
@@ -161,6 +210,14 @@ class Oracle(_Common):
     def _sec(self, f, m): return self.lib.or_get_secondary_kernel(self.ctx, f, m)
     def _nsub(self, *a): return self.lib.or_nsub(self.ctx, *a)
     def _buckets(self, *a): return self.lib.or_buckets(*a)
+
+    def _dsa(self, prm, sh, n, mass, dunit, dt, mode, reacc, crp, cre, qpi, qepri, dis, nin):
+        gp, ge = self.grid(0), self.grid(1)
+        self._dsa_grids = (np.ascontiguousarray(gp[0]), np.ascontiguousarray(gp[1]),
+                           np.ascontiguousarray(ge[0]), np.ascontiguousarray(ge[1]))
+        g = [a.ctypes.data for a in self._dsa_grids]
+        return self.lib.or_dsa_inject(prm, self.nb, *g, sh, n, mass, dunit, dt, mode, reacc, crp, cre,
+                                      qpi, qepri, dis, nin)
 
     def beta_p(self):
         out = np.empty(self.nb)
@@ -243,6 +300,7 @@ class ReferenceCPU(_Common):
                                          _D, _D]
         L.ref_snapshot.argtypes = [_i, _D, _D, _d, _d, _i, _d, _d, _D, _D, _vp, _vp, _D, _D, _I, _I,
                                    _I, C.POINTER(_i)]
+        L.ref_dsa_inject.argtypes = [_vp, _vp, _i, _vp, _d, _d, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]
         self.cfg = cfg
         self.nb = cfg.nb
         self.configure(threads)
@@ -259,6 +317,10 @@ class ReferenceCPU(_Common):
     def _nsub(self, n, dt, bg, row, nsub, tgt, non, cap):
         return self.lib.ref_nsub(n, dt, bg, row, nsub, tgt, non, cap)
     def _buckets(self, *a): return self.lib.ref_buckets(*a)
+
+    def _dsa(self, prm, sh, n, mass, dunit, dt, mode, reacc, crp, cre, qpi, qepri, dis, nin):
+        return self.lib.ref_dsa_inject(prm, sh, n, mass, dunit, dt, mode, reacc, crp, cre, qpi, qepri,
+                                       dis, nin)
 
     def threads(self) -> int:
         return self.lib.ref_threads()

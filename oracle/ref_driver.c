@@ -409,3 +409,58 @@ done:
     free(capped); free(dis);
     return ierr;
 }
+
+/* ---- DSA injection through the reference's own snapshot routine ----
+ * Sets the reference's DSA globals (src/params.c:96-113, mu_mol :127) from
+ * prm, builds its DSA grid (dsa_init_grid, src/DSA_MODELS.c:1191) on the
+ * configured FP grids and calls tracer_fp_apply_dsa_tracer_injection_snapshot
+ * (src/tracer_fp_dsa.c:184) on cell-major state. */
+#include "DSA_MODELS.h"
+#include "tracer_fp_dsa.h"
+#include "croma_oracle.h"
+
+int ref_dsa_inject(const OrDsaParams *prm, const OrShockFields *sh, int ntracer,
+                   const double *mass_msun, double density_unit, double dt_gyr, int mode,
+                   int reacc_mode, double *crp, double *cre, double *qpi, double *qepri,
+                   unsigned char *dis, int *ninjected)
+{
+    DSAGrid grid;
+    TracerFpRawBackgroundSlot raw;
+    int rc;
+    if (!g_ready || !prm || !sh) return -1;
+    DSAEtaModelInitial = (DSAModelID)prm->eta_model_initial;
+    DSAEtaModelReacc = (DSAModelID)prm->eta_model_reacc;
+    DSAChiP = prm->chi_p;
+    DSAChiE = prm->chi_e;
+    DSAKep = prm->k_ep;
+    DSAPmaxPmc = prm->pmax_p_mc;
+    DSAPmaxEmc = prm->pmax_e_mc;
+    DSAMinMach = prm->min_mach;
+    DSAGammaGas = prm->gamma_gas;
+    DSAXcrPminPmc = prm->xcr_pmin_pmc;
+    DSAReaccEtaCap = prm->reacc_eta_cap;
+    DSAInjectSpecies = prm->inject_species;
+    DSADebug = 0;
+    mu_mol = prm->mu_mol;
+    memset(&grid, 0, sizeof grid);
+    if (!dsa_init_grid(&grid, &g_crp, &g_cre, prm->pmin_dsa_p_log10, prm->pmin_dsa_e_log10)) return -1;
+    memset(&raw, 0, sizeof raw);
+    raw.mach = (double *)sh->mach;
+    raw.prestemp = (double *)sh->prestemp;
+    raw.presden = (double *)sh->presden;
+    raw.pre_density_cgs = (double *)sh->pre_density_cgs;
+    raw.upstream_speed_cgs = (double *)sh->upstream_speed_cgs;
+    raw.shock_side_code = (double *)sh->shock_side_code;
+    raw.dsa_trigger = (double *)sh->dsa_trigger;
+    raw.dsa_mach = (double *)sh->dsa_mach;
+    raw.dsa_pre_density = (double *)sh->dsa_pre_density;
+    raw.dsa_kinetic_energy_flux_cgs = (double *)sh->dsa_flux_cgs;
+    raw.has_shock = 1;
+    raw.has_dsa = sh->has_dsa;
+    rc = tracer_fp_apply_dsa_tracer_injection_snapshot(
+        &raw, ntracer, NULL, mass_msun, density_unit, dt_gyr, (TracerDsaInjectionMode)mode,
+        (TracerDsaReaccMode)reacc_mode, &g_crp, &g_cre, &grid, crp, cre, qpi, qepri, dis,
+        1, 0, NULL, ninjected);
+    dsa_free_grid(&grid);
+    return rc;
+}

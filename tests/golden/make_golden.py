@@ -94,7 +94,52 @@ def make_case(name, spec):
     print(name, "nsub range", [(int(out[f"nsub_{k}"].min()), int(out[f"nsub_{k}"].max())) for k in range(nrun)])
 
 
+# DSA injection cases: (nb, ntracer, snapshot, seed, shocked fraction, state scale)
+DSA_CASES = {
+    "dsa_128": (128, 32, 20, 301, 0.4, 1.0e3),
+    "dsa_256": (256, 24, 40, 302, 0.4, 1.0e3),
+}
+
+
+def make_dsa_case(name, spec):
+    """Every (shock form, injection mode, reacceleration mode) combination of
+    the reference's tracer_fp_apply_dsa_tracer_injection_snapshot on one set
+    of tracers; drury83 runs with its eta cap on."""
+    nb, nt, isnap, seed, frac, scale = spec
+    cfg = config.config1(nb=nb)
+    ref = pyoracle.ReferenceCPU(cfg)
+    w = synth.Workload(cfg, nt, 100, seed=seed)
+    bg = w.background(isnap)
+    gp, ge = ref.grid(0), ref.grid(1)
+    crp0, cre0 = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), nt, cfg.species)
+    crp0 *= scale
+    cre0 *= scale
+    out = dict(nb=nb, ntracer=nt, isnap=isnap, seed=seed, fraction=frac, dt=float(w.dt[isnap]),
+               mass=w.mass, bg=bg, crp0=crp0, cre0=cre0)
+    for merged in (0, 1):
+        sh = synth.shocks(bg, isnap, seed, fraction=frac, merged=bool(merged))
+        for k, v in sh.items():
+            out[f"shock{merged}_{k}"] = np.asarray(v, dtype=np.float64)
+        for mode in (1, 2):
+            for reacc in (0, 1, 2):
+                prm = config.DsaParams(reacc_eta_cap=0.05 if reacc == 2 else 0.0)
+                crp, cre = crp0.copy(), cre0.copy()
+                qpi, qe = np.zeros_like(crp), np.zeros_like(cre)
+                dis = np.zeros(nt, np.uint8)
+                n = ref.dsa_inject(prm, sh, w.mass, 1.0, float(w.dt[isnap]), mode, reacc, crp, cre,
+                                   qpi, qe, dis)
+                tag = f"m{merged}_mode{mode}_r{reacc}"
+                out[f"{tag}_crp"], out[f"{tag}_cre"] = crp, cre
+                out[f"{tag}_qpi"], out[f"{tag}_qepri"] = qpi, qe
+                out[f"{tag}_dis"], out[f"{tag}_ninj"] = dis, np.int32(n)
+    np.savez_compressed(os.path.join(HERE, f"golden_{name}.npz"), **out)
+    print(name, "written")
+
+
 if __name__ == "__main__":
-    names = sys.argv[1:] or list(CASES)
+    names = sys.argv[1:] or list(CASES) + list(DSA_CASES)
     for n in names:
-        make_case(n, CASES[n])
+        if n in DSA_CASES:
+            make_dsa_case(n, DSA_CASES[n])
+        else:
+            make_case(n, CASES[n])

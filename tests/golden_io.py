@@ -13,8 +13,51 @@ from croma_fp_b200 import config as _config  # noqa: E402
 GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
-def case_names():
+def _names():
     return sorted(os.path.basename(p)[7:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "golden_*.npz")))
+
+
+def case_names():
+    """Snapshot cases (evolve fixtures)."""
+    return [n for n in _names() if not n.startswith("dsa_")]
+
+
+def dsa_case_names():
+    """DSA-injection fixtures."""
+    return [n for n in _names() if n.startswith("dsa_")]
+
+
+DSA_COMBOS = [(m, mode, r) for m in (0, 1) for mode in (1, 2) for r in (0, 1, 2)]
+
+
+class DsaCase:
+    """One DSA fixture: inputs and the reference's outputs for every
+    (shock form m, injection mode, reacceleration mode) combination."""
+
+    def __init__(self, name):
+        self.name = name
+        d = np.load(os.path.join(GOLDEN_DIR, f"golden_{name}.npz"))
+        self.d = d
+        self.nb = int(d["nb"])
+        self.ntracer = int(d["ntracer"])
+        self.cfg = _config.config1(nb=self.nb)
+        self.dt = float(d["dt"])
+
+    def shocks(self, merged):
+        pre = f"shock{merged}_"
+        out = {k[len(pre):]: self.d[k] for k in self.d.files if k.startswith(pre)}
+        out["has_dsa"] = int(out.get("has_dsa", 0))
+        return out
+
+    @staticmethod
+    def params(reacc):
+        return _config.DsaParams(reacc_eta_cap=0.05 if reacc == 2 else 0.0)
+
+    def expected(self, merged, mode, reacc):
+        t = f"m{merged}_mode{mode}_r{reacc}"
+        d = self.d
+        return dict(crp=d[f"{t}_crp"], cre=d[f"{t}_cre"], qpi=d[f"{t}_qpi"], qepri=d[f"{t}_qepri"],
+                    dis=d[f"{t}_dis"], ninj=int(d[f"{t}_ninj"]))
 
 
 class Case:
