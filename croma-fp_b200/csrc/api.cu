@@ -178,6 +178,7 @@ void croma_b200_destroy(CromaB200Context *h)
     cudaFree(c.d_ic);
     cudaFree(c.d_err);
     free_ic_stage(c);
+    free_dsa(c);
     if (c.stream) cudaStreamDestroy(c.stream);
     delete h;
 }
@@ -269,6 +270,28 @@ int croma_b200_get_state(CromaB200Context *h, double *crp, double *cre)
     return check_err(c);
 }
 
+int croma_b200_get_sources(CromaB200Context *h, double *qpi, double *qepri, unsigned char *dis)
+{
+    if (!h) { set_error("null context"); return -1; }
+    Context &c = h->impl;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    int rc = 0;
+    const size_t st = (size_t)NB * c.cap * sizeof(double);
+    auto down = [&](const double *d, double *h) -> int {
+        if (cell_major(c)) {
+            CROMA_CUDA(cudaMemcpyAsync(h, d, st, cudaMemcpyDeviceToHost, c.stream));
+            return 0;
+        }
+        return transpose_to_host(c, d, h, c.cap);
+    };
+    if (qpi && (rc = down(c.d_qpi, qpi))) return rc;
+    CROMA_CUDA(cudaStreamSynchronize(c.stream));
+    if (qepri && (rc = down(c.d_qepri, qepri))) return rc;
+    if (dis) CROMA_CUDA(cudaMemcpyAsync(dis, c.d_dis, (size_t)c.cap, cudaMemcpyDeviceToHost, c.stream));
+    CROMA_CUDA(cudaStreamSynchronize(c.stream));
+    return check_err(c);
+}
+
 int croma_b200_snapshot(CromaB200Context *h, const CromaB200Snapshot *s, int sync)
 {
     if (!h || !s || !s->bg_curr) { set_error("invalid snapshot arguments"); return -1; }
@@ -320,6 +343,25 @@ int croma_b200_snapshot(CromaB200Context *h, const CromaB200Snapshot *s, int syn
     if (rc) return rc;
     if (sync) return check_err(c);
     return 0;
+}
+
+int croma_b200_set_dsa(CromaB200Context *h, const CromaB200DsaParams *params)
+{
+    if (!h) { set_error("null context"); return -1; }
+    CROMA_CUDA(cudaSetDevice(h->impl.device));
+    return set_dsa(h->impl, params);
+}
+
+int croma_b200_dsa_inject(CromaB200Context *h, const CromaB200Shocks *shocks, double density_unit,
+                          double dt_gyr, int mode, int reacc_mode, int *ninjected)
+{
+    if (!h || !shocks) { set_error("null argument"); return -1; }
+    Context &c = h->impl;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    c.last_launches = 0;
+    int rc = dsa_inject(c, shocks, density_unit, dt_gyr, mode, reacc_mode, ninjected);
+    if (rc) return rc;
+    return check_err(c);
 }
 
 int croma_b200_get_schedule(CromaB200Context *h, int *nsub, int *non, int *target, int *bucket_ids,

@@ -122,6 +122,14 @@ struct Context {
     double *d_fac = nullptr;
     double *d_np_seg = nullptr;
     int fused_chunk = 0, fused_nseg = 0, fused_sets = 0;
+
+    // DSA injection
+    CromaB200DsaParams dsa{};
+    int dsa_set = 0;
+    double *d_dsa_p = nullptr;        // [2][nb] DSA-grid momenta at the FP bins
+    unsigned *d_dsa_count = nullptr;
+    double *d_dsa_stage = nullptr;    // [10][dsa_stage_cap] host shock fields
+    int dsa_stage_cap = 0;
     double *d_layout_tmp = nullptr;   // [nb][cap] transpose staging
 
     unsigned *d_err = nullptr;
@@ -165,6 +173,11 @@ int run_plain(Context &ctx, const SnapArgs &a);
 // fused.cu
 int fused_reserve(Context &ctx, int cap);
 int run_fused(Context &ctx, const SnapArgs &a);
+// dsa.cu
+int set_dsa(Context &ctx, const CromaB200DsaParams *prm);
+int dsa_inject(Context &ctx, const CromaB200Shocks *sh, double density_unit, double dt_gyr, int mode,
+               int reacc_mode, int *ninjected);
+void free_dsa(Context &ctx);
 // layout of the resident spectra: cell-major [tracer][nb] for the fused path,
 // momentum-major [nb][tracer] for the plain path
 inline bool cell_major(const Context &ctx) { return ctx.cfg.path == CROMA_PATH_FUSED; }

@@ -71,8 +71,26 @@ def load_library(nb: int) -> C.CDLL:
     L.croma_b200_kernel_stats.argtypes = [_vp, _i, P(_d), P(C.c_longlong)]
     L.croma_b200_reset_kernel_stats.argtypes = [_vp]
     L.croma_b200_fp64_peak.argtypes = [P(_d)]
+    L.croma_b200_get_sources.argtypes = [_vp, _vp, _vp, _vp]
+    L.croma_b200_set_dsa.argtypes = [_vp, P(CromaB200DsaParams)]
+    L.croma_b200_dsa_inject.argtypes = [_vp, P(CromaB200Shocks), _d, _d, _i, _i, P(_i)]
     _LIBS[nb] = L
     return L
+
+
+class CromaB200DsaParams(C.Structure):
+    _fields_ = [("eta_model_initial", _i), ("eta_model_reacc", _i), ("chi_p", _d), ("chi_e", _d),
+                ("k_ep", _d), ("pmax_p_mc", _d), ("pmax_e_mc", _d), ("min_mach", _d),
+                ("gamma_gas", _d), ("xcr_pmin_pmc", _d), ("reacc_eta_cap", _d), ("mu_mol", _d),
+                ("pmin_dsa_p_log10", _d), ("pmin_dsa_e_log10", _d), ("inject_species", _i)]
+
+
+SHOCK_FIELDS = ("mach", "prestemp", "presden", "pre_density_cgs", "upstream_speed_cgs",
+                "shock_side_code", "dsa_trigger", "dsa_mach", "dsa_pre_density", "dsa_flux_cgs")
+
+
+class CromaB200Shocks(C.Structure):
+    _fields_ = [(n, _vp) for n in SHOCK_FIELDS] + [("has_dsa", _i), ("on_device", _i)]
 
 
 class CromaError(RuntimeError):
@@ -219,6 +237,50 @@ class TracerFP:
         ms, n = _d(), C.c_longlong()
         self._check(self.lib.croma_b200_kernel_stats(self.h, self.KERNEL_KINDS[kind], C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def get_sources(self):
+        """(qpi, qepri, disable_adiabatic) as cell-major host arrays."""
+        qpi = np.empty((self.ntracer, self.nb)); qe = np.empty((self.ntracer, self.nb))
+        dis = np.empty(self.ntracer, np.uint8)
+        self._check(self.lib.croma_b200_get_sources(self.h, _p(qpi), _p(qe), _p(dis)))
+        return qpi, qe, dis
+
+    def set_dsa(self, params):
+        """params: an object with the CromaB200DsaParams field names
+        (config.DsaParams)."""
+        p = CromaB200DsaParams()
+        for name, _ in CromaB200DsaParams._fields_:
+            setattr(p, name, getattr(params, name))
+        self._check(self.lib.croma_b200_set_dsa(self.h, C.byref(p)))
+
+    DSA_MODES = {"off": 0, "tracer_state": 1, "tracer_source": 2}
+    DSA_REACC = {"off": 0, "positive_delta": 1, "drury83": 2}
+
+    def dsa_inject(self, shocks: dict, density_unit: float, dt_gyr: float, mode, reacc="off") -> int:
+        """One snapshot's shock injection; shocks maps SHOCK_FIELDS names to
+        host arrays [ntracer] (or device addresses with shocks['on_device'])
+        plus 'has_dsa'.  Returns the number of tracers injected."""
+        sh = CromaB200Shocks()
+        keep = []
+        on_dev = int(shocks.get("on_device", 0))
+        for n in SHOCK_FIELDS:
+            a = shocks.get(n)
+            if a is None:
+                continue
+            if on_dev:
+                setattr(sh, n, int(a))
+            else:
+                arr = np.ascontiguousarray(a, dtype=np.float64)
+                keep.append(arr)
+                setattr(sh, n, arr.ctypes.data)
+        sh.has_dsa = int(shocks.get("has_dsa", 0))
+        sh.on_device = on_dev
+        m = self.DSA_MODES[mode] if isinstance(mode, str) else int(mode)
+        r = self.DSA_REACC[reacc] if isinstance(reacc, str) else int(reacc)
+        nin = _i()
+        self._check(self.lib.croma_b200_dsa_inject(self.h, C.byref(sh), float(density_unit), float(dt_gyr),
+                                                   m, r, C.byref(nin)))
+        return nin.value
 
     def reset_kernel_stats(self):
         self._check(self.lib.croma_b200_reset_kernel_stats(self.h))

@@ -98,6 +98,9 @@ int croma_b200_set_state(CromaB200Context *ctx, int ntracer, const double *crp,
                          const double *cre, const double *qpi, const double *qepri,
                          const double *mass_msun, const unsigned char *disable_adiabatic);
 int croma_b200_get_state(CromaB200Context *ctx, double *crp, double *cre);
+/* The resident sources (cell-major host arrays [ntracer][nb]) and the
+ * disable-adiabatic flags [ntracer]; NULL skips an array. */
+int croma_b200_get_sources(CromaB200Context *ctx, double *qpi, double *qepri, unsigned char *dis);
 
 /* One snapshot on the context's stream; asynchronous unless sync != 0. */
 int croma_b200_snapshot(CromaB200Context *ctx, const CromaB200Snapshot *snap, int sync);
@@ -130,6 +133,46 @@ int croma_b200_last_launch_count(CromaB200Context *ctx);
 int croma_b200_set_kernel_timing(CromaB200Context *ctx, int enable);
 int croma_b200_kernel_stats(CromaB200Context *ctx, int kind, double *total_ms, long long *launches);
 int croma_b200_reset_kernel_stats(CromaB200Context *ctx);
+
+/* ---- DSA (diffusive shock acceleration) injection ----
+ * The per-snapshot shock injection of tracer_fp_apply_dsa_tracer_injection_snapshot
+ * (src/tracer_fp_dsa.c:184-565), run on the resident spectra.  Parameters
+ * mirror the reference's globals (src/params.c:96-113, mu_mol :127) and the
+ * DSA grid bounds passed to dsa_init_grid (src/tracer_fp.c:841).  Model ids
+ * follow DSAModelID: 0 KR07, 1 KR07r, 2 KR13, 3 KR13r, 4 CS14, 5 CS14r,
+ * 6 Ryu19, 7 Ryu19r. */
+typedef struct {
+    int eta_model_initial, eta_model_reacc;
+    double chi_p, chi_e, k_ep, pmax_p_mc, pmax_e_mc;
+    double min_mach, gamma_gas, xcr_pmin_pmc, reacc_eta_cap, mu_mol;
+    double pmin_dsa_p_log10, pmin_dsa_e_log10;
+    int inject_species;              /* 0 both, 1 electrons, 2 protons */
+} CromaB200DsaParams;
+
+/* Shock fields of every resident tracer ([ntracer] each; NULL = absent), the
+ * TracerFpRawBackgroundSlot fields of include/tracer_fp_types.h:292-313. */
+typedef struct {
+    const double *mach, *prestemp, *presden, *pre_density_cgs, *upstream_speed_cgs, *shock_side_code;
+    const double *dsa_trigger, *dsa_mach, *dsa_pre_density, *dsa_flux_cgs;
+    int has_dsa;                     /* 1: merged-DSA fields, 0: raw shock fields */
+    int on_device;                   /* 1: device pointers, 0: host pointers */
+} CromaB200Shocks;
+
+enum { CROMA_DSA_OFF = 0, CROMA_DSA_TRACER_STATE = 1, CROMA_DSA_TRACER_SOURCE = 2 };
+enum { CROMA_DSA_REACC_OFF = 0, CROMA_DSA_REACC_POSITIVE_DELTA = 1, CROMA_DSA_REACC_DRURY83 = 2 };
+
+int croma_b200_set_dsa(CromaB200Context *ctx, const CromaB200DsaParams *params);
+
+/* One snapshot's injection, before croma_b200_snapshot.  tracer_state adds
+ * source x V_down to the spectra; tracer_source replaces the sources with
+ * source x V_down / dt_gyr (they start from zero, as in the reference's
+ * snapshot driver).  The disable-adiabatic flags are cleared and set for the
+ * tracers drury83 reaccelerates.  A species that receives particles joins the
+ * context's species mask (the reference always evolves both species).
+ * Synchronous; *ninjected (may be NULL) receives the number of tracers
+ * injected. */
+int croma_b200_dsa_inject(CromaB200Context *ctx, const CromaB200Shocks *shocks, double density_unit,
+                          double dt_gyr, int mode, int reacc_mode, int *ninjected);
 
 /* FP64 FMA throughput of the current device, measured by a kernel of
  * independent fused multiply-add chains on every SM (TFLOP/s, FMA = 2 flops);
