@@ -44,8 +44,12 @@ class RunConfig:
         return DPP_MODELS[self.dpp_mode]
 
     def species_mask(self) -> int:
-        """bit 0: protons evolve, bit 1: electrons evolve."""
-        return {"electron_only": 2, "proton_only": 1, "electron_proton": 3}[self.species]
+        """bit 0: protons evolve, bit 1: electrons evolve.  `species` names the
+        seed spectra (seed_cr_species, src/params.c:69); the reference evolves
+        both species whatever the seed, so the mask leaves out only a species
+        that stays zero: protons of an electron-only seed.  A proton seed
+        feeds secondary electrons, so both evolve."""
+        return {"electron_only": 2, "proton_only": 3, "electron_proton": 3}[self.species]
 
 
 def config0(**kw) -> RunConfig:

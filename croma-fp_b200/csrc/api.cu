@@ -183,6 +183,13 @@ void croma_b200_destroy(CromaB200Context *h)
     delete h;
 }
 
+int croma_b200_set_workspace_limit(CromaB200Context *h, double bytes)
+{
+    if (!h || bytes < 0.0 || !isfinite(bytes)) { set_error("invalid workspace limit"); return -1; }
+    h->impl.workspace_bytes = bytes;
+    return 0;
+}
+
 int croma_b200_reserve(CromaB200Context *h, int ntracer)
 {
     if (!h || ntracer <= 0) { set_error("invalid reserve"); return -1; }

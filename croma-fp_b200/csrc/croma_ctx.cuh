@@ -122,6 +122,7 @@ struct Context {
     double *d_fac = nullptr;
     double *d_np_seg = nullptr;
     int fused_chunk = 0, fused_nseg = 0, fused_sets = 0;
+    double workspace_bytes = 0.0;     // fused workspace cap; 0 = CROMA_B200_WORKSPACE_GB or 24 GB
 
     // DSA injection
     CromaB200DsaParams dsa{};
@@ -172,6 +173,8 @@ int plain_reserve(Context &ctx, int cap);
 int run_plain(Context &ctx, const SnapArgs &a);
 // fused.cu
 int fused_reserve(Context &ctx, int cap);
+// device bytes fused_reserve allocates for cap tracers under a workspace cap
+double fused_workspace_bytes(const ModelParams &mp, int cap, double workspace_cap);
 int run_fused(Context &ctx, const SnapArgs &a);
 // dsa.cu
 int set_dsa(Context &ctx, const CromaB200DsaParams *prm);

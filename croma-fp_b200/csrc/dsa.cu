@@ -563,12 +563,10 @@ int dsa_inject(Context &c, const CromaB200Shocks *sh, double density_unit, doubl
     CROMA_CUDA(cudaMemsetAsync(c.d_dis, 0, (size_t)n, c.stream));
     CROMA_CUDA(cudaMemsetAsync(c.d_dsa_count, 0, sizeof(unsigned), c.stream));
     constexpr size_t smem = kDsaWarps * sizeof(DsaSmem);
-    static bool configured = false;
-    if (!configured) {
-        CROMA_CUDA(cudaFuncSetAttribute(dsa_inject_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem));
-        configured = true;
-    }
+    // set once per process; thread-safe (function-local static initialisation)
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(dsa_inject_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    CROMA_CUDA(attr);
     dsa_inject_kernel<<<(n + kDsaWarps - 1) / kDsaWarps, kDsaWarps * 32, smem, c.stream>>>(A);
     CROMA_CUDA(cudaGetLastError());
     c.last_launches += 1;

@@ -754,13 +754,10 @@ __global__ void __launch_bounds__(256, 2) secondary_kernel(FusedParams P)
 cudaError_t launch_secondary(Context &ctx, const FusedParams &P)
 {
     constexpr size_t smem = sizeof(GemmSmem);
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(secondary_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    // set once per process; thread-safe (function-local static initialisation)
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(secondary_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (attr != cudaSuccess) return attr;
     const long long rows = (long long)(P.g1 - P.g0) * P.nt;
     if (rows > 0x7fffffffLL) return cudaErrorInvalidValue;
     const long long blocks = (rows + kGM - 1) / kGM * (NB / kGN);
@@ -773,15 +770,19 @@ template <int S>
 cudaError_t launch_factor(Context &ctx, const FusedParams &P)
 {
     constexpr size_t smem = (size_t)kTab * kTabStride * sizeof(double) + kFacWarps * sizeof(WarpSmem);
-    static int resident = 0;   // blocks per SM, per instantiation; found before the first launch
-    if (!resident) {
-        cudaError_t e = cudaFuncSetAttribute(factor_kernel<S>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, factor_kernel<S>, kFacWarps * 32, smem);
-        if (e != cudaSuccess) return e;
-        if (resident < 1) return cudaErrorInvalidConfiguration;
-    }
+    // blocks per SM, per instantiation: found once (thread-safe static initialisation)
+    struct Occupancy { cudaError_t e; int resident; };
+    static const Occupancy occ = [] {
+        Occupancy o{cudaSuccess, 0};
+        o.e = cudaFuncSetAttribute(factor_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (o.e == cudaSuccess)
+            o.e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.resident, factor_kernel<S>, kFacWarps * 32,
+                                                                smem);
+        return o;
+    }();
+    if (occ.e != cudaSuccess) return occ.e;
+    if (occ.resident < 1) return cudaErrorInvalidConfiguration;
+    const int resident = occ.resident;
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -816,15 +817,40 @@ double workspace_budget_bytes()
 
 }  // namespace
 
+namespace {
+
+struct WorkspaceShape {
+    int nseg, sets;
+    long long chunk;
+    double per_tracer;
+};
+
+WorkspaceShape workspace_shape(const ModelParams &mp, int cap, double workspace_cap)
+{
+    WorkspaceShape w;
+    w.nseg = mp.interp_max_segments < 1 ? 1 : (mp.interp_max_segments > 64 ? 64 : mp.interp_max_segments);
+    w.sets = mp.window_centred ? 2 : 1;
+    w.per_tracer = 8.0 * NB * ((double)2 * w.nseg * w.sets * 3 + 2.0 * w.nseg);
+    const double budget = workspace_cap > 0.0 ? workspace_cap : workspace_budget_bytes();
+    w.chunk = (long long)(budget / w.per_tracer);
+    if (w.chunk < 1) w.chunk = 1;
+    if (w.chunk > cap) w.chunk = cap;
+    return w;
+}
+
+}  // namespace
+
+double fused_workspace_bytes(const ModelParams &mp, int cap, double workspace_cap)
+{
+    const WorkspaceShape w = workspace_shape(mp, cap, workspace_cap);
+    return (double)w.chunk * w.per_tracer + 8.0 * cap;
+}
+
 int fused_reserve(Context &ctx, int cap)
 {
-    const int nseg = ctx.mp.interp_max_segments < 1 ? 1
-                   : (ctx.mp.interp_max_segments > 64 ? 64 : ctx.mp.interp_max_segments);
-    const int sets = ctx.mp.window_centred ? 2 : 1;
-    const double per_tracer = 8.0 * NB * ((double)2 * nseg * sets * 3 + 2.0 * nseg);
-    long long chunk = (long long)(workspace_budget_bytes() / per_tracer);
-    if (chunk < 1) chunk = 1;
-    if (chunk > cap) chunk = cap;
+    const WorkspaceShape w = workspace_shape(ctx.mp, cap, ctx.workspace_bytes);
+    const int nseg = w.nseg, sets = w.sets;
+    const long long chunk = w.chunk;
     cudaFree(ctx.d_inje);
     cudaFree(ctx.d_eta_scale);
     cudaFree(ctx.d_fac);

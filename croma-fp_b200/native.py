@@ -97,6 +97,21 @@ class CromaError(RuntimeError):
     pass
 
 
+def make_config(cfg: RunConfig, path: str = "plain") -> CromaB200Config:
+    """CromaB200Config from a RunConfig."""
+    c = CromaB200Config()
+    for name, _ in CromaB200Config._fields_:
+        if name == "dpp_model":
+            c.dpp_model = cfg.dpp_model_id()
+        elif name == "species_mask":
+            c.species_mask = cfg.species_mask()
+        elif name == "path":
+            c.path = PATHS[path]
+        else:
+            setattr(c, name, getattr(cfg, name))
+    return c
+
+
 def fp64_peak(nb: int = 256) -> float:
     """FP64 FMA throughput of the current device in TFLOP/s (measured live)."""
     L = load_library(nb)
@@ -121,16 +136,7 @@ class TracerFP:
         self.cfg = cfg
         self.nb = cfg.nb
         self.lib = load_library(cfg.nb)
-        c = CromaB200Config()
-        for name, _ in CromaB200Config._fields_:
-            if name == "dpp_model":
-                c.dpp_model = cfg.dpp_model_id()
-            elif name == "species_mask":
-                c.species_mask = cfg.species_mask()
-            elif name == "path":
-                c.path = PATHS[path]
-            else:
-                setattr(c, name, getattr(cfg, name))
+        c = make_config(cfg, path)
         h = _vp()
         self._check(self.lib.croma_b200_create(C.byref(c), device, C.byref(h)))
         self.h = h

@@ -46,7 +46,10 @@ enum {
 
 /* Species bits: bit 0 protons, bit 1 electrons.  A species outside the mask
  * must have zero spectra and zero source; it is then left untouched, which
- * is exactly what the implicit solve returns for it. */
+ * is exactly what the implicit solve returns for it.  The reference evolves
+ * both species whatever its seed (seed_cr_species): an electron-only seed
+ * maps to mask 2, a proton or mixed seed to mask 3 (protons feed secondary
+ * electrons).  Mask 1 skips the electrons, secondaries included. */
 enum { CROMA_SPECIES_PROTON = 1, CROMA_SPECIES_ELECTRON = 2 };
 
 typedef struct {
@@ -91,6 +94,11 @@ void croma_b200_destroy(CromaB200Context *ctx);
 
 /* Device workspace and state for up to ntracer tracers. */
 int croma_b200_reserve(CromaB200Context *ctx, int ntracer);
+
+/* Cap (device bytes) on the fused path's evolve workspace; tracers beyond
+ * what it holds run in chunks.  Takes effect at the next reserve; 0 restores
+ * the default (CROMA_B200_WORKSPACE_GB, else 24 GB). */
+int croma_b200_set_workspace_limit(CromaB200Context *ctx, double bytes);
 
 /* Host <-> device spectra, cell-major host arrays [ntracer][nb] (the
  * reference's layout).  NULL skips an array; sources default to zero. */
