@@ -375,6 +375,13 @@ def run_gpu_arm(args):
                                              "frac": (sec_flops / (sec_ms / 1e3) / 1e12) / peak
                                              if sec_ms > 0 else None}}}
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        # p50 / p99 request latency of the serving workload (Poisson arrivals
+        # of tracer chunks), a bounded sample run after the timed region
+        fp.close()
+        from croma_fp_b200 import serve_bench
+        serving = serve_bench.run(nrequests=args.serving_requests)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -392,6 +399,7 @@ def run_gpu_arm(args):
                     "d2h_bytes_per_step": int(d2h), "api": "croma_b200_set_state/snapshot/get_state"},
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "serving": serving,
             "clocks": clocks.summary(),
             "gpu_launches": int(launches),
             "kernel_ms": {"evolve": evolve_ms, "coeff": coeff_ms, "secondary": sec_ms},
@@ -415,6 +423,8 @@ def main():
     ap.add_argument("--tracers", type=int, default=NTRACER)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=16)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -231,6 +231,21 @@ __global__ void hadronic_emission_kernel(int ncell, int nbins, const double *crp
     out[(size_t)icell * nbins + ng] = E[ng] * (integral * 0.5) * n_gas[icell];
 }
 
+// prepare_ic_emission_cell_major (src/fp_shared_core.c:2131-2157): per
+// (cell, band) the sum over electron bins of fic x N x dp, in bin order.
+__global__ void ic_emission_kernel(int ncell, int nbins, const double *cre, const double *fic,
+                                   const double *dp, double *out)
+{
+    const int nic = blockIdx.y * blockDim.y + threadIdx.y;
+    const int icell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (icell >= ncell || nic >= nbins) return;
+    const double *N = cre + (size_t)icell * NB;
+    const double *f = fic + (size_t)nic * NB;
+    double integral = 0.0;
+    for (int je = 0; je < NB; je++) integral += f[je] * N[je] * dp[je];
+    out[(size_t)icell * nbins + nic] = integral;
+}
+
 // prepare_synch_emission_cell_major, pitch-kernel-table branch
 // (src/fp_shared_core.c:2070-2112 with tracer_fp_interp_synch_kernel_logk :2054-2068).
 __global__ void synch_table_kernel(int ncell, int nfreq, int nlogb, double logb_min, double inv_dlogb,
@@ -701,6 +716,38 @@ int run_tracer_pipeline_group(const FpCudaPipelineInput *inputs, int ninput,
         acc.total_ms += one.total_ms;
     }
     if (times) *times = acc;
+    return 0;
+}
+
+int prepare_ic_emission_cuda_batch(const FpIcEmissionBatchInput *in, const CRspectrum *cre_grid,
+                                   double *eps_ic_out, double *elapsed_ms)
+{
+    if (!in || !cre_grid || !eps_ic_out || in->ncell <= 0 || in->nbins <= 0 || !in->cre_batch ||
+        !in->fic_flat)
+        return fail(-1, "invalid IC emission input");
+    const int ncell = in->ncell, nbins = in->nbins;
+    Scratch s;
+    double *d_cre, *d_fic, *d_dp, *d_out;
+    CROMA_CUDA(s.get((void **)&d_cre, (size_t)ncell * NB * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_fic, (size_t)nbins * NB * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_dp, NB * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_out, (size_t)ncell * nbins * sizeof(double)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    CROMA_CUDA(cudaMemcpy(d_cre, in->cre_batch, (size_t)ncell * NB * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_fic, in->fic_flat, (size_t)nbins * NB * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_dp, cre_grid->dp, NB * sizeof(double), cudaMemcpyHostToDevice));
+    dim3 blk(32, 4), grd((ncell + 31) / 32, (nbins + 3) / 4);
+    ic_emission_kernel<<<grd, blk>>>(ncell, nbins, d_cre, d_fic, d_dp, d_out);
+    CROMA_CUDA(cudaGetLastError());
+    CROMA_CUDA(cudaMemcpy(eps_ic_out, d_out, (size_t)ncell * nbins * sizeof(double), cudaMemcpyDeviceToHost));
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    if (elapsed_ms) *elapsed_ms = elapsed(e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     return 0;
 }
 

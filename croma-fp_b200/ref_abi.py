@@ -52,6 +52,11 @@ class FpHadronicEmissionBatchInput(C.Structure):
                 ("n_gas", _D), ("crp_batch", _D), ("beta_p", _D), ("kernel_flat", _D)]
 
 
+class FpIcEmissionBatchInput(C.Structure):
+    _fields_ = [("ncell", _i), ("nbins", _i), ("z", _d), ("nu_min", _d), ("nu_max", _d),
+                ("cre_batch", _D), ("fic_flat", _D)]
+
+
 class FpChangCooperSolveBatchInput(C.Structure):
     _fields_ = [("nsys", _i), ("nrow", _i), ("dt", _d), ("a_batch", _D), ("b_batch", _D),
                 ("c_batch", _D), ("source_batch", _D)]

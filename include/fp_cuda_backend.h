@@ -106,6 +106,17 @@ typedef struct {
     const double *nus;
 } FpSynchEmissionBatchInput;
 
+/* include/fp_shared_core.h:494-503 */
+typedef struct {
+    int ncell;
+    int nbins;
+    double z;
+    double nu_min;                     /* log10(nu/Hz) */
+    double nu_max;                     /* log10(nu/Hz) */
+    const double *cre_batch;           /* [ncell * npe] cell-major */
+    const double *fic_flat;            /* [nbins * npe] row-major */
+} FpIcEmissionBatchInput;
+
 /* include/fp_shared_core.h:502-514 */
 typedef struct {
     int ncell;
@@ -237,6 +248,13 @@ int prepare_synch_emission_cuda_batch(const FpSynchEmissionBatchInput *in,   /* 
                                       const CRspectrum *cre_grid,
                                       double *eps_syn_out,
                                       double *elapsed_ms);
+/* The device form of the CPU routine prepare_ic_emission_batch
+ * (src/fp_shared_core.c:2131-2164), which the reference's CUDA backend does not
+ * provide: eps_ic[cell][band] = sum_je fic[band][je] N[cell][je] dp[je]. */
+int prepare_ic_emission_cuda_batch(const FpIcEmissionBatchInput *in,
+                                   const CRspectrum *cre_grid,
+                                   double *eps_ic_out,
+                                   double *elapsed_ms);
 int prepare_gamma_emission_cuda_batch(const FpGammaEmissionBatchInput *in,   /* :102-105 */
                                       const CRspectrum *crp_grid,
                                       double *eps_gamma_out,

@@ -301,6 +301,7 @@ class ReferenceCPU(_Common):
         L.ref_snapshot.argtypes = [_i, _D, _D, _d, _d, _i, _d, _d, _D, _D, _vp, _vp, _D, _D, _I, _I,
                                    _I, C.POINTER(_i)]
         L.ref_dsa_inject.argtypes = [_vp, _vp, _i, _vp, _d, _d, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]
+        L.ref_ic_emission.argtypes = [_i, _i, _d, _d, _d, _D, _D, _D]
         self.cfg = cfg
         self.nb = cfg.nb
         self.configure(threads)
@@ -321,6 +322,15 @@ class ReferenceCPU(_Common):
     def _dsa(self, prm, sh, n, mass, dunit, dt, mode, reacc, crp, cre, qpi, qepri, dis, nin):
         return self.lib.ref_dsa_inject(prm, sh, n, mass, dunit, dt, mode, reacc, crp, cre, qpi, qepri,
                                        dis, nin)
+
+    def ic_emission(self, cre, nbins, z, nu_min, nu_max):
+        """(fic [nbins][nb], eps [ncell][nbins]) from the reference's
+        prepare_ic_kernel_flat and prepare_ic_emission_batch."""
+        cre = np.ascontiguousarray(cre, dtype=np.float64)
+        fic = np.empty((nbins, self.nb)); eps = np.empty((cre.shape[0], nbins))
+        if self.lib.ref_ic_emission(cre.shape[0], nbins, z, nu_min, nu_max, cre, fic, eps) != 0:
+            raise RuntimeError("ref_ic_emission failed")
+        return fic, eps
 
     def threads(self) -> int:
         return self.lib.ref_threads()

@@ -464,3 +464,24 @@ int ref_dsa_inject(const OrDsaParams *prm, const OrShockFields *sh, int ntracer,
     dsa_free_grid(&grid);
     return rc;
 }
+
+/* IC emissivity through the reference: the kernel table of
+ * prepare_ic_kernel_flat (src/fp_shared_core.c:1780-1807) for nbins bands over
+ * [nu_min, nu_max] (log10 Hz) at redshift z, and prepare_ic_emission_batch
+ * (src/fp_shared_core.c:2131-2164) on cell-major electron spectra. */
+int ref_ic_emission(int ncell, int nbins, double z, double nu_min, double nu_max,
+                    const double *cre, double *fic_out, double *eps_out)
+{
+    FpIcEmissionBatchInput in;
+    if (!g_ready || ncell <= 0 || nbins <= 0 || !cre || !fic_out || !eps_out) return -1;
+    prepare_ic_kernel_flat(&g_cre, nbins, nu_min, nu_max, z, fic_out);
+    memset(&in, 0, sizeof in);
+    in.ncell = ncell;
+    in.nbins = nbins;
+    in.z = z;
+    in.nu_min = nu_min;
+    in.nu_max = nu_max;
+    in.cre_batch = cre;
+    in.fic_flat = fic_out;
+    return prepare_ic_emission_batch(&in, &g_cre, eps_out);
+}

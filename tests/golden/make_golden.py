@@ -136,10 +136,31 @@ def make_dsa_case(name, spec):
     print(name, "written")
 
 
+def make_ic_emission(name="emission_ic"):
+    """IC emissivities of the reference (prepare_ic_kernel_flat +
+    prepare_ic_emission_batch) for 128- and 256-bin electron spectra."""
+    out = {}
+    for nb in (128, 256):
+        cfg = config.config1(nb=nb)
+        ref = pyoracle.ReferenceCPU(cfg)
+        w = synth.Workload(cfg, 12, 100, seed=404)
+        gp, ge = ref.grid(0), ref.grid(1)
+        _, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), 12, cfg.species)
+        cre = cre * np.random.default_rng(nb).uniform(0.5, 2.0, (12, 1))
+        fic, eps = ref.ic_emission(cre, 20, 0.3, 14.0, 26.0)
+        out[f"nb{nb}_cre"], out[f"nb{nb}_fic"], out[f"nb{nb}_eps"] = cre, fic, eps
+        out[f"nb{nb}_dp"] = ge[1]
+    out["z"], out["nu_min"], out["nu_max"], out["nbins"] = 0.3, 14.0, 26.0, 20
+    np.savez_compressed(os.path.join(HERE, f"golden_{name}.npz"), **out)
+    print(name, "written")
+
+
 if __name__ == "__main__":
-    names = sys.argv[1:] or list(CASES) + list(DSA_CASES)
+    names = sys.argv[1:] or list(CASES) + list(DSA_CASES) + ["emission_ic"]
     for n in names:
         if n in DSA_CASES:
             make_dsa_case(n, DSA_CASES[n])
+        elif n == "emission_ic":
+            make_ic_emission(n)
         else:
             make_case(n, CASES[n])

@@ -19,7 +19,7 @@ def _names():
 
 def case_names():
     """Snapshot cases (evolve fixtures)."""
-    return [n for n in _names() if not n.startswith("dsa_")]
+    return [n for n in _names() if not n.startswith(("dsa_", "emission_"))]
 
 
 def dsa_case_names():
