@@ -289,18 +289,27 @@ def run_gpu_arm(args):
         ms_max = float(t.item())
     value = world * nt * args.steps / (ms_max / 1e3)
 
-    # ---- e2e through the C ABI with host buffers ----
-    crp_h, cre_h = fp.get_state()
-    bg_host = [w.background(first + k) for k in range(nsteps_total + 1)]
+    # ---- e2e through the C ABI with page-locked host buffers ----
+    def pinned(shape):
+        return torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+    crp_h, cre_h = pinned((nt, cfg.nb)), pinned((nt, cfg.nb))
+    fp.get_state(crp_h, cre_h)
+    mass_h = pinned((nt,))
+    mass_h[:] = w.mass
+    bg_host = []
+    for k in range(min(args.steps, 3) + 1):
+        b = pinned((8, nt))
+        b[:] = w.background(first + k)
+        bg_host.append(b)
     e2e_times = []
     h2d = d2h = 0
     for k in range(min(args.steps, 3)):
         isnap = snaps[k]
         t0 = time.perf_counter()
-        fp.set_state(crp_h, cre_h, mass=w.mass)
+        fp.set_state(crp_h, cre_h, mass=mass_h)
         fp.snapshot(bg_host[k], bg_host[k + 1], float(w.z[isnap]), float(w.z[isnap + 1]), True,
                     float(w.dt[isnap]), float(w.elapsed[isnap]), sync=False)
-        crp_h, cre_h = fp.get_state()
+        fp.get_state(crp_h, cre_h)
         e2e_times.append(time.perf_counter() - t0)
         h2d = crp_h.nbytes + cre_h.nbytes + w.mass.nbytes + bg_host[k].nbytes * 2
         d2h = crp_h.nbytes + cre_h.nbytes
@@ -396,7 +405,8 @@ def run_gpu_arm(args):
             "config": dict(workload_desc(nt), parallelism=f"dp{world} (independent tracer shards)",
                            path=args.path),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "api": "croma_b200_set_state/snapshot/get_state"},
+                    "d2h_bytes_per_step": int(d2h), "host_buffers": "page-locked",
+                    "api": "croma_b200_set_state/snapshot/get_state"},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "serving": serving,

@@ -21,13 +21,13 @@ struct SegInfo {
     double alpha, dt;
 };
 
-__device__ __forceinline__ SegInfo seg_info(const Schedule &s, int t, int slot, double dt_snap)
+// Segment `slot` of a tracer with the given schedule entries.
+__device__ __forceinline__ SegInfo seg_info_of(int nseg, int nsub, int non, int slot, double dt_snap)
 {
     SegInfo g{};
-    g.nseg = s.nseg[t];
+    g.nseg = nseg;
     if (slot >= g.nseg) return g;
-    g.nsub = s.nsub[t];
-    const int non = s.non[t];
+    g.nsub = nsub;
     // slot < 64 and nsub <= 1e6 (the sub-step ceiling), so 32-bit products suffice
     g.b = (slot * g.nsub) / g.nseg;
     g.e = ((slot + 1) * g.nsub) / g.nseg;
@@ -45,6 +45,18 @@ __device__ __forceinline__ SegInfo seg_info(const Schedule &s, int t, int slot, 
     g.dt = dt_snap / (double)g.nsub;
     return g;
 }
+
+__device__ __forceinline__ SegInfo seg_info(const Schedule &s, int t, int slot, double dt_snap)
+{
+    const int nseg = s.nseg[t];
+    if (slot >= nseg) {
+        SegInfo g{};
+        g.nseg = nseg;
+        return g;
+    }
+    return seg_info_of(nseg, s.nsub[t], s.non[t], slot, dt_snap);
+}
+
 
 __device__ __forceinline__ double lerp(double c, double n, double a)
 {
@@ -66,6 +78,15 @@ __device__ __forceinline__ Bg load_bg(const SnapArgs &a, int t, const SegInfo &g
         const double c = a.bg_curr[f * N + t];
         v[f] = (g.nseg > 1) ? lerp(c, a.bg_next[f * N + t], g.alpha) : c;
     }
+    return Bg{v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]};
+}
+
+// Background of segment g from the raw rows of the current and next snapshot.
+__device__ __forceinline__ Bg lerp_bg(const double cur[kNbg], const double nxt[kNbg], const SegInfo &g)
+{
+    double v[kNbg];
+#pragma unroll
+    for (int f = 0; f < kNbg; f++) v[f] = (g.nseg > 1) ? lerp(cur[f], nxt[f], g.alpha) : cur[f];
     return Bg{v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]};
 }
 

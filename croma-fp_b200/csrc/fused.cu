@@ -200,6 +200,7 @@ __device__ __forceinline__ SegTerms<S> seg_terms(const GridTables &gt, const Bg 
 
 struct WarpSmem {
     double B[kSw], C[kSw], D[kSw], Wp[kSw], Wm[kSw];
+    double bg[2][kNbg];     // the tracer's current and next background rows
 };
 
 
@@ -353,8 +354,8 @@ __device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int la
 
 
 // Factor kernel, persistent: each block stages the species' grid tables in
-// shared memory once, then its warps take work items u -> (segment gi, set,
-// tracer tl), tl fastest, strided by the grid.
+// shared memory once, then each warp takes tracers strided by the grid and
+// factors every segment (and on/off set) of each.
 template <int S>
 __global__ void __launch_bounds__(kFacWarps * 32, (NB <= 256 ? 2 : 1)) factor_kernel(FusedParams P)
 {
@@ -389,33 +390,52 @@ __global__ void __launch_bounds__(kFacWarps * 32, (NB <= 256 ? 2 : 1)) factor_ke
         tab[TB_IDXR * kTabStride + swz(i)] = st.inv_dxr[i];
     }
     __syncthreads();
-    const int total = (P.g1 - P.g0) * P.sets * P.nt;   // < 2^31, checked on the host
+    // a warp takes one tracer at a time and factors all its segments (and
+    // on/off sets): the schedule entries and both background rows are read
+    // once per tracer (lanes 0-15 fetch one value each, shuffles spread them)
     const int stride = gridDim.x * kFacWarps;
+    const int nslot = P.g1 - P.g0;
 #pragma unroll 1
-    for (int u = blockIdx.x * kFacWarps + w; u < total; u += stride) {
-        const int tl = u % P.nt;
-        const int rest = u / P.nt;
-        const int set = rest % P.sets, gi = rest / P.sets;
+    for (int tl = blockIdx.x * kFacWarps + w; tl < P.nt; tl += stride) {
         const int t = P.t0 + tl;
-        const SegInfo g = segment_of(P, t, P.g0 + gi);
-        if (!g.active || !needs_set(g, set)) continue;
-        if (needs_set(g, 1) && P.sets < 2) {   // checked on the host; never write past the sets
-            if (lane == 0) atomicOr(a.err, kErrBadInput);
-            continue;
+        int nseg = 0, nsub = 0, non = 0;
+        if (!P.explicit_seg) {
+            nseg = a.sched.nseg[t];
+            nsub = a.sched.nsub[t];
+            non = a.sched.non[t];
         }
-        const Bg bg = load_bg(a, t, g);
-        const int dis = a.dis ? a.dis[t] : 0;
-        SegTerms<S> T = seg_terms<S>(P.gt, bg, dis, a, g, t, P.ic_stride);
-        if (set == 0) {
-            const double tacc = segment_tacc(P.mp, a, g);
-            const DppForm on = dpp_form(P.mp, P.mp.dpp_model, bg, tacc);
-            T.dpp_fill = on.fill;
-            T.dpp_inv = on.inv;
-            T.dpp_scale = (P.mp.dpp_model != kDppOff && P.eta_scale) ? P.eta_scale[t] : 1.0;
-        }
-        const unsigned err = factor_store<S>(T, tab, lane, smem[w], fac_ptr(P, S, gi, set, tl));
-        if (err && lane == 0) atomicOr(a.err, err);
+        WarpSmem &ws = smem[w];
         __syncwarp();
+        if (lane < kNbg) ws.bg[0][lane] = a.bg_curr[(size_t)lane * a.ntracer + t];
+        else if (lane < 2 * kNbg) ws.bg[1][lane - kNbg] = a.bg_next[(size_t)(lane - kNbg) * a.ntracer + t];
+        __syncwarp();
+        const int dis = a.dis ? a.dis[t] : 0;
+        const double eta = (P.mp.dpp_model != kDppOff && P.eta_scale) ? P.eta_scale[t] : 1.0;
+#pragma unroll 1
+        for (int gi = 0; gi < nslot; gi++) {
+            const SegInfo g = P.explicit_seg ? P.ex : seg_info_of(nseg, nsub, non, P.g0 + gi, a.dt_snap);
+            if (!g.active) break;
+            if (needs_set(g, 1) && P.sets < 2) {   // checked on the host; never write past the sets
+                if (lane == 0) atomicOr(a.err, kErrBadInput);
+                continue;
+            }
+            const Bg bg = lerp_bg(ws.bg[0], ws.bg[1], g);
+#pragma unroll 1
+            for (int set = 0; set < P.sets; set++) {
+                if (!needs_set(g, set)) continue;
+                SegTerms<S> T = seg_terms<S>(P.gt, bg, dis, a, g, t, P.ic_stride);
+                if (set == 0) {
+                    const double tacc = segment_tacc(P.mp, a, g);
+                    const DppForm on = dpp_form(P.mp, P.mp.dpp_model, bg, tacc);
+                    T.dpp_fill = on.fill;
+                    T.dpp_inv = on.inv;
+                    T.dpp_scale = eta;
+                }
+                const unsigned err = factor_store<S>(T, tab, lane, ws, fac_ptr(P, S, gi, set, tl));
+                if (err && lane == 0) atomicOr(a.err, err);
+                __syncwarp();
+            }
+        }
     }
 }
 
@@ -629,19 +649,36 @@ __global__ void __launch_bounds__(128) eta_scale_kernel(FusedParams P, double *e
 
 // Secondary source of every segment of the chunk, cell-major:
 // inje[m][je] = Gyr n_gas(t, segment) sum_{jp} N_p[m][jp] fqe[jp][je] + qepri[t][je]
-// over the rows m = gi * nt + tl of np_seg.  An FP64 GEMM on the CUDA cores:
-// 128 x 64 output tile per 256-thread block, 8 x 4 outputs per thread,
-// k-tiles of 16 double-buffered in shared memory with the next tile
-// prefetched into registers.  The proton index starts at the first k-tile
+// over the rows m = gi * nt + tl of np_seg -- a [rows x nb] . [nb x nb] FP64
+// GEMM on the FP64 tensor cores (mma.sync m8n8k4 .f64: one instruction is
+// 256 multiply-adds).  A 128 x 64 output tile per 256-thread block, each warp
+// a 32 x 32 tile of 4 x 4 MMA fragments; k-tiles of 16 double-buffered in
+// shared memory by cp.async.  The proton index starts at the first k-tile
 // holding a nonzero weight for the block's columns; fqe is zero below
 // np_min_qe[je] (prepare_secondary_kernel_flat, src/fp_shared_core.c:1453-1506),
 // so the rounded-down start adds exact zeros only.
-constexpr int kGM = 128, kGN = 64, kGK = 16, kGPad = 4;
+constexpr int kGM = 128, kGN = 64, kGK = 16;
+constexpr int kGPitchA = kGK + 4;    // sA[m][k], 20 doubles per row
+constexpr int kGPitchB = kGN + 8;    // sB[k][n], 72 doubles per row
 
 struct GemmSmem {
-    double A[2][kGK][kGM + kGPad];   // transposed: [k][m]
-    double B[2][kGK][kGN];
+    double A[2][kGM][kGPitchA];
+    double B[2][kGK][kGPitchB];
 };
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int n = valid ? 16 : 0;   // 0 source bytes: the 16 destination bytes are zero-filled
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
 
 __global__ void __launch_bounds__(256, 2) secondary_kernel(FusedParams P)
 {
@@ -649,105 +686,94 @@ __global__ void __launch_bounds__(256, 2) secondary_kernel(FusedParams P)
     GemmSmem &sm = *reinterpret_cast<GemmSmem *>(smem_raw);
     const SnapArgs &a = P.a;
     const int nrows = (P.g1 - P.g0) * P.nt;   // < 2^31, checked on the host
-    const int tid = threadIdx.x;
-    const int tx = tid & 15, ty = tid >> 4;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;   // warp tile origin in the block tile
+    const int gid = lane >> 2, tig = lane & 3;                // MMA fragment coordinates
     // column tile fastest, so the NB / kGN blocks of one row tile run together
     // and read their A tile from L2
     const int n0 = (int)(blockIdx.x % (NB / kGN)) * kGN;
     const int m0 = (int)(blockIdx.x / (NB / kGN)) * kGM;
     int jstart = NB;
-    for (int i = 0; i < kGN && n0 + i < NB; i++) jstart = min(jstart, P.np_min_qe[n0 + i]);
+    for (int i = 0; i < kGN; i++) jstart = min(jstart, P.np_min_qe[n0 + i]);
     jstart = max(jstart, P.gt.fqe_jp0);
     const int kbeg = (jstart / kGK) * kGK;
 
-    // loader roles: A row lm, k-half lh (8 doubles); B row lk, 4 columns ln
-    const int lm = tid >> 1, lh = tid & 1;
-    const int lk = tid >> 4, ln = (tid & 15) * 4;
-    const bool arow = (m0 + lm) < nrows;
-    const double *Arow = P.np_seg + (size_t)(m0 + lm) * NB + lh * 8;
-    const double *Bp = P.gt.fqe + n0 + ln;
-    double ra[8], rb[4];
-    auto fetch = [&](int k0) {
-        if (arow) {
+    // loader roles: A rows (4 chunks of 16 B per thread), B rows (2 chunks)
+    auto load_tile = [&](int buf, int k0) {
 #pragma unroll
-            for (int i = 0; i < 8; i += 2) {
-                const double2 v = __ldcs(reinterpret_cast<const double2 *>(Arow + k0 + i));
-                ra[i] = v.x;
-                ra[i + 1] = v.y;
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < 8; i++) ra[i] = 0.0;
+        for (int c = 0; c < 4; c++) {
+            const int q = tid + 256 * c;          // 0..1023: row q / 8, chunk q % 8
+            const int r = q >> 3, ch = q & 7;
+            const int m = m0 + r;
+            const bool ok = m < nrows;
+            const double *src = P.np_seg + (size_t)(ok ? m : 0) * NB + k0 + ch * 2;
+            cp_async16(&sm.A[buf][r][ch * 2], src, ok);
         }
-        const double2 b0 = __ldg(reinterpret_cast<const double2 *>(Bp + (size_t)(k0 + lk) * NB));
-        const double2 b1 = __ldg(reinterpret_cast<const double2 *>(Bp + (size_t)(k0 + lk) * NB + 2));
-        rb[0] = b0.x; rb[1] = b0.y; rb[2] = b1.x; rb[3] = b1.y;
-    };
-    auto stash = [&](int buf) {
 #pragma unroll
-        for (int i = 0; i < 8; i++) sm.A[buf][lh * 8 + i][lm] = ra[i];
-        *reinterpret_cast<double2 *>(&sm.B[buf][lk][ln]) = make_double2(rb[0], rb[1]);
-        *reinterpret_cast<double2 *>(&sm.B[buf][lk][ln + 2]) = make_double2(rb[2], rb[3]);
+        for (int c = 0; c < 2; c++) {
+            const int q = tid + 256 * c;          // 0..511: row q / 32, chunk q % 32
+            const int r = q >> 5, ch = q & 31;
+            const double *src = P.gt.fqe + (size_t)(k0 + r) * NB + n0 + ch * 2;
+            cp_async16(&sm.B[buf][r][ch * 2], src, true);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
 
-    double acc[8][4];
+    double acc[4][4][2];
 #pragma unroll
-    for (int i = 0; i < 8; i++)
+    for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+        for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
 
+    if (kbeg < NB) load_tile(0, kbeg);
     int buf = 0;
-    if (kbeg < NB) {
-        fetch(kbeg);
-        stash(0);
-    }
-    __syncthreads();
 #pragma unroll 1
     for (int k0 = kbeg; k0 < NB; k0 += kGK) {
         const bool more = k0 + kGK < NB;
-        if (more) fetch(k0 + kGK);
-#pragma unroll
-        for (int kk = 0; kk < kGK; kk++) {
-            double av[8], bv[4];
-#pragma unroll
-            for (int i = 0; i < 8; i += 2) {
-                const double2 v = *reinterpret_cast<const double2 *>(&sm.A[buf][kk][ty * 8 + i]);
-                av[i] = v.x;
-                av[i + 1] = v.y;
-            }
-            const double2 b0 = *reinterpret_cast<const double2 *>(&sm.B[buf][kk][tx * 4]);
-            const double2 b1 = *reinterpret_cast<const double2 *>(&sm.B[buf][kk][tx * 4 + 2]);
-            bv[0] = b0.x; bv[1] = b0.y; bv[2] = b1.x; bv[3] = b1.y;
-#pragma unroll
-            for (int i = 0; i < 8; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        if (more) {
+            load_tile(buf ^ 1, k0 + kGK);
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         }
-        if (more) stash(buf ^ 1);
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kGK; kk += 4) {
+            double af[4], bf[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) af[i] = sm.A[buf][wm + 8 * i + gid][kk + tig];
+#pragma unroll
+            for (int j = 0; j < 4; j++) bf[j] = sm.B[buf][kk + tig][wn + 8 * j + gid];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
         __syncthreads();
         buf ^= 1;
     }
 
+    // epilogue: fragment (i, j) holds C[wm + 8i + gid][wn + 8j + 2 tig + {0, 1}]
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-        const int m = m0 + ty * 8 + i;
+    for (int i = 0; i < 4; i++) {
+        const int m = m0 + wm + 8 * i + gid;
         if (m >= nrows) continue;
         const int gi = m / P.nt, tl = m - gi * P.nt;
         const int t = P.t0 + tl;
         const SegInfo g = segment_of(P, t, P.g0 + gi);
         if (!g.active) continue;
         const double ng = (g.nseg > 1) ? lerp(a.bg_curr[t], a.bg_next[t], g.alpha) : a.bg_curr[t];
-        const int je = n0 + tx * 4;
-        double q[4] = {0.0, 0.0, 0.0, 0.0};
-        if (a.qepri) {
 #pragma unroll
-            for (int j = 0; j < 4; j++) q[j] = a.qepri[(size_t)t * NB + je + j];
+        for (int j = 0; j < 4; j++) {
+            const int je = n0 + wn + 8 * j + 2 * tig;
+            double q0 = 0.0, q1 = 0.0;
+            if (a.qepri) {
+                q0 = a.qepri[(size_t)t * NB + je];
+                q1 = a.qepri[(size_t)t * NB + je + 1];
+            }
+            *reinterpret_cast<double2 *>(P.inje + (size_t)m * NB + je) =
+                make_double2(acc[i][j][0] * kGyr * ng + q0, acc[i][j][1] * kGyr * ng + q1);
         }
-        double *o = P.inje + (size_t)m * NB + je;
-        *reinterpret_cast<double2 *>(o) =
-            make_double2(acc[i][0] * kGyr * ng + q[0], acc[i][1] * kGyr * ng + q[1]);
-        *reinterpret_cast<double2 *>(o + 2) =
-            make_double2(acc[i][2] * kGyr * ng + q[2], acc[i][3] * kGyr * ng + q[3]);
     }
 }
 
@@ -786,9 +812,7 @@ cudaError_t launch_factor(Context &ctx, const FusedParams &P)
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const long long warps = (long long)(P.g1 - P.g0) * P.sets * P.nt;
-    if (warps > 0x7fffffffLL) return cudaErrorInvalidValue;
-    long long blocks = (warps + kFacWarps - 1) / kFacWarps;
+    long long blocks = ((long long)P.nt + kFacWarps - 1) / kFacWarps;
     const long long full = (long long)nsm * resident;
     if (blocks > full) blocks = full;
     if (blocks < 1) return cudaSuccess;

@@ -168,9 +168,16 @@ class TracerFP:
                                                   _p(mass), _p(dis)))
         self.ntracer = n
 
-    def get_state(self):
-        crp = np.empty((self.ntracer, self.nb))
-        cre = np.empty((self.ntracer, self.nb))
+    def get_state(self, crp=None, cre=None):
+        """Spectra as cell-major host arrays; crp / cre may be given (e.g.
+        page-locked buffers) to be filled in place."""
+        if crp is None:
+            crp = np.empty((self.ntracer, self.nb))
+        if cre is None:
+            cre = np.empty((self.ntracer, self.nb))
+        for a in (crp, cre):
+            if a.shape != (self.ntracer, self.nb) or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("state buffers must be C-contiguous float64 [ntracer][nb]")
         self._check(self.lib.croma_b200_get_state(self.h, _p(crp), _p(cre)))
         return crp, cre
 
