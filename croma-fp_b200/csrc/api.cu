@@ -106,6 +106,19 @@ int ic_slot(Context &c, double z, int avoid_slot, double **out)
 }  // namespace
 }  // namespace croma
 
+namespace croma {
+namespace {
+// row[j] into every tracer's bin j; element (t, j) at base + t * ts + j * js
+__global__ void broadcast_rows_kernel(int n, const double *row, double *dst, size_t ts, size_t js)
+{
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (size_t)n * NB) return;
+    const size_t t = k / NB, j = k % NB;
+    dst[t * ts + j * js] = row[j];
+}
+}  // namespace
+}  // namespace croma
+
 using namespace croma;
 
 extern "C" {
@@ -206,7 +219,7 @@ int croma_b200_reserve(CromaB200Context *h, int ntracer)
     CROMA_CUDA(cudaMalloc(&c.d_mass, n * sizeof(double)));
     CROMA_CUDA(cudaMalloc(&c.d_dis, n));
     CROMA_CUDA(cudaMalloc(&c.d_bg, 2 * (size_t)kNbg * n * sizeof(double)));
-    CROMA_CUDA(cudaMalloc(&c.d_layout_tmp, st));
+    if (!cell_major(c)) CROMA_CUDA(cudaMalloc(&c.d_layout_tmp, st));   // host <-> momentum-major staging
     CROMA_CUDA(cudaMemsetAsync(c.d_crp, 0, st, c.stream));
     CROMA_CUDA(cudaMemsetAsync(c.d_cre, 0, st, c.stream));
     CROMA_CUDA(cudaMemsetAsync(c.d_qpi, 0, st, c.stream));
@@ -253,6 +266,43 @@ int croma_b200_set_state(CromaB200Context *h, int ntracer, const double *crp, co
     if (dis) CROMA_CUDA(cudaMemcpyAsync(c.d_dis, dis, ntracer, cudaMemcpyHostToDevice, c.stream));
     else CROMA_CUDA(cudaMemsetAsync(c.d_dis, 0, ntracer, c.stream));
     CROMA_CUDA(cudaStreamSynchronize(c.stream));
+    return 0;
+}
+
+int croma_b200_set_state_broadcast(CromaB200Context *h, int ntracer, const double *crp_row,
+                                   const double *cre_row, double mass_msun)
+{
+    if (!h || ntracer <= 0 || !crp_row || !cre_row) { set_error("invalid set_state_broadcast"); return -1; }
+    Context &c = h->impl;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    if (ntracer != c.cap) {
+        int rc = croma_b200_reserve(h, ntracer);
+        if (rc) return rc;
+    }
+    double *d_rows = nullptr;
+    CROMA_CUDA(cudaMalloc(&d_rows, 2 * NB * sizeof(double)));
+    cudaError_t e = cudaMemcpy(d_rows, crp_row, NB * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_rows + NB, cre_row, NB * sizeof(double), cudaMemcpyHostToDevice);
+    const size_t ts = cell_major(c) ? (size_t)NB : 1, js = cell_major(c) ? 1 : (size_t)ntracer;
+    const size_t total = (size_t)ntracer * NB;
+    const unsigned blocks = (unsigned)((total + 255) / 256);
+    if (e == cudaSuccess) {
+        broadcast_rows_kernel<<<blocks, 256, 0, c.stream>>>(ntracer, d_rows, c.d_crp, ts, js);
+        broadcast_rows_kernel<<<blocks, 256, 0, c.stream>>>(ntracer, d_rows + NB, c.d_cre, ts, js);
+        e = cudaGetLastError();
+    }
+    const size_t st = total * sizeof(double);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c.d_qpi, 0, st, c.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c.d_qepri, 0, st, c.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c.d_dis, 0, (size_t)ntracer, c.stream);
+    if (e == cudaSuccess) {
+        std::vector<double> m((size_t)ntracer, mass_msun);
+        e = cudaMemcpyAsync(c.d_mass, m.data(), (size_t)ntracer * sizeof(double), cudaMemcpyHostToDevice, c.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+    }
+    cudaFree(d_rows);
+    if (e != cudaSuccess) return cuda_fail(e, "set_state_broadcast");
+    c.has_sources = 0;
     return 0;
 }
 

@@ -72,6 +72,7 @@ def load_library(nb: int) -> C.CDLL:
     L.croma_b200_reset_kernel_stats.argtypes = [_vp]
     L.croma_b200_fp64_peak.argtypes = [P(_d)]
     L.croma_b200_get_sources.argtypes = [_vp, _vp, _vp, _vp]
+    L.croma_b200_set_state_broadcast.argtypes = [_vp, _i, _vp, _vp, _d]
     L.croma_b200_set_dsa.argtypes = [_vp, P(CromaB200DsaParams)]
     L.croma_b200_dsa_inject.argtypes = [_vp, P(CromaB200Shocks), _d, _d, _i, _i, P(_i)]
     _LIBS[nb] = L
@@ -167,6 +168,12 @@ class TracerFP:
         self._check(self.lib.croma_b200_set_state(self.h, n, _p(crp), _p(cre), _p(qpi), _p(qepri),
                                                   _p(mass), _p(dis)))
         self.ntracer = n
+
+    def set_state_broadcast(self, ntracer: int, crp_row, cre_row, mass: float = 1.0e7):
+        """Every tracer from the same seed rows [nb]."""
+        a, b = _c(crp_row), _c(cre_row)
+        self._check(self.lib.croma_b200_set_state_broadcast(self.h, int(ntracer), _p(a), _p(b), float(mass)))
+        self.ntracer = int(ntracer)
 
     def get_state(self, crp=None, cre=None):
         """Spectra as cell-major host arrays; crp / cre may be given (e.g.

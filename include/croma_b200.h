@@ -106,6 +106,10 @@ int croma_b200_set_state(CromaB200Context *ctx, int ntracer, const double *crp,
                          const double *cre, const double *qpi, const double *qepri,
                          const double *mass_msun, const unsigned char *disable_adiabatic);
 int croma_b200_get_state(CromaB200Context *ctx, double *crp, double *cre);
+/* Every tracer starts from the same seed spectra (host rows [nb]) and mass, as
+ * the reference's seed initialisation gives them; sources and flags zero. */
+int croma_b200_set_state_broadcast(CromaB200Context *ctx, int ntracer, const double *crp_row,
+                                   const double *cre_row, double mass_msun);
 /* The resident sources (cell-major host arrays [ntracer][nb]) and the
  * disable-adiabatic flags [ntracer]; NULL skips an array. */
 int croma_b200_get_sources(CromaB200Context *ctx, double *qpi, double *qepri, unsigned char *dis);
