@@ -40,7 +40,7 @@ UNIT = "tracer-snapshot updates/s"
 # proton and electron launches of an ncu capture of this workload at 32,768
 # tracers (profiles/steps_factor_secondary_batching_e_p_256.txt); traffic
 # scales with the tracer count (every tracer moves its own rows).
-NCU_DRAM_BYTES_PER_TRACER_STEPS_LAUNCH = (3.289135e9 + 1.119739e9 + 4.397054e9 + 0.114189e9) / 2 / 32768
+NCU_DRAM_BYTES_PER_TRACER_STEPS_LAUNCH = (3.289360e9 + 1.120041e9 + 4.395261e9 + 0.114444e9) / 2 / 32768
 
 
 def load_package():
