@@ -192,6 +192,11 @@ void croma_b200_destroy(CromaB200Context *h)
     cudaFree(c.d_err);
     free_ic_stage(c);
     free_dsa(c);
+    for (auto e : c.pipe_up) cudaEventDestroy(e);
+    for (auto e : c.pipe_done) cudaEventDestroy(e);
+    if (c.pipe_start) cudaEventDestroy(c.pipe_start);
+    if (c.h2d_stream) cudaStreamDestroy(c.h2d_stream);
+    if (c.d2h_stream) cudaStreamDestroy(c.d2h_stream);
     if (c.stream) cudaStreamDestroy(c.stream);
     delete h;
 }
@@ -349,10 +354,13 @@ int croma_b200_get_sources(CromaB200Context *h, double *qpi, double *qepri, unsi
     return check_err(c);
 }
 
-int croma_b200_snapshot(CromaB200Context *h, const CromaB200Snapshot *s, int sync)
+}  // extern "C"
+
+namespace croma {
+namespace {
+
+int snapshot_impl(Context &c, const CromaB200Snapshot *s, int sync)
 {
-    if (!h || !s || !s->bg_curr) { set_error("invalid snapshot arguments"); return -1; }
-    Context &c = h->impl;
     if (c.cap <= 0) { set_error("reserve/set_state before snapshot"); return -1; }
     if (!(s->dt_snap > 0.0)) { set_error("dt_snap must be positive"); return -1; }
     CROMA_CUDA(cudaSetDevice(c.device));
@@ -400,6 +408,118 @@ int croma_b200_snapshot(CromaB200Context *h, const CromaB200Snapshot *s, int syn
     if (rc) return rc;
     if (sync) return check_err(c);
     return 0;
+}
+
+// [from, to) appended to the chunk bounds in near-equal pieces of at most
+// maxc tracers.
+void push_split(std::vector<int> &b, int from, int to, int maxc)
+{
+    const long long len = (long long)to - from;
+    if (len <= 0) return;
+    const long long n = (len + maxc - 1) / maxc;
+    for (long long i = 1; i <= n; i++) b.push_back(from + (int)(len * i / n));
+}
+
+}  // namespace
+}  // namespace croma
+
+extern "C" {
+
+int croma_b200_snapshot(CromaB200Context *h, const CromaB200Snapshot *s, int sync)
+{
+    if (!h || !s || !s->bg_curr) { set_error("invalid snapshot arguments"); return -1; }
+    return snapshot_impl(h->impl, s, sync);
+}
+
+int croma_b200_snapshot_host(CromaB200Context *h, const CromaB200Snapshot *s, int ntracer, double *crp,
+                             double *cre, const double *mass, int chunks)
+{
+    if (!h || !s || !s->bg_curr || ntracer <= 0 || !crp || !cre) {
+        set_error("invalid snapshot_host arguments");
+        return -1;
+    }
+    Context &c = h->impl;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    if (!cell_major(c)) {
+        // momentum-major resident spectra go through the transposes: no overlap
+        int rc = croma_b200_set_state(h, ntracer, crp, cre, nullptr, nullptr, mass, nullptr);
+        if (!rc) rc = snapshot_impl(c, s, 1);
+        if (!rc) rc = croma_b200_get_state(h, crp, cre);
+        return rc;
+    }
+    if (ntracer != c.cap) {
+        const int rc = croma_b200_reserve(h, ntracer);
+        if (rc) return rc;
+    }
+    if (c.fused_chunk <= 0) { set_error("fused workspace not reserved"); return -1; }
+    HostPipe pipe;
+    pipe.crp = crp;
+    pipe.cre = cre;
+    pipe.down_p = (c.mp.species_mask & CROMA_SPECIES_PROTON) != 0;
+    pipe.down_e = (c.mp.species_mask & CROMA_SPECIES_ELECTRON) != 0;
+    // chunk bounds: by default an eighth at each end, so that only a small
+    // upload precedes the first kernels and a small download follows the
+    // last, and the middle in pieces the workspace holds
+    pipe.bounds.push_back(0);
+    if (chunks > 0) {
+        const long long k = chunks < ntracer ? chunks : ntracer;
+        int prev = 0;
+        for (long long i = 1; i <= k; i++) {
+            const int next = (int)((long long)ntracer * i / k);
+            push_split(pipe.bounds, prev, next, c.fused_chunk);
+            prev = next;
+        }
+    } else if (ntracer >= 8192) {
+        const int edge = ntracer / 8;
+        push_split(pipe.bounds, 0, edge, c.fused_chunk);
+        push_split(pipe.bounds, edge, ntracer - edge, c.fused_chunk);
+        push_split(pipe.bounds, ntracer - edge, ntracer, c.fused_chunk);
+    } else {
+        push_split(pipe.bounds, 0, ntracer, c.fused_chunk);
+    }
+    const int nchunk = (int)pipe.bounds.size() - 1;
+    if (!c.h2d_stream) CROMA_CUDA(cudaStreamCreateWithFlags(&c.h2d_stream, cudaStreamNonBlocking));
+    if (!c.d2h_stream) CROMA_CUDA(cudaStreamCreateWithFlags(&c.d2h_stream, cudaStreamNonBlocking));
+    if (!c.pipe_start) CROMA_CUDA(cudaEventCreateWithFlags(&c.pipe_start, cudaEventDisableTiming));
+    while ((int)c.pipe_up.size() < nchunk) {
+        cudaEvent_t u = nullptr, d = nullptr;
+        CROMA_CUDA(cudaEventCreateWithFlags(&u, cudaEventDisableTiming));
+        c.pipe_up.push_back(u);
+        CROMA_CUDA(cudaEventCreateWithFlags(&d, cudaEventDisableTiming));
+        c.pipe_done.push_back(d);
+    }
+    // the rest of the state as set_state with these arguments leaves it
+    const size_t st = (size_t)NB * ntracer * sizeof(double);
+    CROMA_CUDA(cudaMemsetAsync(c.d_qpi, 0, st, c.stream));
+    CROMA_CUDA(cudaMemsetAsync(c.d_qepri, 0, st, c.stream));
+    c.has_sources = 0;
+    if (mass) CROMA_CUDA(cudaMemcpyAsync(c.d_mass, mass, ntracer * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    CROMA_CUDA(cudaMemsetAsync(c.d_dis, 0, ntracer, c.stream));
+    // uploads, chunk by chunk, after whatever the compute stream still runs
+    CROMA_CUDA(cudaEventRecord(c.pipe_start, c.stream));
+    CROMA_CUDA(cudaStreamWaitEvent(c.h2d_stream, c.pipe_start, 0));
+    int rc = 0;
+    for (int k = 0; k < nchunk && !rc; k++) {
+        const size_t off = (size_t)pipe.bounds[k] * NB;
+        const size_t bytes = (size_t)(pipe.bounds[k + 1] - pipe.bounds[k]) * NB * sizeof(double);
+        cudaError_t e = cudaMemcpyAsync(c.d_crp + off, crp + off, bytes, cudaMemcpyHostToDevice, c.h2d_stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(c.d_cre + off, cre + off, bytes, cudaMemcpyHostToDevice, c.h2d_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c.pipe_up[k], c.h2d_stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "snapshot_host upload");
+    }
+    if (!rc) {
+        c.pipe = &pipe;
+        rc = snapshot_impl(c, s, 0);
+        c.pipe = nullptr;
+    }
+    // the host rows stay in use until both copy streams have drained
+    const cudaError_t e1 = cudaStreamSynchronize(c.h2d_stream);
+    const cudaError_t e2 = cudaStreamSynchronize(c.d2h_stream);
+    if (rc) return rc;
+    if (e1 != cudaSuccess) return cuda_fail(e1, "snapshot_host uploads");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "snapshot_host downloads");
+    return check_err(c);
 }
 
 int croma_b200_set_dsa(CromaB200Context *h, const CromaB200DsaParams *params)

@@ -47,6 +47,16 @@ struct SnapArgs {
     unsigned *err;
 };
 
+// One host-buffer snapshot in flight: the cell-major spectra of tracer chunk
+// k, [bounds[k], bounds[k+1]), are uploaded on the context's h2d stream
+// (event pipe_up[k]) and, once the chunk is evolved (event pipe_done[k] on
+// the compute stream), downloaded into the same host rows on d2h.
+struct HostPipe {
+    double *crp = nullptr, *cre = nullptr;   // host [ntracer][nb]
+    int down_p = 1, down_e = 1;              // species whose rows come back
+    std::vector<int> bounds;                 // chunk starts, then ntracer
+};
+
 struct ModelParams {
     int species_mask;
     int dpp_model;
@@ -132,6 +142,13 @@ struct Context {
     double *d_dsa_stage = nullptr;    // [10][dsa_stage_cap] host shock fields
     int dsa_stage_cap = 0;
     double *d_layout_tmp = nullptr;   // [nb][cap] transpose staging
+
+    // host-buffer snapshot (croma_b200_snapshot_host): copy streams and
+    // per-chunk events, created on first use; pipe is set for one call
+    cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;
+    std::vector<cudaEvent_t> pipe_up, pipe_done;
+    cudaEvent_t pipe_start = nullptr;   // compute stream's earlier work, gating the uploads
+    const HostPipe *pipe = nullptr;
 
     unsigned *d_err = nullptr;
     int last_launches = 0;

@@ -968,9 +968,22 @@ static int fused_chunks(Context &ctx, FusedParams &P, int nslots)
     const bool cap = ctx.mp.eta_dpp_cap > 0.0 && isfinite(ctx.mp.eta_dpp_cap) && ctx.mp.dpp_model != kDppOff;
     P.sets = ctx.fused_sets;
     P.fac = ctx.d_fac;
-    for (int t0 = 0; t0 < P.a.ntracer; t0 += ctx.fused_chunk) {
-        P.t0 = t0;
-        P.nt = P.a.ntracer - t0 < ctx.fused_chunk ? P.a.ntracer - t0 : ctx.fused_chunk;
+    // chunks: the workspace's uniform split, or the host pipeline's bounds
+    // (each within the workspace chunk), whose uploads gate the chunk and
+    // whose downloads follow it
+    const HostPipe *pipe = ctx.pipe;
+    const int nchunk = pipe ? (int)pipe->bounds.size() - 1
+                            : (P.a.ntracer + ctx.fused_chunk - 1) / ctx.fused_chunk;
+    for (int k = 0; k < nchunk; k++) {
+        P.t0 = pipe ? pipe->bounds[k] : k * ctx.fused_chunk;
+        const int t1 = pipe ? pipe->bounds[k + 1]
+                            : (P.a.ntracer - P.t0 < ctx.fused_chunk ? P.a.ntracer : P.t0 + ctx.fused_chunk);
+        P.nt = t1 - P.t0;
+        if (P.nt <= 0 || P.nt > ctx.fused_chunk) {
+            set_error("internal: tracer chunk outside the fused workspace");
+            return -1;
+        }
+        if (pipe) CROMA_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.pipe_up[k], 0));
         if (!cap) {
             const int rc = fused_range(ctx, P, 0, nslots);
             if (rc) return rc;
@@ -979,6 +992,17 @@ static int fused_chunks(Context &ctx, FusedParams &P, int nslots)
                 const int rc = fused_range(ctx, P, g, g + 1);
                 if (rc) return rc;
             }
+        }
+        if (pipe) {
+            CROMA_CUDA(cudaEventRecord(ctx.pipe_done[k], ctx.stream));
+            CROMA_CUDA(cudaStreamWaitEvent(ctx.d2h_stream, ctx.pipe_done[k], 0));
+            const size_t off = (size_t)P.t0 * NB, bytes = (size_t)P.nt * NB * sizeof(double);
+            if (pipe->down_p)
+                CROMA_CUDA(cudaMemcpyAsync(pipe->crp + off, P.a.crp + off, bytes, cudaMemcpyDeviceToHost,
+                                           ctx.d2h_stream));
+            if (pipe->down_e)
+                CROMA_CUDA(cudaMemcpyAsync(pipe->cre + off, P.a.cre + off, bytes, cudaMemcpyDeviceToHost,
+                                           ctx.d2h_stream));
         }
     }
     return 0;

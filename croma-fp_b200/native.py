@@ -58,6 +58,7 @@ def load_library(nb: int) -> C.CDLL:
     L.croma_b200_set_state.argtypes = [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp]
     L.croma_b200_get_state.argtypes = [_vp, _vp, _vp]
     L.croma_b200_snapshot.argtypes = [_vp, P(CromaB200Snapshot), _i]
+    L.croma_b200_snapshot_host.argtypes = [_vp, P(CromaB200Snapshot), _i, _vp, _vp, _vp, _i]
     L.croma_b200_get_schedule.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.croma_b200_ic_row.argtypes = [_vp, _d, _vp]
     L.croma_b200_get_grid.argtypes = [_vp, _i, _vp]
@@ -210,6 +211,34 @@ class TracerFP:
         s.dt_snap, s.elapsed_gyr = dt, elapsed
         self._check(self.lib.croma_b200_snapshot(self.h, C.byref(s), int(bool(sync))))
         del keep
+
+    def snapshot_host(self, crp, cre, bg_curr, bg_next, z_curr, z_next, allow, dt, elapsed, mass=None,
+                      chunks=0):
+        """One snapshot from host spectra to host spectra with the copies
+        overlapped with the evolve (croma_b200_snapshot_host).  crp / cre are
+        C-contiguous float64 [ntracer][nb] host arrays, overwritten in place
+        with the evolved spectra (page-locked ones let the copies overlap);
+        bg_* are host arrays [8][ntracer]."""
+        for a in (crp, cre):
+            if a.ndim != 2 or a.shape[1] != self.nb or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("state buffers must be C-contiguous float64 [ntracer][nb]")
+        if crp.shape != cre.shape:
+            raise ValueError("crp and cre must have the same shape")
+        n = crp.shape[0]
+        m = _c(mass)
+        if m is not None and m.shape != (n,):
+            raise ValueError("mass must have one value per tracer")
+        bc = _c(bg_curr)
+        bn = _c(bg_next) if bg_next is not None else bc
+        if bc.size != 8 * n or bn.size != 8 * n:
+            raise ValueError("backgrounds must be [8][ntracer]")
+        s = CromaB200Snapshot()
+        s.bg_curr, s.bg_next, s.bg_on_device = bc.ctypes.data, bn.ctypes.data, 0
+        s.z_curr, s.z_next, s.allow_interp = z_curr, z_next, int(bool(allow))
+        s.dt_snap, s.elapsed_gyr = dt, elapsed
+        self._check(self.lib.croma_b200_snapshot_host(self.h, C.byref(s), n, _p(crp), _p(cre), _p(m),
+                                                      int(chunks)))
+        self.ntracer = n
 
     def sync(self):
         self._check(self.lib.croma_b200_sync(self.h))

@@ -117,6 +117,21 @@ int croma_b200_get_sources(CromaB200Context *ctx, double *qpi, double *qepri, un
 /* One snapshot on the context's stream; asynchronous unless sync != 0. */
 int croma_b200_snapshot(CromaB200Context *ctx, const CromaB200Snapshot *snap, int sync);
 
+/* One snapshot from host spectra to host spectra: the same result and
+ * resident state as set_state(crp, cre, NULL, NULL, mass, NULL), snapshot,
+ * get_state(crp, cre), with the copies overlapped with the evolve.  The
+ * tracers run in chunks: the upload of later chunks and the download of
+ * earlier ones proceed on two copy streams while a chunk is evolved (the
+ * cell-major fused path; the plain path runs the three calls in turn).
+ * crp / cre ([ntracer][nb], cell-major) are read and overwritten with the
+ * evolved spectra; a species the mask does not evolve is not copied back.
+ * Page-locked host memory is needed for the copies to overlap.
+ * chunks <= 0: an eighth of the tracers at each end and the middle in
+ * workspace-sized pieces; otherwise that many near-equal chunks.
+ * Synchronous: returns after the last download. */
+int croma_b200_snapshot_host(CromaB200Context *ctx, const CromaB200Snapshot *snap, int ntracer,
+                             double *crp, double *cre, const double *mass_msun, int chunks);
+
 /* Schedule of the last snapshot (host arrays of ntracer ints); NULL skips. */
 int croma_b200_get_schedule(CromaB200Context *ctx, int *nsub, int *n_on, int *target_nsub,
                             int *bucket_ids, int *bucket_indices, int *nbuckets);
