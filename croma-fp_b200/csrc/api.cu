@@ -62,8 +62,9 @@ void free_state(Context &c)
     c.d_dis = nullptr;
     cudaFree(c.d_coef); cudaFree(c.d_inje); cudaFree(c.d_seg_ngas); cudaFree(c.d_eta_scale);
     c.d_coef = c.d_inje = c.d_seg_ngas = c.d_eta_scale = nullptr;
-    cudaFree(c.d_fac); cudaFree(c.d_np_seg);
+    cudaFree(c.d_fac); cudaFree(c.d_np_seg); cudaFree(c.d_segpre);
     c.d_fac = c.d_np_seg = nullptr;
+    c.d_segpre = nullptr;
     c.fused_chunk = c.fused_nseg = c.fused_sets = 0;
     cudaFree(c.d_sched_int); cudaFree(c.d_capped); cudaFree(c.d_cub_tmp);
     cudaFree(c.d_keys); cudaFree(c.d_vals);

@@ -62,6 +62,7 @@ struct SpeciesTables {
     const double *inv_dxl;      // 1 / (p[j] - p[j-1])   (j >= 1)
     const double *inv_dxr;      // 1 / (p[j+1] - p[j])   (j <= nb-2)
     const double *dxf;          // p[j+1] - p[j]         (j <= nb-2), face widths
+    const double *face_rf;      // dxf[j] / (g[j] + g[j+1]), g = p^2 expE exp(-1/p) (j <= nb-2)
     double pm1, pp1;
     double pm1_p2, pp1_p2, pm1_exp_cut, pp1_exp_cut;
     double expE_m1, expE_p1;    // exp(-m_p sqrt(1+p^2)/E_max) at the ghost edges

@@ -3,6 +3,9 @@
 // sub-step of every segment with the spectrum held in registers.
 //
 // Per chunk of tracers (sized to the workspace budget) and species:
+//   0. seg_pre_kernel, one thread per (segment, tracer): the segment's
+//      interpolated background and the scalars of its coefficients, once for
+//      both species.
 //   1. factor_kernel, one warp per (segment, tracer[, on/off set]): the loss /
 //      diffusion terms of every bin and the Chang-Cooper face weights in
 //      rolled lane-strided loops into the warp's slice of shared memory
@@ -48,12 +51,25 @@ constexpr int kFacDoubles = 3 * NB;  // 1/d, a/d, c/d of one system
 constexpr int kFacWarps = 8;         // warps per factor-kernel block
 
 // Grid tables of one species staged in shared memory by the factor kernel.
-// X0..X4: protons expE, cp_Ep, cp_inv2mpkin, cp_inv_betap2, sig_eff;
-// electrons ce_inv_beta2, ce_logp and the shared IC rows of z_curr, z_next.
-enum { TB_P, TB_P2, TB_CUT, TB_2P, TB_DXF, TB_X0, TB_X1, TB_X2, TB_X3, TB_X4,
+// X0..X3: protons expE, cp_Ep, cp_inv2mpkin, cp_inv_betap2; electrons
+// ce_inv_beta2, ce_logp and the shared IC rows of z_curr, z_next.  RF: the
+// face factor dx / (g_j + g_j+1) of the filled Dpp form.
+enum { TB_P, TB_P2, TB_CUT, TB_2P, TB_DXF, TB_RF, TB_X0, TB_X1, TB_X2, TB_X3,
+       TB_X4,                      // protons sig_eff, in swizzled order (row loss term)
        TB_IDX, TB_IDXL, TB_IDXR,   // 1/dp, 1/(p[m]-p[m-1]), 1/(p[m+1]-p[m]) in swizzled order
        kTab };
 constexpr int kTabStride = (NB > kSw ? NB : kSw);   // doubles per staged table
+
+// Per-segment scalars of one (segment slot, tracer): what the factor kernels
+// of both species need of the schedule's segment and of the background
+// interpolated to it, computed once by seg_pre_kernel.
+struct SegPre {
+    double n_gas, kbt, inv_kbt, log_n, adiab, synch_coeff, coulomb_coeff;
+    double dt, dt_over_tloss_pref, dtT_e, alpha, dpp_inv;
+    int flags;               // bit 0 active, 1 windowed, 2 interpolated, 3 "on" Dpp filled
+    int sl, el, steps;       // Dpp window within the segment, sub-steps
+};
+enum { kPreActive = 1, kPreWindowed = 2, kPreInterp = 4, kPreFill = 8 };
 
 struct FusedParams {
     SnapArgs a;              // spectra and sources cell-major [tracer][nb]
@@ -71,6 +87,7 @@ struct FusedParams {
     int ic_stride;
     const double *eta_scale; // [ntracer] Dpp eta-cap scale of slot g0, or null (no cap)
     double *fac;             // [2 species][g1 - g0][sets][nt][3][nb]
+    SegPre *pre;             // [g1 - g0][nt]
     double *np_seg;          // [g1 - g0][nt][nb] proton spectra at segment starts, or null
     double *inje;            // [g1 - g0][nt][nb] electron source per segment, or null
     const int *np_min_qe;    // [nb]
@@ -125,9 +142,9 @@ struct SegTerms {
     double alpha;
     int interp;
 
-    // B = radp - 2 Dpp / p, C = Dpp, dT = dt / tloss at bin j, from the grid
-    // tables staged in shared memory (tab, kTab arrays of nb)
-    __device__ __forceinline__ void at(const double *tab, int j, double &B, double &C, double &dT) const
+    // B = radp - 2 Dpp / p and C = Dpp at bin j, from the grid tables staged
+    // in shared memory (tab, kTab arrays of nb)
+    __device__ __forceinline__ void at(const double *tab, int j, double &B, double &C) const
     {
         const double p = tab[TB_P * kTabStride + j];
         const double p2 = tab[TB_P2 * kTabStride + j];
@@ -147,7 +164,6 @@ struct SegTerms {
                 ? 0.0
                 : kGyr * kC / (kMp * kGeV) * sum * n_gas * tab[TB_X3 * kTabStride + j] * thermal * 3.5e-29;
             radp = coul + adiab * p;
-            dT = tab[TB_X4 * kTabStride + j] * dt_over_tloss_pref;
         } else {
             double r0, r1;
             if (ric_stride == 0) {
@@ -162,10 +178,16 @@ struct SegTerms {
             const double coulomb = coulomb_coeff * (1.0 + (tab[TB_X1 * kTabStride + j] - log_n) * (1.0 / 74.8)) *
                                    tab[TB_X0 * kTabStride + j];
             radp = synch_coeff * p2 + r + coulomb + adiab * p;
-            dT = dtT_e;
         }
         B = radp - tab[TB_2P * kTabStride + j] * D;
         C = D;
+    }
+
+    // dT = dt / tloss of row r of a lane's block (swizzled index r * 33 + lane)
+    __device__ __forceinline__ double row_dT(const double *tab, int r, int lane) const
+    {
+        if (S == 0) return tab[TB_X4 * kTabStride + r * 33 + lane] * dt_over_tloss_pref;
+        return dtT_e;
     }
 };
 
@@ -198,9 +220,36 @@ __device__ __forceinline__ SegTerms<S> seg_terms(const GridTables &gt, const Bg 
     return T;
 }
 
+// SegTerms of species S from the precomputed scalars of the segment.
+template <int S>
+__device__ __forceinline__ SegTerms<S> seg_terms_pre(const GridTables &gt, const SegPre *__restrict__ p,
+                                                     const SnapArgs &a, int t, int ic_stride)
+{
+    SegTerms<S> T;
+    T.gt = &gt;
+    T.n_gas = p->n_gas;
+    T.kbt = p->kbt;
+    T.inv_kbt = p->inv_kbt;
+    T.log_n = p->log_n;
+    T.adiab = p->adiab;
+    T.synch_coeff = p->synch_coeff;
+    T.coulomb_coeff = p->coulomb_coeff;
+    T.dt = p->dt;
+    T.dt_over_tloss_pref = p->dt_over_tloss_pref;
+    T.dtT_e = p->dtT_e;
+    T.ric = a.ic_curr + (ic_stride ? t : 0);
+    T.ric_next = a.ic_next + (ic_stride ? t : 0);
+    T.ric_stride = ic_stride;
+    T.alpha = p->alpha;
+    T.interp = (p->flags & kPreInterp) ? 1 : 0;
+    T.dpp_inv = 0.0;
+    T.dpp_scale = 1.0;
+    T.dpp_fill = 0;
+    return T;
+}
+
 struct WarpSmem {
-    double B[kSw], C[kSw], D[kSw], Wp[kSw], Wm[kSw];
-    double bg[2][kNbg];     // the tracer's current and next background rows
+    double B[kSw], C[kSw], Wp[kSw], Wm[kSw];
 };
 
 
@@ -217,14 +266,17 @@ __device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int la
 #pragma unroll 2
     for (int k = 0; k < kR; k++) {
         const int j = k * 32 + lane;
-        double B, C, D;
-        T.at(tab, j, B, C, D);
+        double B, C;
+        T.at(tab, j, B, C);
         sm.B[swz(j)] = B;
         sm.C[swz(j)] = C;
-        sm.D[swz(j)] = D;
     }
     __syncwarp();
-    // faces j (between bins j and j+1), lane-strided
+    // faces j (between bins j and j+1), lane-strided.  The drift / diffusion
+    // ratio (B_j + B_j+1) / (C_j + C_j+1) * dx: with the filled Dpp form the C
+    // sum is kappa times a grid factor, so the division becomes a product with
+    // the tabulated dx / (g_j + g_j+1) and 1 / kappa (equal to a few ulp).
+    const double inv_kappa = T.dpp_fill ? 1.0 / (T.dpp_inv * T.dpp_scale) : 0.0;
 #pragma unroll 2
     for (int k = 0; k < kR; k++) {
         const int j = k * 32 + lane;
@@ -232,8 +284,11 @@ __device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int la
         if (j <= NB - 2) {
             const double cl = sm.C[swz(j)];
             if (fabs(cl) > 1.0e-200) {
-                const double w = (sm.B[swz(j)] + sm.B[swz(j + 1)]) / (cl + sm.C[swz(j + 1)]) *
-                                 tab[TB_DXF * kTabStride + j];
+                const double bsum = sm.B[swz(j)] + sm.B[swz(j + 1)];
+                const double rf = tab[TB_RF * kTabStride + j] * inv_kappa;
+                const double w = (T.dpp_fill && isfinite(rf))
+                                     ? bsum * rf
+                                     : bsum / (cl + sm.C[swz(j + 1)]) * tab[TB_DXF * kTabStride + j];
                 face_weights_fast(w, wp, wm);
             }
         }
@@ -249,7 +304,7 @@ __device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int la
     for (int r = 0; r < kR; r++) {
         const int m = row0 + r;
         const double k = T.dt * tab[TB_IDX * kTabStride + r * 33 + lane];
-        const double Cm = sm.C[r * 33 + lane], Bm = sm.B[r * 33 + lane], Dm = sm.D[r * 33 + lane];
+        const double Cm = sm.C[r * 33 + lane], Bm = sm.B[r * 33 + lane], Dm = T.row_dT(tab, r, lane);
         double av = 0.0, bv, cv = 0.0;
         if (m == 0) {
             const double nC = sm.C[swz(1)], nB = sm.B[swz(1)];
@@ -372,18 +427,19 @@ __global__ void __launch_bounds__(kFacWarps * 32, (NB <= 256 ? 2 : 1)) factor_ke
         tab[TB_CUT * kTabStride + i] = st.exp_cut[i];
         tab[TB_2P * kTabStride + i] = st.two_over_p[i];
         tab[TB_DXF * kTabStride + i] = st.dxf[i];
+        tab[TB_RF * kTabStride + i] = st.face_rf[i];
         if (S == 0) {
             tab[TB_X0 * kTabStride + i] = st.expE[i];
             tab[TB_X1 * kTabStride + i] = P.gt.cp_Ep[i];
             tab[TB_X2 * kTabStride + i] = P.gt.cp_inv2mpkin[i];
             tab[TB_X3 * kTabStride + i] = P.gt.cp_inv_betap2[i];
-            tab[TB_X4 * kTabStride + i] = P.gt.sig_eff[i];
+            tab[TB_X4 * kTabStride + swz(i)] = P.gt.sig_eff[i];
         } else {
             tab[TB_X0 * kTabStride + i] = P.gt.ce_inv_beta2[i];
             tab[TB_X1 * kTabStride + i] = P.gt.ce_logp[i];
             tab[TB_X2 * kTabStride + i] = (P.ic_stride == 0) ? a.ic_curr[i] : 0.0;
             tab[TB_X3 * kTabStride + i] = (P.ic_stride == 0) ? a.ic_next[i] : 0.0;
-            tab[TB_X4 * kTabStride + i] = 0.0;
+            tab[TB_X4 * kTabStride + swz(i)] = 0.0;
         }
         tab[TB_IDX * kTabStride + swz(i)] = st.inv_dx[i];
         tab[TB_IDXL * kTabStride + swz(i)] = st.inv_dxl[i];
@@ -391,44 +447,35 @@ __global__ void __launch_bounds__(kFacWarps * 32, (NB <= 256 ? 2 : 1)) factor_ke
     }
     __syncthreads();
     // a warp takes one tracer at a time and factors all its segments (and
-    // on/off sets): the schedule entries and both background rows are read
-    // once per tracer (lanes 0-15 fetch one value each, shuffles spread them)
+    // on/off sets) from the segments' precomputed scalars
     const int stride = gridDim.x * kFacWarps;
     const int nslot = P.g1 - P.g0;
 #pragma unroll 1
     for (int tl = blockIdx.x * kFacWarps + w; tl < P.nt; tl += stride) {
         const int t = P.t0 + tl;
-        int nseg = 0, nsub = 0, non = 0;
-        if (!P.explicit_seg) {
-            nseg = a.sched.nseg[t];
-            nsub = a.sched.nsub[t];
-            non = a.sched.non[t];
-        }
         WarpSmem &ws = smem[w];
-        __syncwarp();
-        if (lane < kNbg) ws.bg[0][lane] = a.bg_curr[(size_t)lane * a.ntracer + t];
-        else if (lane < 2 * kNbg) ws.bg[1][lane - kNbg] = a.bg_next[(size_t)(lane - kNbg) * a.ntracer + t];
-        __syncwarp();
-        const int dis = a.dis ? a.dis[t] : 0;
         const double eta = (P.mp.dpp_model != kDppOff && P.eta_scale) ? P.eta_scale[t] : 1.0;
 #pragma unroll 1
         for (int gi = 0; gi < nslot; gi++) {
-            const SegInfo g = P.explicit_seg ? P.ex : seg_info_of(nseg, nsub, non, P.g0 + gi, a.dt_snap);
-            if (!g.active) break;
+            const SegPre *__restrict__ pre = P.pre + (size_t)gi * P.nt + tl;
+            const int flags = pre->flags;
+            if (!(flags & kPreActive)) break;
+            SegInfo g{};
+            g.windowed = (flags & kPreWindowed) ? 1 : 0;
+            g.sl = pre->sl;
+            g.el = pre->el;
+            g.steps = pre->steps;
             if (needs_set(g, 1) && P.sets < 2) {   // checked on the host; never write past the sets
                 if (lane == 0) atomicOr(a.err, kErrBadInput);
                 continue;
             }
-            const Bg bg = lerp_bg(ws.bg[0], ws.bg[1], g);
 #pragma unroll 1
             for (int set = 0; set < P.sets; set++) {
                 if (!needs_set(g, set)) continue;
-                SegTerms<S> T = seg_terms<S>(P.gt, bg, dis, a, g, t, P.ic_stride);
+                SegTerms<S> T = seg_terms_pre<S>(P.gt, pre, a, t, P.ic_stride);
                 if (set == 0) {
-                    const double tacc = segment_tacc(P.mp, a, g);
-                    const DppForm on = dpp_form(P.mp, P.mp.dpp_model, bg, tacc);
-                    T.dpp_fill = on.fill;
-                    T.dpp_inv = on.inv;
+                    T.dpp_fill = (flags & kPreFill) ? 1 : 0;
+                    T.dpp_inv = pre->dpp_inv;
                     T.dpp_scale = eta;
                 }
                 const unsigned err = factor_store<S>(T, tab, lane, ws, fac_ptr(P, S, gi, set, tl));
@@ -615,6 +662,49 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) steps_kernel
 #pragma unroll
     for (int r = 0; r < kR; r += 2)
         *reinterpret_cast<double2 *>(Nrow + r) = make_double2(N[r], N[r + 1]);
+}
+
+// The per-segment scalars of every (slot, tracer) of the chunk, one thread
+// each: the schedule's segment (tracer_fp_batch.c segment split), the
+// background interpolated to it, the loss coefficients and the "on" Dpp form
+// (prepare_momentumdiff_cell_major, src/fp_shared_core.c:1241-1317) -- the
+// same arithmetic the factor kernels would repeat per species and set.
+__global__ void __launch_bounds__(256) seg_pre_kernel(FusedParams P)
+{
+    const SnapArgs &a = P.a;
+    const long long total = (long long)(P.g1 - P.g0) * P.nt;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int gi = (int)(i / P.nt);
+        const int tl = (int)(i - (long long)gi * P.nt);
+        const int t = P.t0 + tl;
+        SegPre o{};
+        const SegInfo g = segment_of(P, t, P.g0 + gi);
+        if (g.active) {
+            const Bg bg = load_bg(a, t, g);
+            const int dis = a.dis ? a.dis[t] : 0;
+            const SegTerms<0> T = seg_terms<0>(P.gt, bg, dis, a, g, t, P.ic_stride);
+            const DppForm on = dpp_form(P.mp, P.mp.dpp_model, bg, segment_tacc(P.mp, a, g));
+            o.n_gas = T.n_gas;
+            o.kbt = T.kbt;
+            o.inv_kbt = T.inv_kbt;
+            o.log_n = T.log_n;
+            o.adiab = T.adiab;
+            o.synch_coeff = T.synch_coeff;
+            o.coulomb_coeff = T.coulomb_coeff;
+            o.dt = T.dt;
+            o.dt_over_tloss_pref = T.dt_over_tloss_pref;
+            o.dtT_e = T.dtT_e;
+            o.alpha = T.alpha;
+            o.dpp_inv = on.inv;
+            o.flags = kPreActive | (g.windowed ? kPreWindowed : 0) | (T.interp ? kPreInterp : 0) |
+                      (on.fill ? kPreFill : 0);
+            o.sl = g.sl;
+            o.el = g.el;
+            o.steps = g.steps;
+        }
+        P.pre[i] = o;
+    }
 }
 
 // Dpp eta-cap scale of every tracer of the chunk with a segment in slot g0,
@@ -854,7 +944,7 @@ WorkspaceShape workspace_shape(const ModelParams &mp, int cap, double workspace_
     WorkspaceShape w;
     w.nseg = mp.interp_max_segments < 1 ? 1 : (mp.interp_max_segments > 64 ? 64 : mp.interp_max_segments);
     w.sets = mp.window_centred ? 2 : 1;
-    w.per_tracer = 8.0 * NB * ((double)2 * w.nseg * w.sets * 3 + 2.0 * w.nseg);
+    w.per_tracer = 8.0 * NB * ((double)2 * w.nseg * w.sets * 3 + 2.0 * w.nseg) + (double)w.nseg * sizeof(SegPre);
     const double budget = workspace_cap > 0.0 ? workspace_cap : workspace_budget_bytes();
     w.chunk = (long long)(budget / w.per_tracer);
     if (w.chunk < 1) w.chunk = 1;
@@ -879,13 +969,16 @@ int fused_reserve(Context &ctx, int cap)
     cudaFree(ctx.d_eta_scale);
     cudaFree(ctx.d_fac);
     cudaFree(ctx.d_np_seg);
+    cudaFree(ctx.d_segpre);
     ctx.d_inje = ctx.d_eta_scale = ctx.d_fac = ctx.d_np_seg = nullptr;
+    ctx.d_segpre = nullptr;
     ctx.fused_chunk = ctx.fused_nseg = ctx.fused_sets = 0;
     const size_t rows = (size_t)nseg * chunk * NB;
     CROMA_CUDA(cudaMalloc(&ctx.d_fac, (size_t)2 * sets * rows * 3 * sizeof(double)));
     CROMA_CUDA(cudaMalloc(&ctx.d_np_seg, rows * sizeof(double)));
     CROMA_CUDA(cudaMalloc(&ctx.d_inje, rows * sizeof(double)));
     CROMA_CUDA(cudaMalloc(&ctx.d_eta_scale, (size_t)cap * sizeof(double)));
+    CROMA_CUDA(cudaMalloc(&ctx.d_segpre, (size_t)nseg * chunk * sizeof(SegPre)));
     ctx.fused_chunk = (int)chunk;
     ctx.fused_nseg = nseg;
     ctx.fused_sets = sets;
@@ -917,6 +1010,16 @@ static int fused_range(Context &ctx, FusedParams &P, int g0, int g1)
         eta_scale_kernel<<<(P.nt + 3) / 4, 128, 0, ctx.stream>>>(P, ctx.d_eta_scale);
         ctx.last_launches += 1;
         P.eta_scale = ctx.d_eta_scale;
+    }
+    if (protons || electrons) {
+        const long long total = (long long)(g1 - g0) * P.nt;
+        int dev = 0, nsm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        long long blocks = (total + 255) / 256;
+        if (blocks > 8LL * nsm) blocks = 8LL * nsm;
+        seg_pre_kernel<<<(unsigned)blocks, 256, 0, ctx.stream>>>(P);
+        ctx.last_launches += 1;
     }
     if (protons) {
         CROMA_CUDA(launch_factor<0>(ctx, P));
@@ -968,6 +1071,7 @@ static int fused_chunks(Context &ctx, FusedParams &P, int nslots)
     const bool cap = ctx.mp.eta_dpp_cap > 0.0 && isfinite(ctx.mp.eta_dpp_cap) && ctx.mp.dpp_model != kDppOff;
     P.sets = ctx.fused_sets;
     P.fac = ctx.d_fac;
+    P.pre = static_cast<SegPre *>(ctx.d_segpre);
     // chunks: the workspace's uniform split, or the host pipeline's bounds
     // (each within the workspace chunk), whose uploads gate the chunk and
     // whose downloads follow it

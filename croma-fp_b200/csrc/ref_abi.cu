@@ -479,6 +479,7 @@ void cuda_pipeline_workspace_destroy(FpCudaPipelineWorkspace *w)
     cudaFree(c.d_eta_scale);
     cudaFree(c.d_fac);
     cudaFree(c.d_np_seg);
+    cudaFree(c.d_segpre);
     cudaFree(c.d_tables);
     cudaFree(c.d_np_min_qe);
     cudaFree(c.d_err);

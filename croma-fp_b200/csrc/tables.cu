@@ -165,7 +165,7 @@ int build_tables(Context &ctx)
     }
 
     // ---- caches, FP_Coef.c:77-156 and the grid-only kinematics ----
-    enum { T_P, T_DP, T_E, T_P2, T_CUT, T_2P, T_EXPE, T_IDX, T_IDXL, T_IDXR, T_DXF, T_PER };   // per species
+    enum { T_P, T_DP, T_E, T_P2, T_CUT, T_2P, T_EXPE, T_IDX, T_IDXL, T_IDXR, T_DXF, T_RFF, T_PER };   // per species
     const int nspecies_arrays = T_PER * 2;
     // cp_Ep, cp_kin, cp_inv_betap2, sig_eff, ce_beta2, cp_inv2mpkin, ce_inv_beta2, ce_logp
     const int n_extra = 8;
@@ -177,7 +177,7 @@ int build_tables(Context &ctx)
         double *P2 = arr(s * T_PER + T_P2), *CUT = arr(s * T_PER + T_CUT);
         double *TWO = arr(s * T_PER + T_2P), *EXPE = arr(s * T_PER + T_EXPE);
         double *IDX = arr(s * T_PER + T_IDX), *IDXL = arr(s * T_PER + T_IDXL), *IDXR = arr(s * T_PER + T_IDXR);
-        double *DXF = arr(s * T_PER + T_DXF);
+        double *DXF = arr(s * T_PER + T_DXF), *RFF = arr(s * T_PER + T_RFF);
         for (int j = 0; j < n; j++) {
             P[j] = ctx.h_p[s][j];
             DP[j] = ctx.h_dp[s][j];
@@ -192,6 +192,14 @@ int build_tables(Context &ctx)
             IDXL[j] = (j >= 1) ? 1.0 / (ctx.h_p[s][j] - ctx.h_p[s][j - 1]) : 0.0;
             IDXR[j] = (j <= n - 2) ? 1.0 / (ctx.h_p[s][j + 1] - ctx.h_p[s][j]) : 0.0;
             DXF[j] = (j <= n - 2) ? ctx.h_p[s][j + 1] - ctx.h_p[s][j] : 0.0;
+        }
+        // face j of the filled Dpp form: Dpp_j = kappa * p_j^2 expE_j exp(-1/p_j)
+        // with kappa = dpp_inv * scale shared by the segment, so the face's
+        // dx / (Dpp_j + Dpp_j+1) is this grid factor over kappa
+        for (int j = 0; j < n; j++) {
+            const double gl = P2[j] * EXPE[j] * CUT[j];
+            const double gr = (j <= n - 2) ? P2[j + 1] * EXPE[j + 1] * CUT[j + 1] : 0.0;
+            RFF[j] = (j <= n - 2) ? DXF[j] / (gl + gr) : 0.0;
         }
     }
     double *cpEp = arr(nspecies_arrays + 0), *cpKin = arr(nspecies_arrays + 1);
@@ -246,6 +254,7 @@ int build_tables(Context &ctx)
         st.inv_dxl = darr(s * T_PER + T_IDXL);
         st.inv_dxr = darr(s * T_PER + T_IDXR);
         st.dxf = darr(s * T_PER + T_DXF);
+        st.face_rf = darr(s * T_PER + T_RFF);
         st.pm1 = ctx.h_pm1[s];
         st.pp1 = ctx.h_pp1[s];
         st.pm1_p2 = st.pm1 * st.pm1;
