@@ -113,6 +113,7 @@ __device__ __forceinline__ bool needs_set(const SegInfo &g, int set)
 }
 
 __device__ __forceinline__ int swz(int m) { return (m % kR) * 33 + m / kR; }
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 __device__ __forceinline__ double sup(double v, int d) { return __shfl_up_sync(kFull, v, d); }
 __device__ __forceinline__ double sdn(double v, int d) { return __shfl_down_sync(kFull, v, d); }
 
@@ -622,10 +623,27 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) steps_kernel
     }
     const double *qsrc = (S == 0) ? a.qpi : a.qepri;
     Coef<SRC> F;
+    const int nslot = P.g1 - P.g0;
 #pragma unroll 1
-    for (int gi = 0; gi < P.g1 - P.g0; gi++) {
-        const SegInfo g = segment_of(P, t, P.g0 + gi);
-        if (!g.active) continue;
+    for (int gi = 0; gi < nslot; gi++) {
+        const SegPre *__restrict__ pre = P.pre + (size_t)gi * P.nt + tl;
+        const int flags = pre->flags;
+        if (!(flags & kPreActive)) continue;
+        SegInfo g{};
+        g.windowed = (flags & kPreWindowed) ? 1 : 0;
+        g.sl = pre->sl;
+        g.el = pre->el;
+        g.steps = pre->steps;
+        g.dt = pre->dt;
+        // the next segment's rows (Dpp-on set) and source into L2 while this
+        // segment's sub-steps run: its loads then wait on L2, not on DRAM
+        if (gi + 1 < nslot) {
+            const double *nf = fac_ptr(P, S, gi + 1, 0, tl) + row0;
+            prefetch_l2(nf);
+            prefetch_l2(nf + NB);
+            prefetch_l2(nf + 2 * NB);
+            if (SRC && S == 1 && P.inje) prefetch_l2(P.inje + ((size_t)(gi + 1) * P.nt + tl) * NB + row0);
+        }
         if (S == 0 && P.np_seg) {
             double *o = P.np_seg + ((size_t)gi * P.nt + tl) * NB + row0;
 #pragma unroll
@@ -641,12 +659,12 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) steps_kernel
         // window, on inside it, off after it (all on when not windowed)
         const int sl = g.windowed ? min(max(g.sl, 0), g.steps) : 0;
         const int el = g.windowed ? min(max(g.el, sl), g.steps) : g.steps;
-        const int run_n[3] = {sl, el - sl, g.steps - el};
         int cur = -1;
 #pragma unroll 1
         for (int k = 0; k < 3; k++) {
             const int want = (k == 1) ? 0 : 1;
-            if (run_n[k] <= 0) continue;
+            const int run_n = (k == 0) ? sl : (k == 1 ? el - sl : g.steps - el);
+            if (run_n <= 0) continue;
             if (want >= P.sets) {   // no off set in the workspace: report, leave N as it was
                 if (lane == 0) atomicOr(a.err, kErrBadInput);
                 return;
@@ -656,7 +674,7 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) steps_kernel
                 cur = want;
             }
 #pragma unroll 1
-            for (int istep = 0; istep < run_n[k]; istep++) substep<SRC>(F, N);
+            for (int istep = 0; istep < run_n; istep++) substep<SRC>(F, N);
         }
     }
 #pragma unroll
