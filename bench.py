@@ -342,8 +342,12 @@ def run_gpu_arm(args):
     nspecies = 2
     if args.path == "plain":
         # algorithmic bytes of the sub-step kernels (reference data contract):
-        # a, b, c, source and N read, N written per row per sub-step
-        bytes_per_snapshot = float(np.sum(nsub)) * nspecies * nb * 6 * 8
+        # a, b, c and N read, N written per row per sub-step, plus the source
+        # of a species that has one (electrons: the secondaries; protons: none
+        # in this workload)
+        e_src = 1 if cfg.species == "electron_proton" else 0
+        doubles = (5 + e_src) + 5
+        bytes_per_snapshot = float(np.sum(nsub)) * nb * doubles * 8
         alg_bytes_total = bytes_per_snapshot * args.steps
         per_launch = alg_bytes_total / max(1, evolve_n)
         avg_launch_ms = evolve_ms / max(1, evolve_n)
@@ -354,7 +358,8 @@ def run_gpu_arm(args):
                     "kernel": "plain_steps_kernel", "launches": evolve_n,
                     "kernel_ms_total": evolve_ms, "share_of_step": evolve_ms / ms if ms > 0 else None,
                     "alg_bytes_per_launch": per_launch,
-                    "alg_bytes_rule": "per tracer-snapshot: nsub x 2 species x nb x 6 doubles"}
+                    "alg_bytes_rule": "per tracer-snapshot: nsub x nb x (6 doubles electrons with their "
+                                      "secondary source + 5 protons without a source)"}
     else:
         # The steps kernel runs every sub-step with the spectrum and the factored
         # rows in registers: the bound is the FP64 pipe.  Algorithmic flops are

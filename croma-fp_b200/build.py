@@ -21,7 +21,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 OBJROOT = os.path.join(HERE, "_build")
 NBS = (128, 256, 512)
-SOURCES = ("api.cu", "tables.cu", "schedule.cu", "plain.cu", "fused.cu", "dsa.cu", "serve.cu",
+SOURCES = ("api.cu", "tables.cu", "schedule.cu", "fused.cu", "dsa.cu", "serve.cu",
            "ref_abi.cu", "noalloc.cu")
 NO_FMAD = {"schedule.cu"}
 

@@ -8,7 +8,7 @@ evolve workspace runs the tracers in chunks.  Every tracer starts from the
 seed spectra; backgrounds and shocks are seeded per snapshot.  Device time
 (CUDA events) of DSA + snapshot is reported as tracer-snapshot updates/s.
 
-    python croma-fp_b200/config4_bench.py [--tracers 4194304] [--steps 2] [--warmup 1]
+    python croma-fp_b200/config4_bench.py [--tracers 4194304] [--steps 2] [--warmup 1] [--path fused|plain]
 """
 from __future__ import annotations
 
@@ -34,13 +34,13 @@ def _package():
     return sys.modules["croma_fp_b200"]
 
 
-def run(ntracer=4194304, steps=2, warmup=1, seed=4242, dsa_fraction=0.05):
+def run(ntracer=4194304, steps=2, warmup=1, seed=4242, dsa_fraction=0.05, path="fused"):
     _package()
     import torch
     from croma_fp_b200 import config, native, synth
     cfg = config.config4()
     w = synth.Workload(cfg, ntracer, 100, seed=seed)
-    fp = native.TracerFP(cfg, path="fused")
+    fp = native.TracerFP(cfg, path=path)
     gp, ge = fp.grid(0), fp.grid(1)
     crp1, cre1 = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), 1, cfg.species)
     fp.set_state_broadcast(ntracer, crp1[0], cre1[0], 1.0e7)
@@ -72,7 +72,7 @@ def run(ntracer=4194304, steps=2, warmup=1, seed=4242, dsa_fraction=0.05):
     ms = float(np.mean(times))
     return {"metric": "tracer-snapshot updates/s (DSA + snapshot, device time)",
             "value": ntracer / (ms / 1e3), "ms_per_snapshot": ms, "dsa_ms_per_snapshot": float(np.mean(dsa_ms)),
-            "tracers": ntracer, "bins_per_species": 512, "steps": steps, "warmup": warmup,
+            "tracers": ntracer, "bins_per_species": 512, "steps": steps, "warmup": warmup, "path": path,
             "dsa_injected_per_snapshot": float(np.mean(injected)),
             "nsub": {"min": int(sched["nsub"].min()), "mean": float(sched["nsub"].mean()),
                      "max": int(sched["nsub"].max())},
@@ -85,9 +85,10 @@ def main():
     ap.add_argument("--tracers", type=int, default=4194304)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--path", default="fused", choices=["fused", "plain"])
     args = ap.parse_args()
     t0 = time.time()
-    res = run(args.tracers, args.steps, args.warmup)
+    res = run(args.tracers, args.steps, args.warmup, path=args.path)
     res["wall_s"] = time.time() - t0
     print(json.dumps(res), flush=True)
 

@@ -57,11 +57,11 @@ namespace {
 void free_state(Context &c)
 {
     cudaFree(c.d_crp); cudaFree(c.d_cre); cudaFree(c.d_qpi); cudaFree(c.d_qepri);
-    cudaFree(c.d_mass); cudaFree(c.d_dis); cudaFree(c.d_bg); cudaFree(c.d_layout_tmp);
-    c.d_crp = c.d_cre = c.d_qpi = c.d_qepri = c.d_mass = c.d_bg = c.d_layout_tmp = nullptr;
+    cudaFree(c.d_mass); cudaFree(c.d_dis); cudaFree(c.d_bg);
+    c.d_crp = c.d_cre = c.d_qpi = c.d_qepri = c.d_mass = c.d_bg = nullptr;
     c.d_dis = nullptr;
-    cudaFree(c.d_coef); cudaFree(c.d_inje); cudaFree(c.d_seg_ngas); cudaFree(c.d_eta_scale);
-    c.d_coef = c.d_inje = c.d_seg_ngas = c.d_eta_scale = nullptr;
+    cudaFree(c.d_inje); cudaFree(c.d_eta_scale);
+    c.d_inje = c.d_eta_scale = nullptr;
     cudaFree(c.d_fac); cudaFree(c.d_np_seg); cudaFree(c.d_segpre);
     c.d_fac = c.d_np_seg = nullptr;
     c.d_segpre = nullptr;
@@ -225,7 +225,6 @@ int croma_b200_reserve(CromaB200Context *h, int ntracer)
     CROMA_CUDA(cudaMalloc(&c.d_mass, n * sizeof(double)));
     CROMA_CUDA(cudaMalloc(&c.d_dis, n));
     CROMA_CUDA(cudaMalloc(&c.d_bg, 2 * (size_t)kNbg * n * sizeof(double)));
-    if (!cell_major(c)) CROMA_CUDA(cudaMalloc(&c.d_layout_tmp, st));   // host <-> momentum-major staging
     CROMA_CUDA(cudaMemsetAsync(c.d_crp, 0, st, c.stream));
     CROMA_CUDA(cudaMemsetAsync(c.d_cre, 0, st, c.stream));
     CROMA_CUDA(cudaMemsetAsync(c.d_qpi, 0, st, c.stream));
@@ -236,7 +235,7 @@ int croma_b200_reserve(CromaB200Context *h, int ntracer)
     c.ntracer = ntracer;
     c.has_sources = 0;
     int rc = schedule_reserve(c, ntracer);
-    if (rc == 0) rc = cell_major(c) ? fused_reserve(c, ntracer) : plain_reserve(c, ntracer);
+    if (rc == 0) rc = fused_reserve(c, ntracer);
     if (rc != 0) { free_state(c); return rc; }
     return 0;
 }
@@ -255,11 +254,8 @@ int croma_b200_set_state(CromaB200Context *h, int ntracer, const double *crp, co
     const size_t st = (size_t)NB * ntracer * sizeof(double);
     int rc = 0;
     auto up = [&](const double *h, double *d) -> int {
-        if (cell_major(c)) {
-            CROMA_CUDA(cudaMemcpyAsync(d, h, st, cudaMemcpyHostToDevice, c.stream));
-            return 0;
-        }
-        return transpose_to_device(c, h, d, ntracer);
+        CROMA_CUDA(cudaMemcpyAsync(d, h, st, cudaMemcpyHostToDevice, c.stream));
+        return 0;
     };
     if (crp && (rc = up(crp, c.d_crp))) return rc;
     if (cre && (rc = up(cre, c.d_cre))) return rc;
@@ -289,7 +285,7 @@ int croma_b200_set_state_broadcast(CromaB200Context *h, int ntracer, const doubl
     CROMA_CUDA(cudaMalloc(&d_rows, 2 * NB * sizeof(double)));
     cudaError_t e = cudaMemcpy(d_rows, crp_row, NB * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_rows + NB, cre_row, NB * sizeof(double), cudaMemcpyHostToDevice);
-    const size_t ts = cell_major(c) ? (size_t)NB : 1, js = cell_major(c) ? 1 : (size_t)ntracer;
+    const size_t ts = (size_t)NB, js = 1;   // cell-major [tracer][nb]
     const size_t total = (size_t)ntracer * NB;
     const unsigned blocks = (unsigned)((total + 255) / 256);
     if (e == cudaSuccess) {
@@ -320,11 +316,8 @@ int croma_b200_get_state(CromaB200Context *h, double *crp, double *cre)
     int rc = 0;
     const size_t st = (size_t)NB * c.cap * sizeof(double);
     auto down = [&](const double *d, double *h) -> int {
-        if (cell_major(c)) {
-            CROMA_CUDA(cudaMemcpyAsync(h, d, st, cudaMemcpyDeviceToHost, c.stream));
-            return 0;
-        }
-        return transpose_to_host(c, d, h, c.cap);
+        CROMA_CUDA(cudaMemcpyAsync(h, d, st, cudaMemcpyDeviceToHost, c.stream));
+        return 0;
     };
     if (crp && (rc = down(c.d_crp, crp))) return rc;
     CROMA_CUDA(cudaStreamSynchronize(c.stream));
@@ -341,11 +334,8 @@ int croma_b200_get_sources(CromaB200Context *h, double *qpi, double *qepri, unsi
     int rc = 0;
     const size_t st = (size_t)NB * c.cap * sizeof(double);
     auto down = [&](const double *d, double *h) -> int {
-        if (cell_major(c)) {
-            CROMA_CUDA(cudaMemcpyAsync(h, d, st, cudaMemcpyDeviceToHost, c.stream));
-            return 0;
-        }
-        return transpose_to_host(c, d, h, c.cap);
+        CROMA_CUDA(cudaMemcpyAsync(h, d, st, cudaMemcpyDeviceToHost, c.stream));
+        return 0;
     };
     if (qpi && (rc = down(c.d_qpi, qpi))) return rc;
     CROMA_CUDA(cudaStreamSynchronize(c.stream));
@@ -405,7 +395,7 @@ int snapshot_impl(Context &c, const CromaB200Snapshot *s, int sync)
     a.err = c.d_err;
     int rc = run_schedule(c, a);
     if (rc) return rc;
-    rc = (c.cfg.path == CROMA_PATH_PLAIN) ? run_plain(c, a) : run_fused(c, a);
+    rc = run_fused(c, a);   // both paths; the plain one runs its per-step kernels
     if (rc) return rc;
     if (sync) return check_err(c);
     return 0;
@@ -441,13 +431,6 @@ int croma_b200_snapshot_host(CromaB200Context *h, const CromaB200Snapshot *s, in
     }
     Context &c = h->impl;
     CROMA_CUDA(cudaSetDevice(c.device));
-    if (!cell_major(c)) {
-        // momentum-major resident spectra go through the transposes: no overlap
-        int rc = croma_b200_set_state(h, ntracer, crp, cre, nullptr, nullptr, mass, nullptr);
-        if (!rc) rc = snapshot_impl(c, s, 1);
-        if (!rc) rc = croma_b200_get_state(h, crp, cre);
-        return rc;
-    }
     if (ntracer != c.cap) {
         const int rc = croma_b200_reserve(h, ntracer);
         if (rc) return rc;

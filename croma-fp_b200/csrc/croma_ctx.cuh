@@ -102,7 +102,7 @@ struct Context {
     cudaEvent_t ic_stage_ev[2] = {nullptr, nullptr};
     int ic_stage_next = 0;
 
-    // resident state (momentum-major [nb][cap])
+    // resident state (cell-major [cap][nb])
     int cap = 0, ntracer = 0;
     double *d_crp = nullptr, *d_cre = nullptr;
     double *d_qpi = nullptr, *d_qepri = nullptr;
@@ -120,10 +120,7 @@ struct Context {
     unsigned long long *d_keys = nullptr, *d_keys_alt = nullptr;
     int *d_vals = nullptr, *d_vals_alt = nullptr, *d_seg_aux = nullptr;
 
-    // plain-path workspace
-    double *d_coef = nullptr;         // [2 sets][2 species][3][nb][cap]
-    double *d_inje = nullptr;         // [nb][cap]
-    double *d_seg_ngas = nullptr;     // [cap]
+    double *d_inje = nullptr;         // electron source per segment (fused workspace)
     double *d_eta_scale = nullptr;    // [cap] Dpp eta-cap scale of the current slot
 
     // fused-path workspace, per tracer chunk: factored matrices of every
@@ -142,7 +139,6 @@ struct Context {
     unsigned *d_dsa_count = nullptr;
     double *d_dsa_stage = nullptr;    // [10][dsa_stage_cap] host shock fields
     int dsa_stage_cap = 0;
-    double *d_layout_tmp = nullptr;   // [nb][cap] transpose staging
 
     // host-buffer snapshot (croma_b200_snapshot_host): copy streams and
     // per-chunk events, created on first use; pipe is set for one call
@@ -186,23 +182,16 @@ int ic_rows(Context &ctx, double z, double *d_out);
 // schedule.cu
 int schedule_reserve(Context &ctx, int cap);
 int run_schedule(Context &ctx, const SnapArgs &a);
-// plain.cu
-int plain_reserve(Context &ctx, int cap);
-int run_plain(Context &ctx, const SnapArgs &a);
-// fused.cu
+// fused.cu: both paths (the plain one as per-step kernels, one slot at a time)
 int fused_reserve(Context &ctx, int cap);
 // device bytes fused_reserve allocates for cap tracers under a workspace cap
-double fused_workspace_bytes(const ModelParams &mp, int cap, double workspace_cap);
+// on path CROMA_PATH_*
+double fused_workspace_bytes(const ModelParams &mp, int cap, double workspace_cap, int path);
 int run_fused(Context &ctx, const SnapArgs &a);
 // dsa.cu
 int set_dsa(Context &ctx, const CromaB200DsaParams *prm);
 int dsa_inject(Context &ctx, const CromaB200Shocks *sh, double density_unit, double dt_gyr, int mode,
                int reacc_mode, int *ninjected);
 void free_dsa(Context &ctx);
-// layout of the resident spectra: cell-major [tracer][nb] for the fused path,
-// momentum-major [nb][tracer] for the plain path
-inline bool cell_major(const Context &ctx) { return ctx.cfg.path == CROMA_PATH_FUSED; }
-int transpose_to_device(Context &ctx, const double *h_cell_major, double *d_mom_major, int n);
-int transpose_to_host(Context &ctx, const double *d_mom_major, double *h_cell_major, int n);
 
 }  // namespace croma

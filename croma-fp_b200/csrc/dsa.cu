@@ -545,8 +545,8 @@ int dsa_inject(Context &c, const CromaB200Shocks *sh, double density_unit, doubl
     A.cre = c.d_cre;
     A.qpi = c.d_qpi;
     A.qepri = c.d_qepri;
-    if (cell_major(c)) { A.ts = NB; A.js = 1; }
-    else { A.ts = 1; A.js = (size_t)c.cap; }
+    A.ts = NB;   // cell-major [tracer][nb]
+    A.js = 1;
     A.dis = c.d_dis;
     A.mass = c.d_mass;
     for (int s = 0; s < 2; s++) { A.p[s] = c.gt.s[s].p; A.dp[s] = c.gt.s[s].dp; }

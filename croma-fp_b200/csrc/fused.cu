@@ -254,10 +254,11 @@ struct WarpSmem {
 };
 
 
-// Terms, faces, rows and the factorisation of one system, stored to out.
+// Terms, faces and the rows a, b, c of one system: lane l holds rows
+// [l*R, (l+1)*R) in A, Bd, Cc.
 template <int S>
-__device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int lane, WarpSmem &sm,
-                                 double *out)
+__device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane, WarpSmem &sm,
+                               double A[kR], double Bd[kR], double Cc[kR])
 {
     const SpeciesTables &st = T.gt->s[S];
     const double *x = st.p;
@@ -300,7 +301,6 @@ __device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int la
 
     // rows a, b, c of this lane (cc_build_{left,interior,right}, Chang_Cooper.c:66-184)
     const int row0 = lane * kR;
-    double A[kR], Bd[kR], Cc[kR];
 #pragma unroll
     for (int r = 0; r < kR; r++) {
         const int m = row0 + r;
@@ -354,8 +354,20 @@ __device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int la
         Cc[r] = cv;
     }
     __syncwarp();
+    return err;
+}
 
-    // ---- pivots: composed Moebius maps d -> b - a c_prev / d ----
+// Thomas pivots of the rows a, b, c held as build_rows leaves them, in place:
+// Bd <- 1/d, A <- a/d, Cc <- c/d (0 on the last row), with
+// d_i = b_i + a_i c'_{i-1}, c'_i = -c_i / d_i (fp_thomas_solve_ws,
+// src/fp_shared_core.c:226-257).  The chain of Moebius maps d -> b - e/d is
+// composed per lane as 2x2 matrices and combined by a warp scan, after which
+// each lane re-runs the exact recurrence on its rows from the scanned
+// incoming pivot.
+__device__ __forceinline__ unsigned pivot_rows(double A[kR], double Bd[kR], double Cc[kR], int lane)
+{
+    unsigned err = 0;
+    const int row0 = lane * kR;
     const double c_in = sup(Cc[kR - 1], 1);   // c of the row before this lane's first
     double t00 = 1.0, t01 = 0.0, t10 = 0.0, t11 = 1.0;
 #pragma unroll
@@ -396,23 +408,47 @@ __device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int la
         Cc[r] = (m == NB - 1) ? 0.0 : cr * inv;
         cp_prev = -cr * inv;
     }
-    // inv, h = a / d, q = c / d of this lane's rows: 64 contiguous bytes per
-    // array per lane, 2 KB per array per warp
+    (void)vp;
+    return err;
+}
+
+// Three row arrays of a lane to out[0..3nb): 64 contiguous bytes per array
+// per lane, 2 KB per array per warp.
+__device__ __forceinline__ void store_rows(double *out, int lane, const double X[kR], const double Y[kR],
+                                           const double Z[kR])
+{
+    const int row0 = lane * kR;
 #pragma unroll
     for (int r = 0; r < kR; r += 2) {
-        __stcg(reinterpret_cast<double2 *>(out + row0 + r), make_double2(Bd[r], Bd[r + 1]));
-        __stcg(reinterpret_cast<double2 *>(out + NB + row0 + r), make_double2(A[r], A[r + 1]));
-        __stcg(reinterpret_cast<double2 *>(out + 2 * NB + row0 + r), make_double2(Cc[r], Cc[r + 1]));
+        __stcg(reinterpret_cast<double2 *>(out + row0 + r), make_double2(X[r], X[r + 1]));
+        __stcg(reinterpret_cast<double2 *>(out + NB + row0 + r), make_double2(Y[r], Y[r + 1]));
+        __stcg(reinterpret_cast<double2 *>(out + 2 * NB + row0 + r), make_double2(Z[r], Z[r + 1]));
     }
-    (void)vp;
+}
+
+// One system of species S to out: factored (1/d, a/d, c/d) for the steps
+// kernel, or the raw rows (a, b, c) for the per-step path, which factors
+// them again on every sub-step.
+template <int S, bool ROWS>
+__device__ unsigned factor_store(const SegTerms<S> &T, const double *tab, int lane, WarpSmem &sm,
+                                 double *out)
+{
+    double A[kR], Bd[kR], Cc[kR];
+    unsigned err = build_rows<S>(T, tab, lane, sm, A, Bd, Cc);
+    if (ROWS) {
+        store_rows(out, lane, A, Bd, Cc);
+        return err;
+    }
+    err |= pivot_rows(A, Bd, Cc, lane);
+    store_rows(out, lane, Bd, A, Cc);
     return err;
 }
 
 
 // Factor kernel, persistent: each block stages the species' grid tables in
 // shared memory once, then each warp takes tracers strided by the grid and
-// factors every segment (and on/off set) of each.
-template <int S>
+// factors every segment (and on/off set) of each (ROWS: stores the raw rows).
+template <int S, bool ROWS>
 __global__ void __launch_bounds__(kFacWarps * 32, (NB <= 256 ? 2 : 1)) factor_kernel(FusedParams P)
 {
     extern __shared__ double4 smem_raw[];
@@ -479,7 +515,7 @@ __global__ void __launch_bounds__(kFacWarps * 32, (NB <= 256 ? 2 : 1)) factor_ke
                     T.dpp_inv = pre->dpp_inv;
                     T.dpp_scale = eta;
                 }
-                const unsigned err = factor_store<S>(T, tab, lane, ws, fac_ptr(P, S, gi, set, tl));
+                const unsigned err = factor_store<S, ROWS>(T, tab, lane, ws, fac_ptr(P, S, gi, set, tl));
                 if (err && lane == 0) atomicOr(a.err, err);
                 __syncwarp();
             }
@@ -503,20 +539,27 @@ struct Coef {
     double hlo, hhi, qlo, qhi;
 };
 
-template <bool SRC>
-__device__ __forceinline__ void load_coef(Coef<SRC> &F, const double *fac, const double *src, double dt,
-                                          int lane)
+// The lane's rows of three arrays at in[0..3nb) (64 contiguous bytes each).
+__device__ __forceinline__ void load_rows(const double *in, int lane, double X[kR], double Y[kR], double Z[kR])
 {
     const int row0 = lane * kR;
 #pragma unroll
     for (int r = 0; r < kR; r += 2) {
-        const double2 vi = __ldcg(reinterpret_cast<const double2 *>(fac + row0 + r));
-        const double2 vh = __ldcg(reinterpret_cast<const double2 *>(fac + NB + row0 + r));
-        const double2 vq = __ldcg(reinterpret_cast<const double2 *>(fac + 2 * NB + row0 + r));
-        F.inv[r] = vi.x; F.inv[r + 1] = vi.y;
-        F.h[r] = vh.x; F.h[r + 1] = vh.y;
-        F.q[r] = vq.x; F.q[r + 1] = vq.y;
+        const double2 vx = __ldcg(reinterpret_cast<const double2 *>(in + row0 + r));
+        const double2 vy = __ldcg(reinterpret_cast<const double2 *>(in + NB + row0 + r));
+        const double2 vz = __ldcg(reinterpret_cast<const double2 *>(in + 2 * NB + row0 + r));
+        X[r] = vx.x; X[r + 1] = vx.y;
+        Y[r] = vy.x; Y[r + 1] = vy.y;
+        Z[r] = vz.x; Z[r + 1] = vz.y;
     }
+}
+
+// The rest of Coef once inv, h, q hold the lane's factored rows: the source
+// term and the scan multipliers.
+template <bool SRC>
+__device__ __forceinline__ void finish_coef(Coef<SRC> &F, const double *src, double dt, int lane)
+{
+    const int row0 = lane * kR;
     if (lane == 0) F.h[0] = 0.0;
     if (lane == 31) F.q[kR - 1] = 0.0;
     if (SRC) {
@@ -545,6 +588,14 @@ __device__ __forceinline__ void load_coef(Coef<SRC> &F, const double *fac, const
         if (lane >= off) H *= Hu;
         if (lane + off < 32) Q *= Qd;
     }
+}
+
+template <bool SRC>
+__device__ __forceinline__ void load_coef(Coef<SRC> &F, const double *fac, const double *src, double dt,
+                                          int lane)
+{
+    load_rows(fac, lane, F.inv, F.h, F.q);
+    finish_coef<SRC>(F, src, dt, lane);
 }
 
 // One implicit sub-step: N <- M^{-1} (N + dt src) with the factored M.
@@ -680,6 +731,61 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) steps_kernel
 #pragma unroll
     for (int r = 0; r < kR; r += 2)
         *reinterpret_cast<double2 *>(Nrow + r) = make_double2(N[r], N[r + 1]);
+}
+
+// Per-step kernel (the plain path): warp w of block b advances tracer
+// t0 + b * kWarps + w through the sub-steps of segment slot g0 with the
+// reference's per-step data contract -- every sub-step reads the rows a, b, c
+// of its on/off set, the source and N from memory, solves M N' = N + dt src
+// with the pivots recomputed (tracer_fp_cpu_evolve, src/tracer_fp_cpu.c:149-190;
+// fp_thomas_solve_ws, src/fp_shared_core.c:226-257) and writes N back.
+template <int S, bool SRC>
+__global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 5 : 2)) plain_steps_kernel(FusedParams P)
+{
+    const int w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int tl = blockIdx.x * kWarps + w;
+    if (tl >= P.nt) return;
+    const int t = P.t0 + tl;
+    const SnapArgs &a = P.a;
+    const SegPre *__restrict__ pre = P.pre + tl;
+    const int flags = pre->flags;
+    if (!(flags & kPreActive)) return;
+    const int windowed = (flags & kPreWindowed) ? 1 : 0;
+    const int sl = pre->sl, el = pre->el, steps = pre->steps;
+    const double dt = pre->dt;
+    const int row0 = lane * kR;
+    double *Nrow = (S == 0 ? a.crp : a.cre) + (size_t)t * NB + row0;
+    const double *src = nullptr;
+    if (SRC) src = (S == 1 && P.inje) ? P.inje + (size_t)tl * NB : ((S == 0) ? a.qpi : a.qepri) + (size_t)t * NB;
+    Coef<SRC> F;
+    double N[kR];
+#pragma unroll 1
+    for (int istep = 0; istep < steps; istep++) {
+        const int set = (!windowed || (istep >= sl && istep < el)) ? 0 : 1;
+        if (set >= P.sets) {   // no off set in the workspace: report, leave N as it is
+            if (lane == 0) atomicOr(a.err, kErrBadInput);
+            return;
+        }
+        // rows a, b, c of the set: A <- a, inv <- b, q <- c, then the pivots
+        load_rows(fac_ptr(P, S, 0, set, tl), lane, F.h, F.inv, F.q);
+#pragma unroll
+        for (int r = 0; r < kR; r += 2) {
+            const double2 v = *reinterpret_cast<const double2 *>(Nrow + r);
+            N[r] = v.x;
+            N[r + 1] = v.y;
+        }
+        const unsigned err = pivot_rows(F.h, F.inv, F.q, lane);
+        if (__any_sync(kFull, err != 0)) {
+            if (lane == 0) atomicOr(a.err, kErrSingular);
+            return;
+        }
+        finish_coef<SRC>(F, src, dt, lane);
+        substep<SRC>(F, N);
+#pragma unroll
+        for (int r = 0; r < kR; r += 2)
+            *reinterpret_cast<double2 *>(Nrow + r) = make_double2(N[r], N[r + 1]);
+    }
 }
 
 // The per-segment scalars of every (slot, tracer) of the chunk, one thread
@@ -900,7 +1006,7 @@ cudaError_t launch_secondary(Context &ctx, const FusedParams &P)
     return cudaGetLastError();
 }
 
-template <int S>
+template <int S, bool ROWS>
 cudaError_t launch_factor(Context &ctx, const FusedParams &P)
 {
     constexpr size_t smem = (size_t)kTab * kTabStride * sizeof(double) + kFacWarps * sizeof(WarpSmem);
@@ -908,10 +1014,11 @@ cudaError_t launch_factor(Context &ctx, const FusedParams &P)
     struct Occupancy { cudaError_t e; int resident; };
     static const Occupancy occ = [] {
         Occupancy o{cudaSuccess, 0};
-        o.e = cudaFuncSetAttribute(factor_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        o.e = cudaFuncSetAttribute(factor_kernel<S, ROWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem);
         if (o.e == cudaSuccess)
-            o.e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.resident, factor_kernel<S>, kFacWarps * 32,
-                                                                smem);
+            o.e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o.resident, factor_kernel<S, ROWS>,
+                                                                kFacWarps * 32, smem);
         return o;
     }();
     if (occ.e != cudaSuccess) return occ.e;
@@ -924,16 +1031,21 @@ cudaError_t launch_factor(Context &ctx, const FusedParams &P)
     const long long full = (long long)nsm * resident;
     if (blocks > full) blocks = full;
     if (blocks < 1) return cudaSuccess;
-    factor_kernel<S><<<(unsigned)blocks, kFacWarps * 32, smem, ctx.stream>>>(P);
+    factor_kernel<S, ROWS><<<(unsigned)blocks, kFacWarps * 32, smem, ctx.stream>>>(P);
     return cudaGetLastError();
 }
 
 template <int S>
-cudaError_t launch_steps(Context &ctx, const FusedParams &P, bool src)
+cudaError_t launch_steps(Context &ctx, const FusedParams &P, bool src, bool perstep)
 {
     const int blocks = (P.nt + kWarps - 1) / kWarps;
-    if (src) steps_kernel<S, true><<<blocks, kWarps * 32, 0, ctx.stream>>>(P);
-    else steps_kernel<S, false><<<blocks, kWarps * 32, 0, ctx.stream>>>(P);
+    if (perstep) {
+        if (src) plain_steps_kernel<S, true><<<blocks, kWarps * 32, 0, ctx.stream>>>(P);
+        else plain_steps_kernel<S, false><<<blocks, kWarps * 32, 0, ctx.stream>>>(P);
+    } else {
+        if (src) steps_kernel<S, true><<<blocks, kWarps * 32, 0, ctx.stream>>>(P);
+        else steps_kernel<S, false><<<blocks, kWarps * 32, 0, ctx.stream>>>(P);
+    }
     return cudaGetLastError();
 }
 
@@ -957,10 +1069,13 @@ struct WorkspaceShape {
     double per_tracer;
 };
 
-WorkspaceShape workspace_shape(const ModelParams &mp, int cap, double workspace_cap)
+// The per-step path holds one segment slot at a time; the on-chip path all
+// of a snapshot's slots.
+WorkspaceShape workspace_shape(const ModelParams &mp, int cap, double workspace_cap, bool perstep)
 {
     WorkspaceShape w;
-    w.nseg = mp.interp_max_segments < 1 ? 1 : (mp.interp_max_segments > 64 ? 64 : mp.interp_max_segments);
+    w.nseg = perstep ? 1
+                     : (mp.interp_max_segments < 1 ? 1 : (mp.interp_max_segments > 64 ? 64 : mp.interp_max_segments));
     w.sets = mp.window_centred ? 2 : 1;
     w.per_tracer = 8.0 * NB * ((double)2 * w.nseg * w.sets * 3 + 2.0 * w.nseg) + (double)w.nseg * sizeof(SegPre);
     const double budget = workspace_cap > 0.0 ? workspace_cap : workspace_budget_bytes();
@@ -972,15 +1087,15 @@ WorkspaceShape workspace_shape(const ModelParams &mp, int cap, double workspace_
 
 }  // namespace
 
-double fused_workspace_bytes(const ModelParams &mp, int cap, double workspace_cap)
+double fused_workspace_bytes(const ModelParams &mp, int cap, double workspace_cap, int path)
 {
-    const WorkspaceShape w = workspace_shape(mp, cap, workspace_cap);
+    const WorkspaceShape w = workspace_shape(mp, cap, workspace_cap, path == CROMA_PATH_PLAIN);
     return (double)w.chunk * w.per_tracer + 8.0 * cap;
 }
 
 int fused_reserve(Context &ctx, int cap)
 {
-    const WorkspaceShape w = workspace_shape(ctx.mp, cap, ctx.workspace_bytes);
+    const WorkspaceShape w = workspace_shape(ctx.mp, cap, ctx.workspace_bytes, ctx.cfg.path == CROMA_PATH_PLAIN);
     const int nseg = w.nseg, sets = w.sets;
     const long long chunk = w.chunk;
     cudaFree(ctx.d_inje);
@@ -1005,22 +1120,26 @@ int fused_reserve(Context &ctx, int cap)
 
 // Segments [g0, g1) of one tracer chunk: the eta-cap scales (if the cap is
 // on), the factored matrices of both species, the proton steps, the
-// secondary source, the electron steps.
-static int fused_range(Context &ctx, FusedParams &P, int g0, int g1)
+// secondary source, the electron steps.  perstep (the plain path, one slot):
+// the raw rows of both species, the secondary source from the protons at the
+// slot start, then the per-step kernels.
+static int fused_range(Context &ctx, FusedParams &P, int g0, int g1, bool perstep)
 {
     const SnapArgs &a = P.a;
     const int protons = ctx.mp.species_mask & CROMA_SPECIES_PROTON;
     const int electrons = ctx.mp.species_mask & CROMA_SPECIES_ELECTRON;
     const bool secondaries = protons && electrons;
     const bool cap = ctx.mp.eta_dpp_cap > 0.0 && isfinite(ctx.mp.eta_dpp_cap) && ctx.mp.dpp_model != kDppOff;
-    if (cap && g1 != g0 + 1) {
-        set_error("internal: the eta cap needs one segment per launch");
+    if ((cap || perstep) && g1 != g0 + 1) {
+        set_error("internal: the eta cap and the per-step path need one segment per launch");
         return -1;
     }
     P.g0 = g0;
     P.g1 = g1;
     P.eta_scale = nullptr;
-    P.np_seg = secondaries ? ctx.d_np_seg : nullptr;
+    // protons at the segment start: recorded by the steps kernel, or (per
+    // step, one slot) the chunk's resident rows themselves
+    P.np_seg = !secondaries ? nullptr : (perstep ? a.crp + (size_t)P.t0 * NB : ctx.d_np_seg);
     P.inje = secondaries ? ctx.d_inje : nullptr;
     cudaEvent_t ev = nullptr;
     timed_begin(ctx, kKindCoeff, &ev);
@@ -1040,21 +1159,27 @@ static int fused_range(Context &ctx, FusedParams &P, int g0, int g1)
         ctx.last_launches += 1;
     }
     if (protons) {
-        CROMA_CUDA(launch_factor<0>(ctx, P));
+        CROMA_CUDA((perstep ? launch_factor<0, true>(ctx, P) : launch_factor<0, false>(ctx, P)));
         ctx.last_launches += 1;
     }
     if (electrons) {
-        CROMA_CUDA(launch_factor<1>(ctx, P));
+        CROMA_CUDA((perstep ? launch_factor<1, true>(ctx, P) : launch_factor<1, false>(ctx, P)));
         ctx.last_launches += 1;
     }
     timed_end(ctx, kKindCoeff, ev);
+    if (secondaries && perstep) {
+        timed_begin(ctx, kKindSecondary, &ev);
+        CROMA_CUDA(launch_secondary(ctx, P));
+        timed_end(ctx, kKindSecondary, ev);
+        ctx.last_launches += 1;
+    }
     if (protons) {
         timed_begin(ctx, kKindEvolve, &ev);
-        CROMA_CUDA(launch_steps<0>(ctx, P, a.qpi != nullptr));
+        CROMA_CUDA(launch_steps<0>(ctx, P, a.qpi != nullptr, perstep));
         timed_end(ctx, kKindEvolve, ev);
         ctx.last_launches += 1;
     }
-    if (secondaries) {
+    if (secondaries && !perstep) {
         timed_begin(ctx, kKindSecondary, &ev);
         CROMA_CUDA(launch_secondary(ctx, P));
         timed_end(ctx, kKindSecondary, ev);
@@ -1062,7 +1187,7 @@ static int fused_range(Context &ctx, FusedParams &P, int g0, int g1)
     }
     if (electrons) {
         timed_begin(ctx, kKindEvolve, &ev);
-        CROMA_CUDA(launch_steps<1>(ctx, P, secondaries || a.qepri != nullptr));
+        CROMA_CUDA(launch_steps<1>(ctx, P, secondaries || a.qepri != nullptr, perstep));
         timed_end(ctx, kKindEvolve, ev);
         ctx.last_launches += 1;
     }
@@ -1071,13 +1196,13 @@ static int fused_range(Context &ctx, FusedParams &P, int g0, int g1)
 }
 
 // Every segment slot of every tracer chunk.
-static int fused_chunks(Context &ctx, FusedParams &P, int nslots)
+static int fused_chunks(Context &ctx, FusedParams &P, int nslots, bool perstep)
 {
     if (ctx.fused_chunk <= 0 || !ctx.d_fac) {
         set_error("fused workspace not reserved");
         return -1;
     }
-    if (nslots > ctx.fused_nseg) {
+    if ((perstep ? 1 : nslots) > ctx.fused_nseg) {
         set_error("internal: more segment slots than the fused workspace holds");
         return -1;
     }
@@ -1106,12 +1231,12 @@ static int fused_chunks(Context &ctx, FusedParams &P, int nslots)
             return -1;
         }
         if (pipe) CROMA_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.pipe_up[k], 0));
-        if (!cap) {
-            const int rc = fused_range(ctx, P, 0, nslots);
+        if (!cap && !perstep) {
+            const int rc = fused_range(ctx, P, 0, nslots, false);
             if (rc) return rc;
         } else {
             for (int g = 0; g < nslots; g++) {
-                const int rc = fused_range(ctx, P, g, g + 1);
+                const int rc = fused_range(ctx, P, g, g + 1, perstep);
                 if (rc) return rc;
             }
         }
@@ -1142,7 +1267,7 @@ int run_fused(Context &ctx, const SnapArgs &a)
     P.ic_stride = 0;
     const int nslots = ctx.mp.interp_max_segments < 1 ? 1
                      : (ctx.mp.interp_max_segments > 64 ? 64 : ctx.mp.interp_max_segments);
-    return fused_chunks(ctx, P, nslots);
+    return fused_chunks(ctx, P, nslots, ctx.cfg.path == CROMA_PATH_PLAIN);
 }
 
 int run_fused_segment(Context &ctx, const SnapArgs &a, const SegInfo &ex, int ic_stride)
@@ -1155,7 +1280,7 @@ int run_fused_segment(Context &ctx, const SnapArgs &a, const SegInfo &ex, int ic
     P.explicit_seg = 1;
     P.ex = ex;
     P.ic_stride = ic_stride;
-    return fused_chunks(ctx, P, 1);
+    return fused_chunks(ctx, P, 1, false);
 }
 
 }  // namespace croma

@@ -64,15 +64,12 @@ constexpr double kDefaultWorkspace = 4.0e9;
 double request_bytes(const CromaB200Server &s, int n)
 {
     const double nn = (double)n;
-    // spectra and sources (4 x nb doubles; plain adds a layout staging row),
-    // mass, flags, background staging (2 x 8 doubles), schedule, bucket keys
-    // and values
-    const double rows = (s.cfg.base.path == CROMA_PATH_FUSED) ? 4.0 : 5.0;
-    double b = nn * (rows * NB * 8 + 8 + 1 + 2 * 8 * 8 + 6 * 4 + 1 + 3 * 8 + 8 * 4);
+    // spectra and sources (4 x nb doubles), mass, flags, background staging
+    // (2 x 8 doubles), schedule, bucket keys and values
+    double b = nn * (4.0 * NB * 8 + 8 + 1 + 2 * 8 * 8 + 6 * 4 + 1 + 3 * 8 + 8 * 4);
     const double ws = s.cfg.workspace_bytes_per_request > 0.0 ? s.cfg.workspace_bytes_per_request
                                                               : kDefaultWorkspace;
-    if (s.cfg.base.path == CROMA_PATH_FUSED) b += fused_workspace_bytes(s.mp, n, ws);
-    else b += nn * (2.0 * 2 * 3 * NB * 8 + NB * 8 + 8);
+    b += fused_workspace_bytes(s.mp, n, ws, s.cfg.base.path);
     // grid tables, secondary weights, IC rows, sort scratch, context slack
     b += (double)NB * NB * 8 + 40.0 * NB * 8 + 2.0 * (NB + 2 + 2049) * 8 + 16.0 * nn + 64.0e6;
     return b;

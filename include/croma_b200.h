@@ -39,7 +39,8 @@ enum { CROMA_DPP_ASA = 1, CROMA_DPP_TTD = 2, CROMA_DPP_OFF = 3, CROMA_DPP_DIRECT
 /* Which evolve kernel family runs. */
 enum {
     CROMA_PATH_PLAIN = 0,   /* FP64, reference data contract: CC rows materialised per
-                               segment, one Thomas system per thread per sub-step */
+                               segment, every sub-step reads them, the source and N
+                               from memory, re-pivots and writes N (per-step) */
     CROMA_PATH_FUSED = 1    /* FP64, on-chip: rows built, factored and swept per tracer
                                inside one kernel, warp-cooperative substitution */
 };
@@ -95,7 +96,7 @@ void croma_b200_destroy(CromaB200Context *ctx);
 /* Device workspace and state for up to ntracer tracers. */
 int croma_b200_reserve(CromaB200Context *ctx, int ntracer);
 
-/* Cap (device bytes) on the fused path's evolve workspace; tracers beyond
+/* Cap (device bytes) on the evolve workspace (either path); tracers beyond
  * what it holds run in chunks.  Takes effect at the next reserve; 0 restores
  * the default (CROMA_B200_WORKSPACE_GB, else 24 GB). */
 int croma_b200_set_workspace_limit(CromaB200Context *ctx, double bytes);
@@ -121,8 +122,7 @@ int croma_b200_snapshot(CromaB200Context *ctx, const CromaB200Snapshot *snap, in
  * resident state as set_state(crp, cre, NULL, NULL, mass, NULL), snapshot,
  * get_state(crp, cre), with the copies overlapped with the evolve.  The
  * tracers run in chunks: the upload of later chunks and the download of
- * earlier ones proceed on two copy streams while a chunk is evolved (the
- * cell-major fused path; the plain path runs the three calls in turn).
+ * earlier ones proceed on two copy streams while a chunk is evolved.
  * crp / cre ([ntracer][nb], cell-major) are read and overwritten with the
  * evolved spectra; a species the mask does not evolve is not copied back.
  * Page-locked host memory is needed for the copies to overlap.

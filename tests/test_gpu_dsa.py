@@ -4,8 +4,8 @@ The golden fixtures golden_dsa_*.npz hold the reference's own results of
 tracer_fp_apply_dsa_tracer_injection_snapshot for every shock form (raw
 shock fields, merged-DSA fields), injection mode (tracer_state,
 tracer_source) and reacceleration mode (off, positive_delta, drury83 with
-its eta cap).  The GPU path runs on the resident spectra of both layouts
-(fused: cell-major, plain: momentum-major).  Its Simpson normalisation and
+its eta cap).  The GPU path runs on the resident spectra of a context of
+either evolve path.  Its Simpson normalisation and
 cumulative integrals are summed in a different order, so the bar is the
 FP64 parity tolerance, 1e-10 relative; counts and flags are exact.  A DSA
 injection followed by a snapshot is checked against the oracle doing the
