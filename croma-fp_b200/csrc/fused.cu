@@ -128,6 +128,18 @@ __device__ __forceinline__ void rescale2(double &m00, double &m01, double &m10, 
     m00 *= sc; m01 *= sc; m10 *= sc; m11 *= sc;
 }
 
+// coulomb_kernel_fast with its erf / exp branch out of line: the proton
+// terms otherwise inline four copies of it, and the factor kernel's code
+// outgrows the instruction cache.  Same arithmetic.
+__device__ __noinline__ double coulomb_slow(double x)
+{
+    return 0.5 * sqrt(kPi) * erf(sqrt(x)) - sqrt(x) * exp(-x);
+}
+__device__ __forceinline__ double coulomb_one(double x)
+{
+    return (x > 40.0) ? 0.5 * sqrt(kPi) : coulomb_slow(x);
+}
+
 // Per-tracer constants of species S for one segment.
 template <int S>
 struct SegTerms {
@@ -159,7 +171,7 @@ struct SegTerms {
         if (S == 0) {
             const double xp = tab[TB_X1 * kTabStride + j] * inv_kbt;
             const double xe = xp * (kMe / kMp);
-            const double sum = coulomb_kernel_fast(xe) + coulomb_kernel_fast(xp) * (kMe / kMp);
+            const double sum = coulomb_one(xe) + coulomb_one(xp) * (kMe / kMp);
             const double thermal = 1.0 - kbt * tab[TB_X2 * kTabStride + j];
             const double coul = (thermal < 0.0)
                 ? 0.0
