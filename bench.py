@@ -41,6 +41,10 @@ UNIT = "tracer-snapshot updates/s"
 # tracers (profiles/steps_factor_secondary_batching_e_p_256.txt); traffic
 # scales with the tracer count (every tracer moves its own rows).
 NCU_DRAM_BYTES_PER_TRACER_STEPS_LAUNCH = (3.289360e9 + 1.120041e9 + 4.395261e9 + 0.114444e9) / 2 / 32768
+# plain_steps_kernel DRAM read + write per tracer per launch (one segment slot
+# of 31.25 sub-steps), mean of the proton and electron launches, from one ncu
+# capture at 32,768 tracers of the same workload
+NCU_DRAM_BYTES_PER_TRACER_PLAIN_LAUNCH = (272.135680e6 + 48.561664e6 + 339.285760e6 + 53.114880e6) / 2 / 32768
 
 
 def load_package():
@@ -353,8 +357,11 @@ def run_gpu_arm(args):
         avg_launch_ms = evolve_ms / max(1, evolve_n)
         achieved = per_launch / (avg_launch_ms / 1e3) / 1e9
         peak = float(peaks.get("hbm_gbs", 6650.0))
+        traffic = NCU_DRAM_BYTES_PER_TRACER_PLAIN_LAUNCH * nt if args.tracers == NTRACER else None
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                    "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                    "traffic_note": "each warp runs its slot's sub-steps back to back, so the per-step "
+                                    "re-reads of the contract hit L2; DRAM sees ~3 % of the contract bytes",
                     "kernel": "plain_steps_kernel", "launches": evolve_n,
                     "kernel_ms_total": evolve_ms, "share_of_step": evolve_ms / ms if ms > 0 else None,
                     "alg_bytes_per_launch": per_launch,

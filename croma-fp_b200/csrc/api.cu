@@ -1,6 +1,8 @@
 // api.cu -- the native C ABI (include/croma_b200.h).
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "croma_ctx.cuh"
@@ -20,6 +22,35 @@ int cuda_fail(cudaError_t e, const char *what)
     set_error(std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) +
               ") at " + what);
     return -3;
+}
+
+// The device's default pool keeps up to this many freed bytes for reuse
+// (instead of returning them to the driver at each synchronisation).
+constexpr uint64_t kPoolKeepBytes = 16ull << 30;
+
+cudaError_t dev_alloc_bytes(Context &c, void **p, size_t bytes)
+{
+    static std::mutex mu;
+    static bool configured[64] = {};
+    if (c.device >= 0 && c.device < 64) {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!configured[c.device]) {
+            cudaMemPool_t pool = nullptr;
+            if (cudaDeviceGetDefaultMemPool(&pool, c.device) == cudaSuccess) {
+                uint64_t keep = kPoolKeepBytes;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            }
+            configured[c.device] = true;
+        }
+    }
+    *p = nullptr;
+    if (bytes == 0) return cudaSuccess;
+    return cudaMallocAsync(p, bytes, c.stream);
+}
+
+void dev_free(Context &c, void *p)
+{
+    if (p) cudaFreeAsync(p, c.stream);
 }
 
 cudaEvent_t pooled_event(Context &ctx)
@@ -56,18 +87,18 @@ namespace {
 
 void free_state(Context &c)
 {
-    cudaFree(c.d_crp); cudaFree(c.d_cre); cudaFree(c.d_qpi); cudaFree(c.d_qepri);
-    cudaFree(c.d_mass); cudaFree(c.d_dis); cudaFree(c.d_bg);
+    dev_free(c, c.d_crp); dev_free(c, c.d_cre); dev_free(c, c.d_qpi); dev_free(c, c.d_qepri);
+    dev_free(c, c.d_mass); dev_free(c, c.d_dis); dev_free(c, c.d_bg);
     c.d_crp = c.d_cre = c.d_qpi = c.d_qepri = c.d_mass = c.d_bg = nullptr;
     c.d_dis = nullptr;
-    cudaFree(c.d_inje); cudaFree(c.d_eta_scale);
+    dev_free(c, c.d_inje); dev_free(c, c.d_eta_scale);
     c.d_inje = c.d_eta_scale = nullptr;
-    cudaFree(c.d_fac); cudaFree(c.d_np_seg); cudaFree(c.d_segpre);
+    dev_free(c, c.d_fac); dev_free(c, c.d_np_seg); dev_free(c, c.d_segpre);
     c.d_fac = c.d_np_seg = nullptr;
     c.d_segpre = nullptr;
     c.fused_chunk = c.fused_nseg = c.fused_sets = 0;
-    cudaFree(c.d_sched_int); cudaFree(c.d_capped); cudaFree(c.d_cub_tmp);
-    cudaFree(c.d_keys); cudaFree(c.d_vals);
+    dev_free(c, c.d_sched_int); dev_free(c, c.d_capped); dev_free(c, c.d_cub_tmp);
+    dev_free(c, c.d_keys); dev_free(c, c.d_vals);
     c.d_sched_int = nullptr; c.d_capped = nullptr; c.d_cub_tmp = nullptr;
     c.d_keys = nullptr; c.d_vals = nullptr;
     c.cap = c.ntracer = 0;
@@ -165,9 +196,9 @@ int croma_b200_create(const CromaB200Config *cfg, int device, CromaB200Context *
     mp.t_acc_off_gyr = cfg->t_acc_off_gyr;
     int rc = 0;
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) rc = -3;
-    if (rc == 0 && cudaMalloc(&c.d_err, sizeof(unsigned)) != cudaSuccess) rc = -3;
+    if (rc == 0 && dev_alloc(c, &c.d_err, sizeof(unsigned)) != cudaSuccess) rc = -3;
     if (rc == 0 && cudaMemsetAsync(c.d_err, 0, sizeof(unsigned), c.stream) != cudaSuccess) rc = -3;
-    if (rc == 0 && cudaMalloc(&c.d_ic, 2 * (size_t)kIcSlotDoubles * sizeof(double)) != cudaSuccess) rc = -3;
+    if (rc == 0 && dev_alloc(c, &c.d_ic, 2 * (size_t)kIcSlotDoubles * sizeof(double)) != cudaSuccess) rc = -3;
     if (rc == 0) rc = build_tables(c);
     if (rc != 0) {
         if (g_last_error.empty()) set_error("context creation failed");
@@ -187,10 +218,10 @@ void croma_b200_destroy(CromaB200Context *h)
     free_state(c);
     for (auto &t : c.timed) { cudaEventDestroy(t.start); cudaEventDestroy(t.stop); }
     for (auto e : c.event_pool) cudaEventDestroy(e);
-    cudaFree(c.d_tables);
-    cudaFree(c.d_np_min_qe);
-    cudaFree(c.d_ic);
-    cudaFree(c.d_err);
+    dev_free(c, c.d_tables);
+    dev_free(c, c.d_np_min_qe);
+    dev_free(c, c.d_ic);
+    dev_free(c, c.d_err);
     free_ic_stage(c);
     free_dsa(c);
     for (auto e : c.pipe_up) cudaEventDestroy(e);
@@ -218,13 +249,13 @@ int croma_b200_reserve(CromaB200Context *h, int ntracer)
     CROMA_CUDA(cudaStreamSynchronize(c.stream));
     free_state(c);
     const size_t n = (size_t)ntracer, st = (size_t)NB * n * sizeof(double);
-    CROMA_CUDA(cudaMalloc(&c.d_crp, st));
-    CROMA_CUDA(cudaMalloc(&c.d_cre, st));
-    CROMA_CUDA(cudaMalloc(&c.d_qpi, st));
-    CROMA_CUDA(cudaMalloc(&c.d_qepri, st));
-    CROMA_CUDA(cudaMalloc(&c.d_mass, n * sizeof(double)));
-    CROMA_CUDA(cudaMalloc(&c.d_dis, n));
-    CROMA_CUDA(cudaMalloc(&c.d_bg, 2 * (size_t)kNbg * n * sizeof(double)));
+    CROMA_CUDA(dev_alloc(c, &c.d_crp, st));
+    CROMA_CUDA(dev_alloc(c, &c.d_cre, st));
+    CROMA_CUDA(dev_alloc(c, &c.d_qpi, st));
+    CROMA_CUDA(dev_alloc(c, &c.d_qepri, st));
+    CROMA_CUDA(dev_alloc(c, &c.d_mass, n * sizeof(double)));
+    CROMA_CUDA(dev_alloc(c, &c.d_dis, n));
+    CROMA_CUDA(dev_alloc(c, &c.d_bg, 2 * (size_t)kNbg * n * sizeof(double)));
     CROMA_CUDA(cudaMemsetAsync(c.d_crp, 0, st, c.stream));
     CROMA_CUDA(cudaMemsetAsync(c.d_cre, 0, st, c.stream));
     CROMA_CUDA(cudaMemsetAsync(c.d_qpi, 0, st, c.stream));
@@ -282,9 +313,10 @@ int croma_b200_set_state_broadcast(CromaB200Context *h, int ntracer, const doubl
         if (rc) return rc;
     }
     double *d_rows = nullptr;
-    CROMA_CUDA(cudaMalloc(&d_rows, 2 * NB * sizeof(double)));
-    cudaError_t e = cudaMemcpy(d_rows, crp_row, NB * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(d_rows + NB, cre_row, NB * sizeof(double), cudaMemcpyHostToDevice);
+    CROMA_CUDA(dev_alloc(c, &d_rows, 2 * NB * sizeof(double)));
+    cudaError_t e = cudaMemcpyAsync(d_rows, crp_row, NB * sizeof(double), cudaMemcpyHostToDevice, c.stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_rows + NB, cre_row, NB * sizeof(double), cudaMemcpyHostToDevice, c.stream);
     const size_t ts = (size_t)NB, js = 1;   // cell-major [tracer][nb]
     const size_t total = (size_t)ntracer * NB;
     const unsigned blocks = (unsigned)((total + 255) / 256);
@@ -302,7 +334,7 @@ int croma_b200_set_state_broadcast(CromaB200Context *h, int ntracer, const doubl
         e = cudaMemcpyAsync(c.d_mass, m.data(), (size_t)ntracer * sizeof(double), cudaMemcpyHostToDevice, c.stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
     }
-    cudaFree(d_rows);
+    dev_free(c, d_rows);
     if (e != cudaSuccess) return cuda_fail(e, "set_state_broadcast");
     c.has_sources = 0;
     return 0;

@@ -166,6 +166,24 @@ cudaEvent_t pooled_event(Context &ctx);
 void timed_begin(Context &ctx, int kind, cudaEvent_t *start);
 void timed_end(Context &ctx, int kind, cudaEvent_t start);
 
+// Stream-ordered device memory of a context (cudaMallocAsync / cudaFreeAsync
+// on its stream): allocating and freeing never synchronise the device, so
+// contexts that run side by side (the request server) do not wait on each
+// other's queued work.  Freed blocks stay in the device's pool for the next
+// allocation.  Other streams use the memory only after an event recorded on
+// the context stream, and host copies go through the context stream too.
+cudaError_t dev_alloc_bytes(Context &c, void **p, size_t bytes);
+template <class T>
+inline cudaError_t dev_alloc(Context &c, T **p, size_t bytes)
+{
+    return dev_alloc_bytes(c, reinterpret_cast<void **>(p), bytes);
+}
+void dev_free(Context &c, void *p);
+// Page-locked host staging rows for the IC outer abscissae, reused across
+// contexts (freeing page-locked memory synchronises the device).
+double *acquire_ic_stage();
+void release_ic_stage(double *p);
+
 // Error reporting shared by the translation units.
 void set_error(const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);

@@ -515,10 +515,10 @@ int dsa_inject(Context &c, const CromaB200Shocks *sh, double density_unit, doubl
         for (int k = 0; k < 10; k++) dev[k] = src[k];
     } else {
         if (c.dsa_stage_cap < n) {
-            cudaFree(c.d_dsa_stage);
+            dev_free(c, c.d_dsa_stage);
             c.d_dsa_stage = nullptr;
             c.dsa_stage_cap = 0;
-            CROMA_CUDA(cudaMalloc(&c.d_dsa_stage, (size_t)10 * n * sizeof(double)));
+            CROMA_CUDA(dev_alloc(c, &c.d_dsa_stage, (size_t)10 * n * sizeof(double)));
             c.dsa_stage_cap = n;
         }
         for (int k = 0; k < 10; k++) {
@@ -614,10 +614,11 @@ int set_dsa(Context &c, const CromaB200DsaParams *prm)
         for (int j = 0; j < NB; j++) h[(size_t)s * NB + j] = pow(10.0, base + dlogp * (double)(j + extra));
     }
     if (!c.d_dsa_p) {
-        CROMA_CUDA(cudaMalloc(&c.d_dsa_p, 2 * NB * sizeof(double)));
-        CROMA_CUDA(cudaMalloc(&c.d_dsa_count, sizeof(unsigned)));
+        CROMA_CUDA(dev_alloc(c, &c.d_dsa_p, 2 * NB * sizeof(double)));
+        CROMA_CUDA(dev_alloc(c, &c.d_dsa_count, sizeof(unsigned)));
     }
-    CROMA_CUDA(cudaMemcpy(c.d_dsa_p, h.data(), 2 * NB * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpyAsync(c.d_dsa_p, h.data(), 2 * NB * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    CROMA_CUDA(cudaStreamSynchronize(c.stream));
     c.dsa = *prm;
     c.dsa_set = 1;
     return 0;
@@ -625,9 +626,9 @@ int set_dsa(Context &c, const CromaB200DsaParams *prm)
 
 void free_dsa(Context &c)
 {
-    cudaFree(c.d_dsa_p);
-    cudaFree(c.d_dsa_count);
-    cudaFree(c.d_dsa_stage);
+    dev_free(c, c.d_dsa_p);
+    dev_free(c, c.d_dsa_count);
+    dev_free(c, c.d_dsa_stage);
     c.d_dsa_p = c.d_dsa_stage = nullptr;
     c.d_dsa_count = nullptr;
     c.dsa_stage_cap = 0;

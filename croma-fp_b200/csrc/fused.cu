@@ -1110,20 +1110,20 @@ int fused_reserve(Context &ctx, int cap)
     const WorkspaceShape w = workspace_shape(ctx.mp, cap, ctx.workspace_bytes, ctx.cfg.path == CROMA_PATH_PLAIN);
     const int nseg = w.nseg, sets = w.sets;
     const long long chunk = w.chunk;
-    cudaFree(ctx.d_inje);
-    cudaFree(ctx.d_eta_scale);
-    cudaFree(ctx.d_fac);
-    cudaFree(ctx.d_np_seg);
-    cudaFree(ctx.d_segpre);
+    dev_free(ctx, ctx.d_inje);
+    dev_free(ctx, ctx.d_eta_scale);
+    dev_free(ctx, ctx.d_fac);
+    dev_free(ctx, ctx.d_np_seg);
+    dev_free(ctx, ctx.d_segpre);
     ctx.d_inje = ctx.d_eta_scale = ctx.d_fac = ctx.d_np_seg = nullptr;
     ctx.d_segpre = nullptr;
     ctx.fused_chunk = ctx.fused_nseg = ctx.fused_sets = 0;
     const size_t rows = (size_t)nseg * chunk * NB;
-    CROMA_CUDA(cudaMalloc(&ctx.d_fac, (size_t)2 * sets * rows * 3 * sizeof(double)));
-    CROMA_CUDA(cudaMalloc(&ctx.d_np_seg, rows * sizeof(double)));
-    CROMA_CUDA(cudaMalloc(&ctx.d_inje, rows * sizeof(double)));
-    CROMA_CUDA(cudaMalloc(&ctx.d_eta_scale, (size_t)cap * sizeof(double)));
-    CROMA_CUDA(cudaMalloc(&ctx.d_segpre, (size_t)nseg * chunk * sizeof(SegPre)));
+    CROMA_CUDA(dev_alloc(ctx, &ctx.d_fac, (size_t)2 * sets * rows * 3 * sizeof(double)));
+    CROMA_CUDA(dev_alloc(ctx, &ctx.d_np_seg, rows * sizeof(double)));
+    CROMA_CUDA(dev_alloc(ctx, &ctx.d_inje, rows * sizeof(double)));
+    CROMA_CUDA(dev_alloc(ctx, &ctx.d_eta_scale, (size_t)cap * sizeof(double)));
+    CROMA_CUDA(dev_alloc(ctx, &ctx.d_segpre, (size_t)nseg * chunk * sizeof(SegPre)));
     ctx.fused_chunk = (int)chunk;
     ctx.fused_nseg = nseg;
     ctx.fused_sets = sets;

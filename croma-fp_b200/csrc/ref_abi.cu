@@ -475,13 +475,15 @@ void cuda_pipeline_workspace_destroy(FpCudaPipelineWorkspace *w)
     cudaFree(w->b_bg); cudaFree(w->b_ric); cudaFree(w->b_crp); cudaFree(w->b_cre);
     cudaFree(w->b_qpi); cudaFree(w->b_qepri); cudaFree(w->b_mass); cudaFree(w->b_dis); cudaFree(w->b_idx);
     cudaFree(w->r_crp); cudaFree(w->r_cre); cudaFree(w->r_qpi); cudaFree(w->r_qepri);
-    cudaFree(c.d_inje);
-    cudaFree(c.d_eta_scale);
-    cudaFree(c.d_fac);
-    cudaFree(c.d_np_seg);
-    cudaFree(c.d_segpre);
-    cudaFree(c.d_tables);
-    cudaFree(c.d_np_min_qe);
+    // buffers the shared context code allocated on the context stream
+    dev_free(c, c.d_inje);
+    dev_free(c, c.d_eta_scale);
+    dev_free(c, c.d_fac);
+    dev_free(c, c.d_np_seg);
+    dev_free(c, c.d_segpre);
+    dev_free(c, c.d_tables);
+    dev_free(c, c.d_np_min_qe);
+    if (c.stream) cudaStreamSynchronize(c.stream);
     cudaFree(c.d_err);
     for (auto &t : c.timed) { cudaEventDestroy(t.start); cudaEventDestroy(t.stop); }
     for (auto e : c.event_pool) cudaEventDestroy(e);

@@ -191,16 +191,16 @@ int schedule_reserve(Context &ctx, int cap)
 {
     // ints: nsub, non, target, nseg, bucket_ids, bucket_indices, nbuckets(+pad), and aux
     if (ctx.d_sched_int) {
-        cudaFree(ctx.d_sched_int);
-        cudaFree(ctx.d_capped);
-        cudaFree(ctx.d_cub_tmp);
-        cudaFree(ctx.d_keys);
-        cudaFree(ctx.d_vals);
+        dev_free(ctx, ctx.d_sched_int);
+        dev_free(ctx, ctx.d_capped);
+        dev_free(ctx, ctx.d_cub_tmp);
+        dev_free(ctx, ctx.d_keys);
+        dev_free(ctx, ctx.d_vals);
         ctx.d_sched_int = nullptr;
     }
     const size_t n = (size_t)cap;
-    CROMA_CUDA(cudaMalloc(&ctx.d_sched_int, (n * 6 + 32) * sizeof(int)));
-    CROMA_CUDA(cudaMalloc(&ctx.d_capped, n));
+    CROMA_CUDA(dev_alloc(ctx, &ctx.d_sched_int, (n * 6 + 32) * sizeof(int)));
+    CROMA_CUDA(dev_alloc(ctx, &ctx.d_capped, n));
     int *p = ctx.d_sched_int;
     ctx.sched.nsub = p;
     ctx.sched.non = p + n;
@@ -211,9 +211,9 @@ int schedule_reserve(Context &ctx, int cap)
     ctx.sched.nbuckets = p + 6 * n;
     ctx.sched.capped = ctx.d_capped;
     // keys/vals double buffers + aux (head/scan, first keys, seg ids, bucket_of_seg, counts)
-    CROMA_CUDA(cudaMalloc(&ctx.d_keys, n * 3 * sizeof(unsigned long long)));
+    CROMA_CUDA(dev_alloc(ctx, &ctx.d_keys, n * 3 * sizeof(unsigned long long)));
     ctx.d_keys_alt = ctx.d_keys + n;
-    CROMA_CUDA(cudaMalloc(&ctx.d_vals, n * 8 * sizeof(int)));
+    CROMA_CUDA(dev_alloc(ctx, &ctx.d_vals, n * 8 * sizeof(int)));
     ctx.d_vals_alt = ctx.d_vals + n;
     ctx.d_seg_aux = ctx.d_vals + 2 * n;
     size_t b1 = 0, b2 = 0;
@@ -222,7 +222,7 @@ int schedule_reserve(Context &ctx, int cap)
     CROMA_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b1, kb, vb, cap, 0, 64, ctx.stream));
     CROMA_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b2, ctx.d_seg_aux, ctx.d_seg_aux, cap, ctx.stream));
     ctx.cub_tmp_bytes = (b1 > b2 ? b1 : b2) + 256;
-    CROMA_CUDA(cudaMalloc(&ctx.d_cub_tmp, ctx.cub_tmp_bytes));
+    CROMA_CUDA(dev_alloc(ctx, &ctx.d_cub_tmp, ctx.cub_tmp_bytes));
     return 0;
 }
 

@@ -14,6 +14,7 @@
 // and the outer abscissae are evaluated on the host and shared by all bins.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "croma_ctx.cuh"
@@ -234,11 +235,11 @@ int build_tables(Context &ctx)
     }
 
     // ---- device allocation ----
-    if (ctx.d_tables) cudaFree(ctx.d_tables);
-    if (ctx.d_np_min_qe) cudaFree(ctx.d_np_min_qe);
+    dev_free(ctx, ctx.d_tables);
+    dev_free(ctx, ctx.d_np_min_qe);
     ctx.d_tables = nullptr;
     ctx.d_np_min_qe = nullptr;
-    CROMA_CUDA(cudaMalloc(&ctx.d_tables, tab_doubles * sizeof(double)));
+    CROMA_CUDA(dev_alloc(ctx, &ctx.d_tables, tab_doubles * sizeof(double)));
     double *d = ctx.d_tables;
     auto darr = [&](int k) { return d + (size_t)k * n; };
     for (int s = 0; s < 2; s++) {
@@ -302,9 +303,9 @@ int build_tables(Context &ctx)
     {
         double *d_vals = nullptr, *d_aux = nullptr;
         int *d_npmin = nullptr;
-        CROMA_CUDA(cudaMalloc(&d_vals, (size_t)n * n * sizeof(double)));
-        CROMA_CUDA(cudaMalloc(&d_aux, (size_t)n * 2 * sizeof(double)));
-        CROMA_CUDA(cudaMalloc(&d_npmin, (size_t)n * sizeof(int)));
+        CROMA_CUDA(dev_alloc(ctx, &d_vals, (size_t)n * n * sizeof(double)));
+        CROMA_CUDA(dev_alloc(ctx, &d_aux, (size_t)n * 2 * sizeof(double)));
+        CROMA_CUDA(dev_alloc(ctx, &d_npmin, (size_t)n * sizeof(int)));
         CROMA_CUDA(cudaMemcpyAsync(d_aux, beta_p.data(), n * sizeof(double), cudaMemcpyHostToDevice,
                                    ctx.stream));
         dim3 g((n + 127) / 128, n);
@@ -319,8 +320,8 @@ int build_tables(Context &ctx)
         CROMA_CUDA(cudaMemcpyAsync(ctx.h_np_min_qe.data(), d_npmin, n * sizeof(int),
                                    cudaMemcpyDeviceToHost, ctx.stream));
         CROMA_CUDA(cudaStreamSynchronize(ctx.stream));
-        cudaFree(d_vals);
-        cudaFree(d_aux);
+        dev_free(ctx, d_vals);
+        dev_free(ctx, d_aux);
         ctx.d_np_min_qe = d_npmin;
         // first proton bin any electron bin draws from (fp_shared_core.c:1615-1623)
         int jp0 = n;
@@ -349,7 +350,11 @@ int ic_rows(Context &ctx, double z, double *d_out)
         return -2;
     }
     if (!ctx.h_ic_stage) {
-        CROMA_CUDA(cudaMallocHost(&ctx.h_ic_stage, 2 * (size_t)(kIcMaxOuter + 1) * sizeof(double)));
+        ctx.h_ic_stage = acquire_ic_stage();
+        if (!ctx.h_ic_stage) {
+            set_error("page-locked IC staging allocation failed");
+            return -4;
+        }
         for (int k = 0; k < 2; k++)
             CROMA_CUDA(cudaEventCreateWithFlags(&ctx.ic_stage_ev[k], cudaEventDisableTiming));
     }
@@ -379,8 +384,34 @@ void free_ic_stage(Context &ctx)
         if (ctx.ic_stage_ev[k]) cudaEventDestroy(ctx.ic_stage_ev[k]);
         ctx.ic_stage_ev[k] = nullptr;
     }
-    if (ctx.h_ic_stage) cudaFreeHost(ctx.h_ic_stage);
+    if (ctx.h_ic_stage) release_ic_stage(ctx.h_ic_stage);
     ctx.h_ic_stage = nullptr;
+}
+
+namespace {
+std::mutex g_stage_mu;
+std::vector<double *> g_stage_free;   // released staging rows, kept for the process
+}  // namespace
+
+double *acquire_ic_stage()
+{
+    {
+        std::lock_guard<std::mutex> lk(g_stage_mu);
+        if (!g_stage_free.empty()) {
+            double *p = g_stage_free.back();
+            g_stage_free.pop_back();
+            return p;
+        }
+    }
+    double *p = nullptr;
+    if (cudaMallocHost(&p, 2 * (size_t)(kIcMaxOuter + 1) * sizeof(double)) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void release_ic_stage(double *p)
+{
+    std::lock_guard<std::mutex> lk(g_stage_mu);
+    g_stage_free.push_back(p);
 }
 
 }  // namespace croma
