@@ -280,6 +280,86 @@ __global__ void synch_table_kernel(int ncell, int nfreq, int nlogb, double logb_
     out[(size_t)icell * nfreq + nf] = A * integral;
 }
 
+// The synchrotron F(x) of the log-tabulated kernel at logx: 0 above the
+// table, 0 below its first cell, the last value past its last cell, else
+// 10^(log-linear interpolation) -- the lookup of SYN_emissivity_from_arrays
+// (src/Synchrotron.c:81-97) and prepare_synch_pitch_kernel_table
+// (src/fp_shared_core.c:2027-2042).
+struct SynchFx {
+    int nx;
+    double xmin, inv_dlogx, logx_last, fx_last;
+    const double *logx_tab, *logfx_tab;
+    __device__ double operator()(double logx) const
+    {
+        if (!(logx <= logx_last)) return 0.0;
+        const int ix = (int)floor((logx - xmin) * inv_dlogx);
+        if (ix < 0) return 0.0;
+        if (ix >= nx - 1) return fx_last;
+        const double frac = (logx - logx_tab[ix]) * inv_dlogx;
+        return pow(10.0, logfx_tab[ix] + frac * (logfx_tab[ix + 1] - logfx_tab[ix]));
+    }
+};
+
+// sum_k F(logy[nf][je][k] - logb) w_k, the pitch-angle integral of one
+// (frequency, electron bin) at one log B
+__device__ __forceinline__ double pitch_integral(const SynchFx &F, const double *logy_row, const double *w,
+                                                 int ntheta, double logb)
+{
+    double s = 0.0;
+    for (int k = 0; k < ntheta; k++) s += F(logy_row[k] - logb) * w[k];
+    return s;
+}
+
+// prepare_synch_pitch_kernel_table (src/fp_shared_core.c:2008-2052): table
+// [nlogb][nfreq][npe], one thread per entry.
+__global__ void synch_pitch_table_kernel(SynchFx F, int nfreq, int ntheta, int nlogb, double logb_min,
+                                         double inv_dlogb, const double *logy, const double *w, double *table)
+{
+    const long long total = (long long)nlogb * nfreq * NB;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int je = (int)(i % NB);
+        const long long r = i / NB;
+        const int nf = (int)(r % nfreq), ib = (int)(r / nfreq);
+        const double logb = logb_min + (double)ib / inv_dlogb;
+        table[i] = pitch_integral(F, logy + ((size_t)nf * NB + je) * ntheta, w, ntheta, logb);
+    }
+}
+
+// prepare_synch_emission_cell_major without a pitch-kernel table
+// (src/fp_shared_core.c:2113-2120 -> SYN_emissivity_from_arrays,
+// src/Synchrotron.c:62-103): one warp per (cell, frequency).  The bins run
+// from 2 up to the first je whose N[je+1] is not positive (found by a
+// ballot); lanes take strided bins and a shuffle tree sums them.
+__global__ void __launch_bounds__(128) synch_theta_kernel(SynchFx F, int ncell, int nfreq, int ntheta,
+                                                          double a0, double den1, double den2,
+                                                          const double *logy, const double *w,
+                                                          const double *b_dyn, const double *logb,
+                                                          const double *cre, const double *dp, double *out)
+{
+    const int lane = threadIdx.x & 31;
+    const long long idx = (long long)blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (idx >= (long long)ncell * nfreq) return;
+    const int icell = (int)(idx / nfreq), nf = (int)(idx % nfreq);
+    const double *N = cre + (size_t)icell * NB;
+    int stop = NB - 1;   // first je >= 2 with N[je+1] <= 0, else npe - 1
+    for (int j0 = 2; j0 < NB - 1; j0 += 32) {
+        const int je = j0 + lane;
+        const unsigned hit = __ballot_sync(0xffffffffu, je < NB - 1 && !(N[je + 1] > 0.0));
+        if (hit) {
+            stop = j0 + __ffs(hit) - 1;
+            break;
+        }
+    }
+    const double lb = logb[icell];
+    double s = 0.0;
+    for (int je = 2 + lane; je < stop; je += 32)
+        s += N[je] * pitch_integral(F, logy + ((size_t)nf * NB + je) * ntheta, w, ntheta, lb) * dp[je];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) out[idx] = a0 * b_dyn[icell] / den1 / den2 * s;
+}
+
 // One-shot device buffers of the stateless entry points (grow-only, guarded).
 struct Scratch {
     std::vector<void *> ptrs;
@@ -770,14 +850,98 @@ int prepare_neutrino_emission_cuda_batch(const FpNeutrinoEmissionBatchInput *in,
                              in->n_gas, in->beta_p, in->fnu_flat, crp_grid, eps_nu_out, elapsed_ms);
 }
 
+}  // extern "C"
+
+namespace {
+
+int synch_emission_theta(const FpSynchEmissionBatchInput *in, const CRspectrum *cre_grid, double *eps_syn_out,
+                         double *elapsed_ms);
+
+// The F(x) table, pitch weights and logy of a synchrotron input on the
+// device (logy gathered from the caller's [nfreq][npe][ntheta] pointer view).
+struct SynchTables {
+    SynchFx F{};
+    double *d_logy = nullptr, *d_w = nullptr;
+};
+
+int upload_synch_tables(const FpSynchEmissionBatchInput *in, Scratch &s, SynchTables &t)
+{
+    if (in->nx_tab <= 0 || in->ntheta_pitch <= 0 || !in->fx_tab || !in->logfx_tab || !in->logx_tab ||
+        !in->logy || !in->pitch_weight)
+        return fail(-1, "incomplete synchrotron tables (fx, logfx, logx, logy, pitch weights)");
+    const int nx = in->nx_tab, nth = in->ntheta_pitch, nfreq = in->nfreq;
+    std::vector<double> logy((size_t)nfreq * NB * nth);
+    for (int nf = 0; nf < nfreq; nf++) {
+        if (!in->logy[nf]) return fail(-1, "null logy plane");
+        for (int je = 0; je < NB; je++) {
+            if (!in->logy[nf][je]) return fail(-1, "null logy row");
+            memcpy(logy.data() + ((size_t)nf * NB + je) * nth, in->logy[nf][je], (size_t)nth * sizeof(double));
+        }
+    }
+    double *d_logx = nullptr, *d_logfx = nullptr;
+    CROMA_CUDA(s.get((void **)&d_logx, (size_t)nx * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_logfx, (size_t)nx * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&t.d_logy, logy.size() * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&t.d_w, (size_t)nth * sizeof(double)));
+    CROMA_CUDA(cudaMemcpy(d_logx, in->logx_tab, (size_t)nx * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_logfx, in->logfx_tab, (size_t)nx * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(t.d_logy, logy.data(), logy.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(t.d_w, in->pitch_weight, (size_t)nth * sizeof(double), cudaMemcpyHostToDevice));
+    t.F.nx = nx;
+    t.F.xmin = in->xmin;
+    t.F.inv_dlogx = (nx > 1) ? 1.0 / (in->logx_tab[1] - in->logx_tab[0]) : 0.0;
+    t.F.logx_last = in->logx_tab[nx - 1];
+    t.F.fx_last = in->fx_tab[nx - 1];
+    t.F.logx_tab = d_logx;
+    t.F.logfx_tab = d_logfx;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int prepare_synch_pitch_kernel_table_cuda(const FpSynchEmissionBatchInput *in, double *kernel_table,
+                                          double *elapsed_ms)
+{
+    if (!in || !kernel_table || in->nlogb <= 1 || in->nfreq <= 0 || !(in->inv_dlogb > 0.0))
+        return fail(-1, "invalid synchrotron pitch-kernel table input");
+    Scratch s;
+    SynchTables t;
+    int rc = upload_synch_tables(in, s, t);
+    if (rc) return rc;
+    const size_t n = (size_t)in->nlogb * in->nfreq * NB;
+    double *d_table = nullptr;
+    CROMA_CUDA(s.get((void **)&d_table, n * sizeof(double)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    long long blocks = ((long long)n + 255) / 256;
+    if (blocks > 16LL * nsm) blocks = 16LL * nsm;
+    synch_pitch_table_kernel<<<(unsigned)blocks, 256>>>(t.F, in->nfreq, in->ntheta_pitch, in->nlogb,
+                                                        in->logb_min, in->inv_dlogb, t.d_logy, t.d_w, d_table);
+    CROMA_CUDA(cudaGetLastError());
+    CROMA_CUDA(cudaMemcpy(kernel_table, d_table, n * sizeof(double), cudaMemcpyDeviceToHost));
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    if (elapsed_ms) *elapsed_ms = elapsed(e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return 0;
+}
+
 int prepare_synch_emission_cuda_batch(const FpSynchEmissionBatchInput *in, const CRspectrum *cre_grid,
                                       double *eps_syn_out, double *elapsed_ms)
 {
     if (!in || !cre_grid || !eps_syn_out || in->ncell <= 0 || in->nfreq <= 0)
         return fail(-1, "invalid synchrotron input");
-    if (!in->pitch_kernel_table || in->nlogb <= 1 || !(in->inv_dlogb > 0.0))
-        return fail(-1, "synchrotron emission needs the pitch-kernel table");
     if (!in->b_dyn || !in->logb || !in->cre_batch) return fail(-1, "incomplete synchrotron input");
+    if (!in->pitch_kernel_table || in->nlogb <= 1 || !(in->inv_dlogb > 0.0))
+        return synch_emission_theta(in, cre_grid, eps_syn_out, elapsed_ms);
     const int ncell = in->ncell, nfreq = in->nfreq, nlogb = in->nlogb;
     Scratch s;
     double *d_tab, *d_b, *d_lb, *d_cre, *d_dp, *d_out;
@@ -813,3 +977,46 @@ int prepare_synch_emission_cuda_batch(const FpSynchEmissionBatchInput *in, const
 }
 
 }  // extern "C"
+
+namespace {
+
+// prepare_synch_emission_cell_major's branch without a pitch-kernel table:
+// the pitch-angle integral per (frequency, bin) at each cell's log B.
+int synch_emission_theta(const FpSynchEmissionBatchInput *in, const CRspectrum *cre_grid, double *eps_syn_out,
+                         double *elapsed_ms)
+{
+    const int ncell = in->ncell, nfreq = in->nfreq;
+    Scratch s;
+    SynchTables t;
+    int rc = upload_synch_tables(in, s, t);
+    if (rc) return rc;
+    double *d_b, *d_lb, *d_cre, *d_dp, *d_out;
+    CROMA_CUDA(s.get((void **)&d_b, ncell * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_lb, ncell * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_cre, (size_t)ncell * NB * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_dp, NB * sizeof(double)));
+    CROMA_CUDA(s.get((void **)&d_out, (size_t)ncell * nfreq * sizeof(double)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    CROMA_CUDA(cudaMemcpy(d_b, in->b_dyn, ncell * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_lb, in->logb, ncell * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_cre, in->cre_batch, (size_t)ncell * NB * sizeof(double), cudaMemcpyHostToDevice));
+    CROMA_CUDA(cudaMemcpy(d_dp, cre_grid->dp, NB * sizeof(double), cudaMemcpyHostToDevice));
+    const double a0 = sqrt(3.0) * pow(4.8e-10, 3.0);
+    const double den1 = 2.0 * 9.11e-28 * kC * kC, den2 = 4.0 * kPi;
+    const long long warps = (long long)ncell * nfreq;
+    synch_theta_kernel<<<(unsigned)((warps + 3) / 4), 128>>>(t.F, ncell, nfreq, in->ntheta_pitch, a0, den1, den2,
+                                                            t.d_logy, t.d_w, d_b, d_lb, d_cre, d_dp, d_out);
+    CROMA_CUDA(cudaGetLastError());
+    CROMA_CUDA(cudaMemcpy(eps_syn_out, d_out, (size_t)ncell * nfreq * sizeof(double), cudaMemcpyDeviceToHost));
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    if (elapsed_ms) *elapsed_ms = elapsed(e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return 0;
+}
+
+}  // namespace

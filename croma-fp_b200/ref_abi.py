@@ -128,6 +128,7 @@ class RefAbi:
         L.prepare_neutrino_emission_cuda_batch.argtypes = L.prepare_gamma_emission_cuda_batch.argtypes
         L.prepare_synch_emission_cuda_batch.argtypes = [C.POINTER(FpSynchEmissionBatchInput),
                                                         C.POINTER(self.CRspectrum), _D, _D]
+        L.prepare_synch_pitch_kernel_table_cuda.argtypes = [C.POINTER(FpSynchEmissionBatchInput), _D, _D]
         L.cuda_get_current_device_id.argtypes = [C.c_char_p, _i]
         L.cuda_bind_local_rank.argtypes = [_i, _I]
         L.cuda_get_binding_state.argtypes = [_I, _I]

@@ -248,6 +248,21 @@ int prepare_synch_emission_cuda_batch(const FpSynchEmissionBatchInput *in,   /* 
                                       const CRspectrum *cre_grid,
                                       double *eps_syn_out,
                                       double *elapsed_ms);
+/* Both branches of prepare_synch_emission_cell_major
+ * (src/fp_shared_core.c:2070-2129): with in->pitch_kernel_table (nlogb > 1,
+ * inv_dlogb > 0) the log-K interpolation of the table; without it the
+ * pitch-angle integral of SYN_emissivity_from_arrays (src/Synchrotron.c:62-103)
+ * from fx_tab / logfx_tab / logx_tab / logy / pitch_weight. */
+
+/* The device form of the host routine prepare_synch_pitch_kernel_table
+ * (src/fp_shared_core.c:2008-2052), which tracer_fp_refresh_synch_kernel_table
+ * (src/tracer_fp_synch.c:175-240) calls on every log B range refresh:
+ * kernel_table[(ib * nfreq + nf) * npe + je] = sum_k F(logy[nf][je][k] - logb_ib)
+ * pitch_weight[k], logb_ib = logb_min + ib / inv_dlogb, written to the host
+ * array kernel_table [nlogb * nfreq * npe]. */
+int prepare_synch_pitch_kernel_table_cuda(const FpSynchEmissionBatchInput *in,
+                                          double *kernel_table,
+                                          double *elapsed_ms);
 /* The device form of the CPU routine prepare_ic_emission_batch
  * (src/fp_shared_core.c:2131-2164), which the reference's CUDA backend does not
  * provide: eps_ic[cell][band] = sum_je fic[band][je] N[cell][je] dp[je]. */

@@ -271,6 +271,58 @@ class Oracle(_Common):
         return nsub, non, bid, nbk.value
 
 
+def synch_fx(logx, xmin, logx_tab, logfx_tab, fx_tab):
+    """F(x) of the log-tabulated synchrotron kernel at each logx, as
+    SYN_emissivity_from_arrays looks it up (src/Synchrotron.c:81-97)."""
+    nx = len(logx_tab)
+    inv_dlogx = 1.0 / (logx_tab[1] - logx_tab[0]) if nx > 1 else 0.0
+    logx = np.asarray(logx, dtype=np.float64)
+    out = np.zeros_like(logx)
+    ok = logx <= logx_tab[nx - 1]
+    ix = np.floor((logx - xmin) * inv_dlogx)
+    last = ok & (ix >= nx - 1)
+    out[last] = fx_tab[nx - 1]
+    mid = ok & (ix >= 0) & (ix < nx - 1)
+    i = ix[mid].astype(np.int64)
+    frac = (logx[mid] - logx_tab[i]) * inv_dlogx
+    out[mid] = 10.0 ** (logfx_tab[i] + frac * (logfx_tab[i + 1] - logfx_tab[i]))
+    return out
+
+
+def synch_pitch_table(logy, w, logb_min, inv_dlogb, nlogb, xmin, logx_tab, logfx_tab, fx_tab):
+    """prepare_synch_pitch_kernel_table (src/fp_shared_core.c:2008-2052):
+    [nlogb][nfreq][npe] = sum_k F(logy[nf][je][k] - logb) w_k."""
+    nfreq, nb, _ = logy.shape
+    out = np.empty((nlogb, nfreq, nb))
+    for ib in range(nlogb):
+        logb = logb_min + ib / inv_dlogb
+        out[ib] = np.sum(synch_fx(logy - logb, xmin, logx_tab, logfx_tab, fx_tab) * w[None, None, :], axis=2)
+    return out
+
+
+def synch_emission_theta(cre, dp, b_dyn, logb, logy, w, xmin, logx_tab, logfx_tab, fx_tab):
+    """prepare_synch_emission_cell_major without a pitch table
+    (src/fp_shared_core.c:2113-2120 -> SYN_emissivity_from_arrays,
+    src/Synchrotron.c:62-103): eps[cell][nf] = A B-dependent prefactor times
+    sum over je = 2 .. (first je with N[je+1] <= 0) of N int_th dp."""
+    ncell, nb = cre.shape
+    nfreq = logy.shape[0]
+    out = np.empty((ncell, nfreq))
+    for i in range(ncell):
+        A = np.sqrt(3.0) * (4.8e-10 ** 3.0) * b_dyn[i] / (2.0 * 9.11e-28 * 2.999e10 * 2.999e10) \
+            / (4.0 * np.pi)
+        stop = 2
+        while stop < nb - 1 and cre[i, stop + 1] > 0.0:
+            stop += 1
+        for nf in range(nfreq):
+            s = 0.0
+            for je in range(2, stop):
+                th = float(np.sum(synch_fx(logy[nf, je] - logb[i], xmin, logx_tab, logfx_tab, fx_tab) * w))
+                s += cre[i, je] * th * dp[je]
+            out[i, nf] = A * s
+    return out
+
+
 def reference_available(nb: int) -> bool:
     return os.path.exists(os.path.join(HERE, "_ref", f"libcroma_ref_np{nb}.so"))
 
@@ -302,6 +354,9 @@ class ReferenceCPU(_Common):
                                    _I, C.POINTER(_i)]
         L.ref_dsa_inject.argtypes = [_vp, _vp, _i, _vp, _d, _d, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]
         L.ref_ic_emission.argtypes = [_i, _i, _d, _d, _d, _D, _D, _D]
+        L.ref_synch_pitch_table.argtypes = [_i, _i, _i, _i, _d, _d, _d, _D, _D, _D, _D, _D, _D]
+        L.ref_synch_emission.argtypes = [_i, _i, _i, _i, _i, _d, _d, _d, _D, _D, _D, _D, _D, _vp, _D, _D,
+                                         _D, _D]
         self.cfg = cfg
         self.nb = cfg.nb
         self.configure(threads)
@@ -331,6 +386,33 @@ class ReferenceCPU(_Common):
         if self.lib.ref_ic_emission(cre.shape[0], nbins, z, nu_min, nu_max, cre, fic, eps) != 0:
             raise RuntimeError("ref_ic_emission failed")
         return fic, eps
+
+    def synch_pitch_table(self, logy, w, logb_min, inv_dlogb, nlogb, xmin, logx_tab, logfx_tab, fx_tab):
+        """The reference's prepare_synch_pitch_kernel_table on these arrays."""
+        logy = np.ascontiguousarray(logy, np.float64)
+        nfreq, _, nth = logy.shape
+        out = np.empty((nlogb, nfreq, self.nb))
+        if self.lib.ref_synch_pitch_table(nfreq, len(logx_tab), nth, nlogb, xmin, logb_min, inv_dlogb,
+                                          _as_d(fx_tab), _as_d(logfx_tab), _as_d(logx_tab), logy,
+                                          _as_d(w), out) != 0:
+            raise RuntimeError("ref_synch_pitch_table failed")
+        return out
+
+    def synch_emission(self, cre, b_dyn, logb, logy, w, xmin, logx_tab, logfx_tab, fx_tab, table=None,
+                       logb_min=0.0, inv_dlogb=0.0):
+        """The reference's prepare_synch_emission_cell_major, with the pitch
+        table when given, else through SYN_emissivity_from_arrays."""
+        cre = np.ascontiguousarray(cre, np.float64)
+        logy = np.ascontiguousarray(logy, np.float64)
+        nfreq, _, nth = logy.shape
+        nlogb = 0 if table is None else table.shape[0]
+        tab = None if table is None else np.ascontiguousarray(table, np.float64)
+        out = np.empty((cre.shape[0], nfreq))
+        if self.lib.ref_synch_emission(cre.shape[0], nfreq, len(logx_tab), nth, nlogb, xmin, logb_min,
+                                       inv_dlogb, _as_d(fx_tab), _as_d(logfx_tab), _as_d(logx_tab), logy,
+                                       _as_d(w), _ptr(tab), _as_d(b_dyn), _as_d(logb), cre, out) != 0:
+            raise RuntimeError("ref_synch_emission failed")
+        return out
 
     def threads(self) -> int:
         return self.lib.ref_threads()

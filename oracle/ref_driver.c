@@ -485,3 +485,94 @@ int ref_ic_emission(int ncell, int nbins, double z, double nu_min, double nu_max
     in.fic_flat = fic_out;
     return prepare_ic_emission_batch(&in, &g_cre, eps_out);
 }
+
+/* ---- synchrotron emission on caller tables -------------------------------
+ * logy [nfreq][npe][ntheta] flat; the pointer views the reference expects
+ * are built here.  ref_synch_pitch_table runs prepare_synch_pitch_kernel_table
+ * (src/fp_shared_core.c:2008-2052); ref_synch_emission runs
+ * prepare_synch_emission_cell_major (src/fp_shared_core.c:2070-2129) with the
+ * table when one is given and through SYN_emissivity_from_arrays
+ * (src/Synchrotron.c:62-103) otherwise, whose pitch loop runs over the
+ * global tracer_synch_ntheta_pitch, set here to ntheta. */
+static int synch_input(FpSynchEmissionBatchInput *in, int nfreq, int nx, int ntheta, int nlogb, double xmin,
+                       double logb_min, double inv_dlogb, const double *fx, const double *logfx,
+                       const double *logx, const double *logy, const double *w, double ****planes_out)
+{
+    double ***planes = (double ***)calloc((size_t)nfreq, sizeof(double **));
+    double **rows = (double **)calloc((size_t)nfreq * (size_t)npe, sizeof(double *));
+    int nf, je;
+    if (!planes || !rows) { free(planes); free(rows); return -1; }
+    for (nf = 0; nf < nfreq; nf++) {
+        planes[nf] = rows + (size_t)nf * (size_t)npe;
+        for (je = 0; je < npe; je++)
+            planes[nf][je] = (double *)logy + ((size_t)nf * (size_t)npe + (size_t)je) * (size_t)ntheta;
+    }
+    memset(in, 0, sizeof *in);
+    in->nfreq = nfreq;
+    in->nx_tab = nx;
+    in->ntheta_pitch = ntheta;
+    in->nlogb = nlogb;
+    in->xmin = xmin;
+    in->logb_min = logb_min;
+    in->inv_dlogb = inv_dlogb;
+    in->fx_tab = fx;
+    in->logfx_tab = logfx;
+    in->logx_tab = logx;
+    in->logy = planes;
+    in->pitch_weight = w;
+    *planes_out = planes;
+    return 0;
+}
+
+static void synch_input_free(double ***planes)
+{
+    if (!planes) return;
+    free(planes[0]);
+    free(planes);
+}
+
+int ref_synch_pitch_table(int nfreq, int nx, int ntheta, int nlogb, double xmin, double logb_min,
+                          double inv_dlogb, const double *fx, const double *logfx, const double *logx,
+                          const double *logy, const double *w, double *table_out)
+{
+    FpSynchEmissionBatchInput in;
+    double ***planes = 0;
+    int rc;
+    if (synch_input(&in, nfreq, nx, ntheta, nlogb, xmin, logb_min, inv_dlogb, fx, logfx, logx, logy, w,
+                    &planes) != 0)
+        return -1;
+    rc = prepare_synch_pitch_kernel_table(&in, table_out);
+    synch_input_free(planes);
+    return rc;
+}
+
+int ref_synch_emission(int ncell, int nfreq, int nx, int ntheta, int nlogb, double xmin, double logb_min,
+                       double inv_dlogb, const double *fx, const double *logfx, const double *logx,
+                       const double *logy, const double *w, const double *table, const double *b_dyn,
+                       const double *logb, const double *cre, double *eps_out)
+{
+    FpSynchEmissionBatchInput in;
+    double ***planes = 0;
+    double *dummy;
+    int rc;
+    if (!g_ready) return -1;
+    if (synch_input(&in, nfreq, nx, ntheta, nlogb, xmin, logb_min, inv_dlogb, fx, logfx, logx, logy, w,
+                    &planes) != 0)
+        return -1;
+    /* fields the routine checks for but this branch does not read */
+    dummy = (double *)calloc((size_t)(npe > ntheta ? npe : ntheta) + (size_t)nfreq, sizeof(double));
+    in.ncell = ncell;
+    in.pitch_kernel_table = table;
+    in.b_dyn = b_dyn;
+    in.logb = logb;
+    in.cre_batch = cre;
+    in.gamma2e = dummy;
+    in.theta = dummy;
+    in.dtheta = dummy;
+    in.nus = dummy;
+    tracer_synch_ntheta_pitch = ntheta;
+    rc = dummy ? prepare_synch_emission_cell_major(&in, &g_cre, eps_out) : -1;
+    free(dummy);
+    synch_input_free(planes);
+    return rc;
+}

@@ -155,12 +155,69 @@ def make_ic_emission(name="emission_ic"):
     print(name, "written")
 
 
+def synch_inputs(ge_p, nfreq, ntheta, nu_min=5.5, nu_max=10.5):
+    """Synchrotron tables built the way tracer_fp_synch_data_init_tables
+    (src/tracer_fp_synch.c:87-121) builds them: logx grid [-25, 2.5) in 2750
+    cells, pitch angles (k + 1/2) pi / ntheta with sin^2 weights, log-spaced
+    frequencies, logy = log10(nu / (1e-6 nu_crit)) with
+    nu_crit = (1 + p^2) 4.194284e6 sin(theta) (src/Synchrotron.c:9-51).  The
+    F(x) values are a smooth positive stand-in, x^(1/3) e^(-x) scaled, not
+    the synchrotron function itself: what is checked is the lookup and the
+    integration, which do not depend on the values."""
+    nx, xmin, xmax = 2750, -25.0, 2.5
+    dx = (xmax - xmin) / nx
+    logx = xmin + dx * np.arange(nx)
+    x = 10.0 ** logx
+    fx = 2.15 * x ** (1.0 / 3.0) * np.exp(-x) + 1e-300
+    logfx = np.log10(fx)
+    fx = 10.0 ** logfx
+    theta = (np.arange(ntheta) + 0.5) * np.pi / ntheta
+    w = np.sin(theta) * np.sin(theta) * (np.pi / ntheta)
+    dnu = (nu_max - nu_min) / nfreq
+    nus = 10.0 ** (nu_min + dnu * np.arange(nfreq))
+    nu_crit = (1.0 + ge_p[:, None] ** 2) * 4.194284e6 * np.sin(theta)[None, :]
+    logy = np.log10(nus[:, None, None] / (1.0e-6 * nu_crit[None, :, :]))
+    return dict(logx=logx, logfx=logfx, fx=fx, xmin=xmin, w=w, logy=np.ascontiguousarray(logy))
+
+
+def make_synch_emission(name="emission_synch"):
+    """The reference's pitch-kernel table and both branches of its
+    synchrotron emissivity (with and without the table) on 128-bin spectra,
+    some cut off at high momenta so the stop rule at N[je+1] <= 0 acts."""
+    nb, ncell, nfreq, ntheta, nlogb = 128, 10, 6, 16, 24
+    cfg = config.config1(nb=nb)
+    ref = pyoracle.ReferenceCPU(cfg)
+    gp, ge = ref.grid(0), ref.grid(1)
+    _, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), ncell, cfg.species)
+    rng = np.random.default_rng(77)
+    cre = cre * rng.uniform(0.5, 2.0, (ncell, 1))
+    for i, cut in enumerate((112, 121, 3, 127)):
+        cre[i, cut:] = 0.0
+    b_dyn = 10.0 ** rng.uniform(-7.5, -5.0, ncell)
+    logb = np.log10(b_dyn)
+    t = synch_inputs(ge[0], nfreq, ntheta)
+    logb_min, logb_max = -8.0, -4.0
+    inv_dlogb = (nlogb - 1) / (logb_max - logb_min)
+    table = ref.synch_pitch_table(t["logy"], t["w"], logb_min, inv_dlogb, nlogb, t["xmin"], t["logx"],
+                                  t["logfx"], t["fx"])
+    eps_table = ref.synch_emission(cre, b_dyn, logb, t["logy"], t["w"], t["xmin"], t["logx"], t["logfx"],
+                                   t["fx"], table=table, logb_min=logb_min, inv_dlogb=inv_dlogb)
+    eps_theta = ref.synch_emission(cre, b_dyn, logb, t["logy"], t["w"], t["xmin"], t["logx"], t["logfx"],
+                                   t["fx"])
+    np.savez_compressed(os.path.join(HERE, f"golden_{name}.npz"), nb=nb, cre=cre, dp=ge[1], b_dyn=b_dyn,
+                        logb=logb, logb_min=logb_min, inv_dlogb=inv_dlogb, nlogb=nlogb, table=table,
+                        eps_table=eps_table, eps_theta=eps_theta, **t)
+    print(name, "written")
+
+
 if __name__ == "__main__":
-    names = sys.argv[1:] or list(CASES) + list(DSA_CASES) + ["emission_ic"]
+    names = sys.argv[1:] or list(CASES) + list(DSA_CASES) + ["emission_ic", "emission_synch"]
     for n in names:
         if n in DSA_CASES:
             make_dsa_case(n, DSA_CASES[n])
         elif n == "emission_ic":
             make_ic_emission(n)
+        elif n == "emission_synch":
+            make_synch_emission(n)
         else:
             make_case(n, CASES[n])
