@@ -355,6 +355,17 @@ class ReferenceCPU(_Common):
         L.ref_dsa_inject.argtypes = [_vp, _vp, _i, _vp, _d, _d, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]
         L.ref_ic_emission.argtypes = [_i, _i, _d, _d, _d, _D, _D, _D]
         L.ref_synch_pitch_table.argtypes = [_i, _i, _i, _i, _d, _d, _d, _D, _D, _D, _D, _D, _D]
+        _s, _l = C.c_char_p, C.c_long
+        L.ref_tile_open.argtypes = [_s, _s, _i, _l, _l, _l, _i]
+        L.ref_tile_write_cr.argtypes = [_i, _i, _i, _l, _vp, _vp, _vp, _vp, _i, _i]
+        L.ref_tile_write_emit.argtypes = [_i, _i, _l, _i, _vp, _vp, _vp, _i]
+        L.ref_tile_close.argtypes = [_i]
+        L.ref_map_open.argtypes = [_s, _s, _i, _i, _l, _i]
+        L.ref_write_cr_map.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _vp, _i]
+        L.ref_write_emit_map.argtypes = [_i, _i, _i, _i, _vp, _vp, _vp, _i]
+        L.ref_map_close.argtypes = [_i]
+        L.ref_ckpt_write.argtypes = [_s, _i, _i, _i, _i, _i, _i, _i, _l, _vp, _vp, _vp, _i, _i]
+        L.ref_ckpt_read.argtypes = [_s, _i, _i, _i, _i, _i, _i, _l, _vp, _vp, _vp, _i, _i, C.POINTER(_i)]
         L.ref_synch_emission.argtypes = [_i, _i, _i, _i, _i, _d, _d, _d, _D, _D, _D, _D, _D, _vp, _D, _D,
                                          _D, _D]
         self.cfg = cfg

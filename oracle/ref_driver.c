@@ -576,3 +576,127 @@ int ref_synch_emission(int ncell, int nfreq, int nx, int ntheta, int nlogb, doub
     synch_input_free(planes);
     return rc;
 }
+
+/* ---- output files and checkpoints (src/tracer_fp_output.c,
+ * src/tracer_fp_restart.c) on caller arrays, for byte comparisons --------
+ * Open writers live in a small table indexed by the returned handle. */
+#include "tracer_fp_output.h"
+#include "tracer_fp_restart.h"
+
+#define REF_MAX_OUT 8
+static TracerFpTileOutput g_tiles[REF_MAX_OUT];
+static TracerFpMappedOutput g_maps[REF_MAX_OUT];
+static int g_tile_used[REF_MAX_OUT], g_map_used[REF_MAX_OUT];
+
+int ref_tile_open(const char *dir, const char *stem, int rank, long nslab, long nrow, long ncol, int resume)
+{
+    int h;
+    for (h = 0; h < REF_MAX_OUT && g_tile_used[h]; h++) {}
+    if (h == REF_MAX_OUT) return -1;
+    if (tracer_fp_tile_open(&g_tiles[h], dir, stem, rank, (size_t)nslab, (size_t)nrow, (size_t)ncol, resume) != 0)
+        return -1;
+    g_tile_used[h] = 1;
+    return h;
+}
+
+int ref_tile_write_cr(int h_e, int h_p, int nlocal, long slab, const double *cre, const double *crp,
+                      const double *rho, const double *mass, int per_cc, int write_crp)
+{
+    if (h_e < 0 || h_e >= REF_MAX_OUT || !g_tile_used[h_e]) return -1;
+    return tracer_fp_tile_write_cr(&g_tiles[h_e], h_p >= 0 ? &g_tiles[h_p] : 0, nlocal, (size_t)slab, cre, crp,
+                                   rho, mass, per_cc, write_crp);
+}
+
+int ref_tile_write_emit(int h, int nlocal, long slab, int nbin, const double *eps, const double *rho,
+                        const double *mass, int per_cc)
+{
+    if (h < 0 || h >= REF_MAX_OUT || !g_tile_used[h]) return -1;
+    return tracer_fp_tile_write_emit(&g_tiles[h], nlocal, (size_t)slab, nbin, eps, rho, mass, per_cc);
+}
+
+int ref_tile_close(int h)
+{
+    if (h < 0 || h >= REF_MAX_OUT || !g_tile_used[h]) return -1;
+    g_tile_used[h] = 0;
+    return tracer_fp_tile_close(&g_tiles[h]);
+}
+
+int ref_map_open(const char *dir, const char *stem, int rank, int nrow, long ncol, int resume)
+{
+    int h;
+    for (h = 0; h < REF_MAX_OUT && g_map_used[h]; h++) {}
+    if (h == REF_MAX_OUT) return -1;
+    if (tracer_fp_map_open(&g_maps[h], dir, stem, rank, nrow, (size_t)ncol, resume) != 0) return -1;
+    g_map_used[h] = 1;
+    return h;
+}
+
+int ref_write_cr_map(int h_e, int h_p, int nlocal, int slot, const double *cre, const double *crp,
+                     const double *rho, const double *mass, int per_cc)
+{
+    if (h_e < 0 || h_e >= REF_MAX_OUT || !g_map_used[h_e]) return -1;
+    return tracer_fp_write_cr_map(&g_maps[h_e], h_p >= 0 ? &g_maps[h_p] : 0, nlocal, slot, cre, crp, rho, mass,
+                                  per_cc);
+}
+
+int ref_write_emit_map(int h, int nlocal, int snapshot_index, int nbin, const double *eps, const double *rho,
+                       const double *mass, int per_cc)
+{
+    if (h < 0 || h >= REF_MAX_OUT || !g_map_used[h]) return -1;
+    return tracer_fp_write_emit_map(&g_maps[h], nlocal, snapshot_index, nbin, eps, rho, mass, per_cc);
+}
+
+int ref_map_close(int h)
+{
+    if (h < 0 || h >= REF_MAX_OUT || !g_map_used[h]) return -1;
+    g_map_used[h] = 0;
+    return tracer_fp_map_close(&g_maps[h]);
+}
+
+/* tracer_fp_ckpt_write / tracer_fp_ckpt_read with the snapshot index range
+ * globals nsnp_i / nsnp_f (params.c) set for the header. */
+int ref_ckpt_write(const char *dir, int rank, int world, int ntracer, int ntracer_global, int nsnap, int nfreq,
+                   int completed, long tracer_start, const int *ids, const double *crp, const double *cre,
+                   int nsnp_i_value, int nsnp_f_value)
+{
+    TracerFpCkptWrite w;
+    nsnp_i = nsnp_i_value;
+    nsnp_f = nsnp_f_value;
+    memset(&w, 0, sizeof w);
+    w.checkpoint_dir = dir;
+    w.mpi_rank = rank;
+    w.world_size = world;
+    w.ntracer = ntracer;
+    w.ntracer_global = ntracer_global;
+    w.nsnap = nsnap;
+    w.nfreq = nfreq;
+    w.completed_snapshot = completed;
+    w.tracer_start = tracer_start;
+    w.tracer_ids = ids;
+    w.crp_state = crp;
+    w.cre_state = cre;
+    return tracer_fp_ckpt_write(&w);
+}
+
+int ref_ckpt_read(const char *dir, int rank, int world, int ntracer, int ntracer_global, int nsnap, int nfreq,
+                  long tracer_start, const int *ids, double *crp, double *cre, int nsnp_i_value,
+                  int nsnp_f_value, int *completed)
+{
+    TracerFpCkptRead r;
+    nsnp_i = nsnp_i_value;
+    nsnp_f = nsnp_f_value;
+    memset(&r, 0, sizeof r);
+    r.restart_dir = dir;
+    r.mpi_rank = rank;
+    r.world_size = world;
+    r.ntracer = ntracer;
+    r.ntracer_global = ntracer_global;
+    r.nsnap = nsnap;
+    r.nfreq = nfreq;
+    r.tracer_start = tracer_start;
+    r.tracer_ids = ids;
+    r.crp_state = crp;
+    r.cre_state = cre;
+    r.completed_snapshot_out = completed;
+    return tracer_fp_ckpt_read(&r);
+}
