@@ -611,6 +611,25 @@ int croma_b200_get_secondary_kernel(CromaB200Context *h, double *fqe, int *np_mi
 
 void *croma_b200_stream(CromaB200Context *h) { return h ? (void *)h->impl.stream : nullptr; }
 
+int croma_b200_set_priority(CromaB200Context *h, int priority)
+{
+    if (!h) { set_error("null context"); return -1; }
+    Context &c = h->impl;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    int least = 0, greatest = 0;
+    CROMA_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    if (priority > least) priority = least;
+    if (priority < greatest) priority = greatest;
+    // the context's memory was allocated in this stream's order: let it
+    // complete before the stream is replaced
+    CROMA_CUDA(cudaStreamSynchronize(c.stream));
+    cudaStream_t s = nullptr;
+    CROMA_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, priority));
+    cudaStreamDestroy(c.stream);
+    c.stream = s;
+    return 0;
+}
+
 int croma_b200_sync(CromaB200Context *h)
 {
     if (!h) { set_error("null context"); return -1; }

@@ -68,7 +68,7 @@ __global__ void qe_weights_kernel(const double *vals, const double *dp_p, double
 // ---------------------------------------------------------------------
 constexpr int kIcMaxOuter = 2048;
 
-__global__ void ic_row_kernel(IcConsts icc, const double *p_e, double pm1, double pp1,
+__global__ void __launch_bounds__(512) ic_row_kernel(IcConsts icc, const double *p_e, double pm1, double pp1,
                               const double *outer, int nout, double z, double *row)
 {
     __shared__ double s_n[kIcMaxOuter + 1];
@@ -372,7 +372,7 @@ int ic_rows(Context &ctx, double z, double *d_out)
     CROMA_CUDA(cudaMemcpyAsync(d_outer, outer, (N + 1) * sizeof(double), cudaMemcpyHostToDevice,
                                ctx.stream));
     CROMA_CUDA(cudaEventRecord(ctx.ic_stage_ev[k], ctx.stream));
-    ic_row_kernel<<<NB + 2, 128, 0, ctx.stream>>>(ctx.icc, ctx.gt.s[1].p, ctx.h_pm1[1], ctx.h_pp1[1],
+    ic_row_kernel<<<NB + 2, 512, 0, ctx.stream>>>(ctx.icc, ctx.gt.s[1].p, ctx.h_pm1[1], ctx.h_pp1[1],
                                                   d_outer, N, z, d_out);
     CROMA_CUDA(cudaGetLastError());
     return 0;

@@ -115,6 +115,13 @@ int croma_b200_set_state_broadcast(CromaB200Context *ctx, int ntracer, const dou
  * disable-adiabatic flags [ntracer]; NULL skips an array. */
 int croma_b200_get_sources(CromaB200Context *ctx, double *qpi, double *qepri, unsigned char *dis);
 
+/* Scheduling priority of the context's stream (CUDA stream priorities: lower
+ * numbers run first; clamped to cudaDeviceGetStreamPriorityRange).  Waits
+ * for the context's queued work and replaces its stream.  The request server
+ * gives small requests the higher priorities so that their blocks are
+ * scheduled ahead of the remaining blocks of large requests' kernels. */
+int croma_b200_set_priority(CromaB200Context *ctx, int priority);
+
 /* One snapshot on the context's stream; asynchronous unless sync != 0. */
 int croma_b200_snapshot(CromaB200Context *ctx, const CromaB200Snapshot *snap, int sync);
 

@@ -15,6 +15,12 @@
  * requests start in submission order while their estimate fits the budget
  * left; a request larger than the whole budget is refused at submission.
  *
+ * Scheduling on the device: each running request's stream gets a CUDA stream
+ * priority from its size (ntracer x nsnap, log-scaled between 1e3 and 1e7
+ * tracer-snapshots; the smallest requests highest), so the blocks of a small
+ * request's kernels start ahead of the blocks a large request still has
+ * queued, instead of after them.
+ *
  * Lifetime: every pointer in a CromaB200Request must stay valid until the
  * request is done, failed or cancelled.  Functions return 0 (or an id >= 1)
  * on success and a negative code on failure (-1 invalid argument, -3 CUDA,
