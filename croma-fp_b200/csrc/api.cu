@@ -226,6 +226,7 @@ void croma_b200_destroy(CromaB200Context *h)
     free_dsa(c);
     for (auto e : c.pipe_up) cudaEventDestroy(e);
     for (auto e : c.pipe_done) cudaEventDestroy(e);
+    for (auto e : c.pipe_done_p) cudaEventDestroy(e);
     if (c.pipe_start) cudaEventDestroy(c.pipe_start);
     if (c.h2d_stream) cudaStreamDestroy(c.h2d_stream);
     if (c.d2h_stream) cudaStreamDestroy(c.d2h_stream);
@@ -498,11 +499,13 @@ int croma_b200_snapshot_host(CromaB200Context *h, const CromaB200Snapshot *s, in
     if (!c.d2h_stream) CROMA_CUDA(cudaStreamCreateWithFlags(&c.d2h_stream, cudaStreamNonBlocking));
     if (!c.pipe_start) CROMA_CUDA(cudaEventCreateWithFlags(&c.pipe_start, cudaEventDisableTiming));
     while ((int)c.pipe_up.size() < nchunk) {
-        cudaEvent_t u = nullptr, d = nullptr;
+        cudaEvent_t u = nullptr, d = nullptr, dp = nullptr;
         CROMA_CUDA(cudaEventCreateWithFlags(&u, cudaEventDisableTiming));
         c.pipe_up.push_back(u);
         CROMA_CUDA(cudaEventCreateWithFlags(&d, cudaEventDisableTiming));
         c.pipe_done.push_back(d);
+        CROMA_CUDA(cudaEventCreateWithFlags(&dp, cudaEventDisableTiming));
+        c.pipe_done_p.push_back(dp);
     }
     // the rest of the state as set_state with these arguments leaves it
     const size_t st = (size_t)NB * ntracer * sizeof(double);

@@ -49,8 +49,9 @@ struct SnapArgs {
 
 // One host-buffer snapshot in flight: the cell-major spectra of tracer chunk
 // k, [bounds[k], bounds[k+1]), are uploaded on the context's h2d stream
-// (event pipe_up[k]) and, once the chunk is evolved (event pipe_done[k] on
-// the compute stream), downloaded into the same host rows on d2h.
+// (event pipe_up[k]) and, once evolved (events pipe_done_p[k] after the
+// proton steps, pipe_done[k] after the electron steps, on the compute
+// stream), downloaded into the same host rows on d2h.
 struct HostPipe {
     double *crp = nullptr, *cre = nullptr;   // host [ntracer][nb]
     int down_p = 1, down_e = 1;              // species whose rows come back
@@ -143,7 +144,7 @@ struct Context {
     // host-buffer snapshot (croma_b200_snapshot_host): copy streams and
     // per-chunk events, created on first use; pipe is set for one call
     cudaStream_t h2d_stream = nullptr, d2h_stream = nullptr;
-    std::vector<cudaEvent_t> pipe_up, pipe_done;
+    std::vector<cudaEvent_t> pipe_up, pipe_done, pipe_done_p;
     cudaEvent_t pipe_start = nullptr;   // compute stream's earlier work, gating the uploads
     const HostPipe *pipe = nullptr;
 

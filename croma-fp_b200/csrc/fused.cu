@@ -1135,7 +1135,22 @@ int fused_reserve(Context &ctx, int cap)
 // secondary source, the electron steps.  perstep (the plain path, one slot):
 // the raw rows of both species, the secondary source from the protons at the
 // slot start, then the per-step kernels.
-static int fused_range(Context &ctx, FusedParams &P, int g0, int g1, bool perstep)
+// Host-pipeline copies of one chunk's rows of one species: after an event on
+// the compute stream, on the d2h stream.
+static int pipe_download(Context &ctx, const FusedParams &P, cudaEvent_t ev, double *host, const double *dev)
+{
+    CROMA_CUDA(cudaEventRecord(ev, ctx.stream));
+    CROMA_CUDA(cudaStreamWaitEvent(ctx.d2h_stream, ev, 0));
+    const size_t off = (size_t)P.t0 * NB, bytes = (size_t)P.nt * NB * sizeof(double);
+    CROMA_CUDA(cudaMemcpyAsync(host + off, dev + off, bytes, cudaMemcpyDeviceToHost, ctx.d2h_stream));
+    return 0;
+}
+
+// pk >= 0 (host pipeline, all segments in one launch): the chunk's upload is
+// awaited only before the first steps kernel -- the per-segment scalars and
+// the factored rows do not read the spectra -- and the proton rows go back as
+// soon as the proton steps are done.
+static int fused_range(Context &ctx, FusedParams &P, int g0, int g1, bool perstep, int pk = -1)
 {
     const SnapArgs &a = P.a;
     const int protons = ctx.mp.species_mask & CROMA_SPECIES_PROTON;
@@ -1179,6 +1194,7 @@ static int fused_range(Context &ctx, FusedParams &P, int g0, int g1, bool perste
         ctx.last_launches += 1;
     }
     timed_end(ctx, kKindCoeff, ev);
+    if (pk >= 0) CROMA_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.pipe_up[pk], 0));
     if (secondaries && perstep) {
         timed_begin(ctx, kKindSecondary, &ev);
         CROMA_CUDA(launch_secondary(ctx, P));
@@ -1190,6 +1206,10 @@ static int fused_range(Context &ctx, FusedParams &P, int g0, int g1, bool perste
         CROMA_CUDA(launch_steps<0>(ctx, P, a.qpi != nullptr, perstep));
         timed_end(ctx, kKindEvolve, ev);
         ctx.last_launches += 1;
+    }
+    if (pk >= 0 && ctx.pipe->down_p) {
+        const int rc = pipe_download(ctx, P, ctx.pipe_done_p[pk], ctx.pipe->crp, a.crp);
+        if (rc) return rc;
     }
     if (secondaries && !perstep) {
         timed_begin(ctx, kKindSecondary, &ev);
@@ -1242,26 +1262,25 @@ static int fused_chunks(Context &ctx, FusedParams &P, int nslots, bool perstep)
             set_error("internal: tracer chunk outside the fused workspace");
             return -1;
         }
-        if (pipe) CROMA_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.pipe_up[k], 0));
         if (!cap && !perstep) {
-            const int rc = fused_range(ctx, P, 0, nslots, false);
+            // one launch per kernel for the chunk: the upload wait and the
+            // proton download sit inside, next to the kernels they gate
+            const int rc = fused_range(ctx, P, 0, nslots, false, pipe ? k : -1);
             if (rc) return rc;
         } else {
+            if (pipe) CROMA_CUDA(cudaStreamWaitEvent(ctx.stream, ctx.pipe_up[k], 0));
             for (int g = 0; g < nslots; g++) {
                 const int rc = fused_range(ctx, P, g, g + 1, perstep);
                 if (rc) return rc;
             }
+            if (pipe && pipe->down_p) {
+                const int rc = pipe_download(ctx, P, ctx.pipe_done_p[k], pipe->crp, P.a.crp);
+                if (rc) return rc;
+            }
         }
-        if (pipe) {
-            CROMA_CUDA(cudaEventRecord(ctx.pipe_done[k], ctx.stream));
-            CROMA_CUDA(cudaStreamWaitEvent(ctx.d2h_stream, ctx.pipe_done[k], 0));
-            const size_t off = (size_t)P.t0 * NB, bytes = (size_t)P.nt * NB * sizeof(double);
-            if (pipe->down_p)
-                CROMA_CUDA(cudaMemcpyAsync(pipe->crp + off, P.a.crp + off, bytes, cudaMemcpyDeviceToHost,
-                                           ctx.d2h_stream));
-            if (pipe->down_e)
-                CROMA_CUDA(cudaMemcpyAsync(pipe->cre + off, P.a.cre + off, bytes, cudaMemcpyDeviceToHost,
-                                           ctx.d2h_stream));
+        if (pipe && pipe->down_e) {
+            const int rc = pipe_download(ctx, P, ctx.pipe_done[k], pipe->cre, P.a.cre);
+            if (rc) return rc;
         }
     }
     return 0;
