@@ -59,6 +59,8 @@ def load_library(nb: int) -> C.CDLL:
     L.croma_b200_get_state.argtypes = [_vp, _vp, _vp]
     L.croma_b200_snapshot.argtypes = [_vp, P(CromaB200Snapshot), _i]
     L.croma_b200_snapshot_host.argtypes = [_vp, P(CromaB200Snapshot), _i, _vp, _vp, _vp, _i]
+    L.croma_b200_set_workspace_limit.argtypes = [_vp, _d]
+    L.croma_b200_set_priority.argtypes = [_vp, _i]
     L.croma_b200_get_schedule.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.croma_b200_ic_row.argtypes = [_vp, _d, _vp]
     L.croma_b200_get_grid.argtypes = [_vp, _i, _vp]
@@ -148,6 +150,15 @@ class TracerFP:
         if rc != 0:
             msg = self.lib.croma_b200_last_error().decode()
             raise CromaError(f"croma_b200 call failed ({rc}): {msg}")
+
+    def set_workspace_limit(self, nbytes: float):
+        """Cap on the evolve workspace (takes effect at the next reserve /
+        set_state with a new tracer count); tracers beyond it run in chunks."""
+        self._check(self.lib.croma_b200_set_workspace_limit(self.h, float(nbytes)))
+
+    def set_priority(self, priority: int):
+        """CUDA stream priority of the context's stream (lower runs first)."""
+        self._check(self.lib.croma_b200_set_priority(self.h, int(priority)))
 
     def close(self):
         if getattr(self, "h", None):
