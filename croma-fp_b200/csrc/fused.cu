@@ -884,8 +884,10 @@ __global__ void __launch_bounds__(128) eta_scale_kernel(FusedParams P, double *e
 // np_min_qe[je] (prepare_secondary_kernel_flat, src/fp_shared_core.c:1453-1506),
 // so the rounded-down start adds exact zeros only.
 constexpr int kGM = 128, kGN = 64, kGK = 16;
+// Row pitches chosen so that the fragment reads of a half warp (rows gid or
+// tig, 4 x 4 lanes) land on 16 distinct bank pairs: 20 and 68 doubles.
 constexpr int kGPitchA = kGK + 4;    // sA[m][k], 20 doubles per row
-constexpr int kGPitchB = kGN + 8;    // sB[k][n], 72 doubles per row
+constexpr int kGPitchB = kGN + 4;    // sB[k][n], 68 doubles per row
 
 struct GemmSmem {
     double A[2][kGM][kGPitchA];
@@ -986,9 +988,9 @@ __global__ void __launch_bounds__(256, 2) secondary_kernel(FusedParams P)
         if (m >= nrows) continue;
         const int gi = m / P.nt, tl = m - gi * P.nt;
         const int t = P.t0 + tl;
-        const SegInfo g = segment_of(P, t, P.g0 + gi);
-        if (!g.active) continue;
-        const double ng = (g.nseg > 1) ? lerp(a.bg_curr[t], a.bg_next[t], g.alpha) : a.bg_curr[t];
+        const SegPre *__restrict__ pre = P.pre + (size_t)gi * P.nt + tl;
+        if (!(pre->flags & kPreActive)) continue;
+        const double ng = pre->n_gas;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const int je = n0 + wn + 8 * j + 2 * tig;
