@@ -30,7 +30,7 @@
 //      src/fp_shared_core.c:1591-1672), a tiled [segments*tracers x nb] .
 //      [nb x nb] product, between the proton and the electron steps.
 //
-// Shared-memory rows are stored at (m % R) * 33 + m / R, so the blocked reads
+// Shared-memory rows are stored at (m % R) * kPitch + m / R, so the blocked reads
 // of step 1 (lane l, row l*R + r and its neighbours) hit 32 distinct banks.
 // Divisions by grid quantities use reciprocals tabulated on the host; the
 // results agree with the reference's divisions to an ulp per operation.
@@ -44,7 +44,11 @@ namespace croma {
 namespace {
 
 constexpr int kR = NB / 32;          // rows per lane
-constexpr int kSw = 33 * kR;         // swizzled row-array length
+// Row pitch of the swizzled arrays: both access patterns of the factor
+// kernel -- lane-strided (m = 32 k + lane) and lane-blocked (m = R lane + r)
+// -- then touch 16 distinct 8-byte bank pairs per half warp.
+constexpr int kPitch = 32 + 16 / kR;
+constexpr int kSw = kPitch * kR;     // swizzled row-array length
 constexpr int kWarps = 4;            // warps per block
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kFacDoubles = 3 * NB;  // 1/d, a/d, c/d of one system
@@ -112,7 +116,7 @@ __device__ __forceinline__ bool needs_set(const SegInfo &g, int set)
     return (set == 0) ? el > sl : (sl > 0 || el < g.steps);
 }
 
-__device__ __forceinline__ int swz(int m) { return (m % kR) * 33 + m / kR; }
+__device__ __forceinline__ int swz(int m) { return (m % kR) * kPitch + m / kR; }
 __device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 __device__ __forceinline__ double sup(double v, int d) { return __shfl_up_sync(kFull, v, d); }
 __device__ __forceinline__ double sdn(double v, int d) { return __shfl_down_sync(kFull, v, d); }
@@ -196,10 +200,10 @@ struct SegTerms {
         C = D;
     }
 
-    // dT = dt / tloss of row r of a lane's block (swizzled index r * 33 + lane)
+    // dT = dt / tloss of row r of a lane's block (swizzled index r * kPitch + lane)
     __device__ __forceinline__ double row_dT(const double *tab, int r, int lane) const
     {
-        if (S == 0) return tab[TB_X4 * kTabStride + r * 33 + lane] * dt_over_tloss_pref;
+        if (S == 0) return tab[TB_X4 * kTabStride + r * kPitch + lane] * dt_over_tloss_pref;
         return dtT_e;
     }
 };
@@ -316,13 +320,13 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
 #pragma unroll
     for (int r = 0; r < kR; r++) {
         const int m = row0 + r;
-        const double k = T.dt * tab[TB_IDX * kTabStride + r * 33 + lane];
-        const double Cm = sm.C[r * 33 + lane], Bm = sm.B[r * 33 + lane], Dm = T.row_dT(tab, r, lane);
+        const double k = T.dt * tab[TB_IDX * kTabStride + r * kPitch + lane];
+        const double Cm = sm.C[r * kPitch + lane], Bm = sm.B[r * kPitch + lane], Dm = T.row_dT(tab, r, lane);
         double av = 0.0, bv, cv = 0.0;
         if (m == 0) {
             const double nC = sm.C[swz(1)], nB = sm.B[swz(1)];
             if (fabs(Cm) > 1.0e-200) {
-                const double cm12 = 0.5 * (Cm + nC) * tab[TB_IDXR * kTabStride + r * 33 + lane];
+                const double cm12 = 0.5 * (Cm + nC) * tab[TB_IDXR * kTabStride + r * kPitch + lane];
                 bv = 1.0 + k * (0.0 + cm12 * sm.Wm[swz(0)]) + Dm;
                 cv = k * cm12 * sm.Wp[swz(0)];
             } else {
@@ -334,7 +338,7 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
             const double wpm = sm.Wp[swz(m - 1)], wmm = sm.Wm[swz(m - 1)];
             if (m == NB - 1) {
                 if (fabs(Cm) > 1.0e-200) {
-                    const double cm_12 = 0.5 * (Cm + pC) * tab[TB_IDXL * kTabStride + r * 33 + lane];
+                    const double cm_12 = 0.5 * (Cm + pC) * tab[TB_IDXL * kTabStride + r * kPitch + lane];
                     av = k * cm_12 * wmm;
                     bv = 1.0 + k * (cm_12 * wpm) + Dm;
                     if (isnan(av)) err |= kErrCcNan;
@@ -348,8 +352,8 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
             } else {
                 const double nC = sm.C[swz(m + 1)], nB = sm.B[swz(m + 1)];
                 if (fabs(Cm) > 1.0e-200) {
-                    const double cm_12 = 0.5 * (Cm + pC) * tab[TB_IDXL * kTabStride + r * 33 + lane];
-                    const double cm12 = 0.5 * (Cm + nC) * tab[TB_IDXR * kTabStride + r * 33 + lane];
+                    const double cm_12 = 0.5 * (Cm + pC) * tab[TB_IDXL * kTabStride + r * kPitch + lane];
+                    const double cm12 = 0.5 * (Cm + nC) * tab[TB_IDXR * kTabStride + r * kPitch + lane];
                     av = k * cm_12 * wmm;
                     bv = 1.0 + k * (cm_12 * wpm + cm12 * sm.Wm[swz(m)]) + Dm;
                     cv = k * cm12 * sm.Wp[swz(m)];
