@@ -740,7 +740,9 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) steps_kernel
                 load_coef<SRC>(F, fac_ptr(P, S, gi, want, tl), src, g.dt, lane);
                 cur = want;
             }
-#pragma unroll 1
+            // two sub-steps per trip: the carried spectrum keeps its
+            // registers across the loop (fewer copies per sub-step)
+#pragma unroll 2
             for (int istep = 0; istep < run_n; istep++) substep<SRC>(F, N);
         }
     }
