@@ -280,14 +280,20 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
     const double *x = st.p;
     unsigned err = 0;
 
+    // Swizzled positions: for j = 32 k + lane, swz(j) = swz(lane) + k * 32 / R
+    // and swz(j + 1) = swz(lane + 1) + k * 32 / R; for row m = R lane + r of
+    // the lane's block, swz(m) = r * pitch + lane.
+    constexpr int kStep = 32 / kR;
+    const int sb0 = swz(lane), sb1 = swz(lane + 1);
+
     // terms, lane-strided
 #pragma unroll 2
     for (int k = 0; k < kR; k++) {
         const int j = k * 32 + lane;
         double B, C;
         T.at(tab, j, B, C);
-        sm.B[swz(j)] = B;
-        sm.C[swz(j)] = C;
+        sm.B[sb0 + k * kStep] = B;
+        sm.C[sb0 + k * kStep] = C;
     }
     __syncwarp();
     // faces j (between bins j and j+1), lane-strided.  The drift / diffusion
@@ -298,20 +304,21 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
 #pragma unroll 2
     for (int k = 0; k < kR; k++) {
         const int j = k * 32 + lane;
+        const int s0 = sb0 + k * kStep, s1 = sb1 + k * kStep;
         double wp = 0.0, wm = 0.0;
         if (j <= NB - 2) {
-            const double cl = sm.C[swz(j)];
+            const double cl = sm.C[s0];
             if (fabs(cl) > 1.0e-200) {
-                const double bsum = sm.B[swz(j)] + sm.B[swz(j + 1)];
+                const double bsum = sm.B[s0] + sm.B[s1];
                 const double rf = tab[TB_RF * kTabStride + j] * inv_kappa;
                 const double w = (T.dpp_fill && isfinite(rf))
                                      ? bsum * rf
-                                     : bsum / (cl + sm.C[swz(j + 1)]) * tab[TB_DXF * kTabStride + j];
+                                     : bsum / (cl + sm.C[s1]) * tab[TB_DXF * kTabStride + j];
                 face_weights_fast(w, wp, wm);
             }
         }
-        sm.Wp[swz(j)] = wp;
-        sm.Wm[swz(j)] = wm;
+        sm.Wp[s0] = wp;
+        sm.Wm[s0] = wm;
     }
     __syncwarp();
 
@@ -320,22 +327,25 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
 #pragma unroll
     for (int r = 0; r < kR; r++) {
         const int m = row0 + r;
+        const int sm_m = r * kPitch + lane;
+        const int sm_p = r > 0 ? (r - 1) * kPitch + lane : (kR - 1) * kPitch + lane - 1;   // swz(m - 1), m >= 1
+        const int sm_n = r < kR - 1 ? (r + 1) * kPitch + lane : lane + 1;                  // swz(m + 1)
         const double k = T.dt * tab[TB_IDX * kTabStride + r * kPitch + lane];
         const double Cm = sm.C[r * kPitch + lane], Bm = sm.B[r * kPitch + lane], Dm = T.row_dT(tab, r, lane);
         double av = 0.0, bv, cv = 0.0;
         if (m == 0) {
-            const double nC = sm.C[swz(1)], nB = sm.B[swz(1)];
+            const double nC = sm.C[sm_n], nB = sm.B[sm_n];
             if (fabs(Cm) > 1.0e-200) {
                 const double cm12 = 0.5 * (Cm + nC) * tab[TB_IDXR * kTabStride + r * kPitch + lane];
-                bv = 1.0 + k * (0.0 + cm12 * sm.Wm[swz(0)]) + Dm;
-                cv = k * cm12 * sm.Wp[swz(0)];
+                bv = 1.0 + k * (0.0 + cm12 * sm.Wm[sm_m]) + Dm;
+                cv = k * cm12 * sm.Wp[sm_m];
             } else {
                 bv = 1.0 + k * 0.0 + Dm;
                 cv = k * 1.0 * 0.5 * (Bm + nB);
             }
         } else {
-            const double pC = sm.C[swz(m - 1)], pB = sm.B[swz(m - 1)];
-            const double wpm = sm.Wp[swz(m - 1)], wmm = sm.Wm[swz(m - 1)];
+            const double pC = sm.C[sm_p], pB = sm.B[sm_p];
+            const double wpm = sm.Wp[sm_p], wmm = sm.Wm[sm_p];
             if (m == NB - 1) {
                 if (fabs(Cm) > 1.0e-200) {
                     const double cm_12 = 0.5 * (Cm + pC) * tab[TB_IDXL * kTabStride + r * kPitch + lane];
@@ -350,13 +360,13 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
                     bv = 1.0 + k * (0.5 * (pB + Bm)) + Dm;
                 }
             } else {
-                const double nC = sm.C[swz(m + 1)], nB = sm.B[swz(m + 1)];
+                const double nC = sm.C[sm_n], nB = sm.B[sm_n];
                 if (fabs(Cm) > 1.0e-200) {
                     const double cm_12 = 0.5 * (Cm + pC) * tab[TB_IDXL * kTabStride + r * kPitch + lane];
                     const double cm12 = 0.5 * (Cm + nC) * tab[TB_IDXR * kTabStride + r * kPitch + lane];
                     av = k * cm_12 * wmm;
-                    bv = 1.0 + k * (cm_12 * wpm + cm12 * sm.Wm[swz(m)]) + Dm;
-                    cv = k * cm12 * sm.Wp[swz(m)];
+                    bv = 1.0 + k * (cm_12 * wpm + cm12 * sm.Wm[sm_m]) + Dm;
+                    cv = k * cm12 * sm.Wp[sm_m];
                 } else {
                     // interior row below the diffusion floor: every delta the
                     // reference reads here is zero (Chang_Cooper.c:91-103)
