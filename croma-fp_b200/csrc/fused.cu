@@ -49,7 +49,9 @@ constexpr int kR = NB / 32;          // rows per lane
 // -- then touch 16 distinct 8-byte bank pairs per half warp.
 constexpr int kPitch = 32 + 16 / kR;
 constexpr int kSw = kPitch * kR;     // swizzled row-array length
-constexpr int kWarps = 4;            // warps per block
+// One warp per block in the steps kernels: a finished tracer's slot is
+// refilled at once instead of when the slowest warp of its block ends.
+constexpr int kWarps = 1;            // warps per block
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kFacDoubles = 3 * NB;  // 1/d, a/d, c/d of one system
 constexpr int kFacWarps = 8;         // warps per factor-kernel block
@@ -681,7 +683,7 @@ __device__ __forceinline__ void substep(const Coef<SRC> &F, double N[kR])
 // Steps kernel: warp w of block b runs every segment [g0, g1) of tracer
 // t0 + b * kWarps + w for species S.
 template <int S, bool SRC>
-__global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) steps_kernel(FusedParams P)
+__global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 16 : 8)) steps_kernel(FusedParams P)
 {
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -768,7 +770,7 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 4 : 2)) steps_kernel
 // with the pivots recomputed (tracer_fp_cpu_evolve, src/tracer_fp_cpu.c:149-190;
 // fp_thomas_solve_ws, src/fp_shared_core.c:226-257) and writes N back.
 template <int S, bool SRC>
-__global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 5 : 2)) plain_steps_kernel(FusedParams P)
+__global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 20 : 8)) plain_steps_kernel(FusedParams P)
 {
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
