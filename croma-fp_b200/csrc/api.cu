@@ -93,9 +93,10 @@ void free_state(Context &c)
     c.d_dis = nullptr;
     dev_free(c, c.d_inje); dev_free(c, c.d_eta_scale);
     c.d_inje = c.d_eta_scale = nullptr;
-    dev_free(c, c.d_fac); dev_free(c, c.d_np_seg); dev_free(c, c.d_segpre);
+    dev_free(c, c.d_fac); dev_free(c, c.d_np_seg); dev_free(c, c.d_segpre); dev_free(c, c.d_work);
     c.d_fac = c.d_np_seg = nullptr;
     c.d_segpre = nullptr;
+    c.d_work = nullptr;
     c.fused_chunk = c.fused_nseg = c.fused_sets = 0;
     dev_free(c, c.d_sched_int); dev_free(c, c.d_capped); dev_free(c, c.d_cub_tmp);
     dev_free(c, c.d_keys); dev_free(c, c.d_vals);

@@ -130,6 +130,7 @@ struct Context {
     double *d_fac = nullptr;
     double *d_np_seg = nullptr;
     void *d_segpre = nullptr;         // per-segment scalars [nseg][chunk] (fused.cu)
+    unsigned *d_work = nullptr;       // [2] factor-kernel work counters (fused.cu)
     int fused_chunk = 0, fused_nseg = 0, fused_sets = 0;
     double workspace_bytes = 0.0;     // fused workspace cap; 0 = CROMA_B200_WORKSPACE_GB or 24 GB
 

@@ -94,6 +94,7 @@ struct FusedParams {
     const double *eta_scale; // [ntracer] Dpp eta-cap scale of slot g0, or null (no cap)
     double *fac;             // [2 species][g1 - g0][sets][nt][3][nb]
     SegPre *pre;             // [g1 - g0][nt]
+    unsigned *work;          // [2] next-tracer counters of the factor kernels (per species)
     double *np_seg;          // [g1 - g0][nt][nb] proton spectra at segment starts, or null
     double *inje;            // [g1 - g0][nt][nb] electron source per segment, or null
     const int *np_min_qe;    // [nb]
@@ -512,11 +513,14 @@ __global__ void __launch_bounds__(kFacWarps * 32, (NB <= 256 ? 2 : 1)) factor_ke
     }
     __syncthreads();
     // a warp takes one tracer at a time and factors all its segments (and
-    // on/off sets) from the segments' precomputed scalars
+    // on/off sets) from the segments' precomputed scalars; after its first
+    // tracer it takes the next one not yet taken (a counter the host zeroes
+    // before the launch), so no warp is left with a whole extra tracer at the end
     const int stride = gridDim.x * kFacWarps;
     const int nslot = P.g1 - P.g0;
+    int tl = blockIdx.x * kFacWarps + w;
 #pragma unroll 1
-    for (int tl = blockIdx.x * kFacWarps + w; tl < P.nt; tl += stride) {
+    while (tl < P.nt) {
         const int t = P.t0 + tl;
         WarpSmem &ws = smem[w];
         const double eta = (P.mp.dpp_model != kDppOff && P.eta_scale) ? P.eta_scale[t] : 1.0;
@@ -548,6 +552,9 @@ __global__ void __launch_bounds__(kFacWarps * 32, (NB <= 256 ? 2 : 1)) factor_ke
                 __syncwarp();
             }
         }
+        unsigned next = 0;
+        if (lane == 0) next = atomicAdd(P.work + S, 1u);
+        tl = stride + (int)__shfl_sync(kFull, next, 0);
     }
 }
 
@@ -1063,6 +1070,8 @@ cudaError_t launch_factor(Context &ctx, const FusedParams &P)
     const long long full = (long long)nsm * resident;
     if (blocks > full) blocks = full;
     if (blocks < 1) return cudaSuccess;
+    const cudaError_t ez = cudaMemsetAsync(P.work + S, 0, sizeof(unsigned), ctx.stream);
+    if (ez != cudaSuccess) return ez;
     factor_kernel<S, ROWS><<<(unsigned)blocks, kFacWarps * 32, smem, ctx.stream>>>(P);
     return cudaGetLastError();
 }
@@ -1135,8 +1144,10 @@ int fused_reserve(Context &ctx, int cap)
     dev_free(ctx, ctx.d_fac);
     dev_free(ctx, ctx.d_np_seg);
     dev_free(ctx, ctx.d_segpre);
+    dev_free(ctx, ctx.d_work);
     ctx.d_inje = ctx.d_eta_scale = ctx.d_fac = ctx.d_np_seg = nullptr;
     ctx.d_segpre = nullptr;
+    ctx.d_work = nullptr;
     ctx.fused_chunk = ctx.fused_nseg = ctx.fused_sets = 0;
     const size_t rows = (size_t)nseg * chunk * NB;
     CROMA_CUDA(dev_alloc(ctx, &ctx.d_fac, (size_t)2 * sets * rows * 3 * sizeof(double)));
@@ -1144,6 +1155,7 @@ int fused_reserve(Context &ctx, int cap)
     CROMA_CUDA(dev_alloc(ctx, &ctx.d_inje, rows * sizeof(double)));
     CROMA_CUDA(dev_alloc(ctx, &ctx.d_eta_scale, (size_t)cap * sizeof(double)));
     CROMA_CUDA(dev_alloc(ctx, &ctx.d_segpre, (size_t)nseg * chunk * sizeof(SegPre)));
+    CROMA_CUDA(dev_alloc(ctx, &ctx.d_work, 2 * sizeof(unsigned)));
     ctx.fused_chunk = (int)chunk;
     ctx.fused_nseg = nseg;
     ctx.fused_sets = sets;
@@ -1267,6 +1279,7 @@ static int fused_chunks(Context &ctx, FusedParams &P, int nslots, bool perstep)
     P.sets = ctx.fused_sets;
     P.fac = ctx.d_fac;
     P.pre = static_cast<SegPre *>(ctx.d_segpre);
+    P.work = ctx.d_work;
     // chunks: the workspace's uniform split, or the host pipeline's bounds
     // (each within the workspace chunk), whose uploads gate the chunk and
     // whose downloads follow it

@@ -561,6 +561,7 @@ void cuda_pipeline_workspace_destroy(FpCudaPipelineWorkspace *w)
     dev_free(c, c.d_fac);
     dev_free(c, c.d_np_seg);
     dev_free(c, c.d_segpre);
+    dev_free(c, c.d_work);
     dev_free(c, c.d_tables);
     dev_free(c, c.d_np_min_qe);
     if (c.stream) cudaStreamSynchronize(c.stream);
