@@ -154,10 +154,12 @@ def cpu_reference_rate(cfg, budget_s=12.0, max_tracers=NTRACER):
         bgc = w.background(isnap)[:, :n].copy()
         bgn = w.background(isnap + 1)[:, :n].copy()
         crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), n, cfg.species)
+        crp0, cre0 = crp.copy(), cre.copy()
         q = np.zeros_like(crp)
         t0 = time.perf_counter()
-        impl.snapshot(bgc, bgn, float(w.z[isnap]), float(w.z[isnap + 1]), True, float(w.dt[isnap]),
-                      float(w.elapsed[isnap]), q, np.zeros_like(cre), crp, cre, mass=w.mass[:n])
+        nsub, _, _, _ = impl.snapshot(bgc, bgn, float(w.z[isnap]), float(w.z[isnap + 1]), True,
+                                      float(w.dt[isnap]), float(w.elapsed[isnap]), q, np.zeros_like(cre), crp,
+                                      cre, mass=w.mass[:n])
         dt = time.perf_counter() - t0
         spent += dt
         if dt >= budget_s / 4 or n >= max_tracers or spent > budget_s:
@@ -165,9 +167,47 @@ def cpu_reference_rate(cfg, budget_s=12.0, max_tracers=NTRACER):
         n *= 2
     per_tracer = max(dt - t_ic, 1e-9) / n
     t_full = t_ic + per_tracer * max_tracers
+    check = {"w": w, "isnap": isnap, "bgc": bgc, "bgn": bgn, "crp0": crp0, "cre0": cre0, "crp": crp,
+             "cre": cre, "nsub": nsub, "dp": (gp[1], ge[1]), "kind": kind}
     return {"value": max_tracers / t_full, "unit": UNIT, "cores": cores, "kind": kind,
             "sample": f"1 snapshot x {n} tracers in {dt:.2f} s (IC rows {t_ic:.2f} s/snapshot), "
-                      f"extrapolated to {max_tracers} tracers per snapshot"}, dt, n
+                      f"extrapolated to {max_tracers} tracers per snapshot"}, dt, n, check
+
+
+def accuracy_vs_reference(cfg, path, chk):
+    """The GPU path on the CPU baseline's own sample (same tracers, inputs and
+    snapshot) against the reference CPU's result: max and median relative
+    error per bin (bins above 1e-12 of each tracer's peak), the largest
+    particle-number drift |sum N dp - ref| / ref per tracer and species, and
+    the nsub mismatches (which must be 0)."""
+    load_package()
+    from croma_fp_b200 import native
+    w, isnap = chk["w"], chk["isnap"]
+    n = chk["crp0"].shape[0]
+    fp = native.TracerFP(cfg, path=path)
+    try:
+        fp.set_state(chk["crp0"], chk["cre0"], mass=w.mass[:n])
+        fp.snapshot(chk["bgc"], chk["bgn"], float(w.z[isnap]), float(w.z[isnap + 1]), True, float(w.dt[isnap]),
+                    float(w.elapsed[isnap]), sync=True)
+        g_crp, g_cre = fp.get_state()
+        g_nsub = fp.schedule()["nsub"]
+    finally:
+        fp.close()
+    rels, drift = [], 0.0
+    for g, r, dp in ((g_crp, chk["crp"], chk["dp"][0]), (g_cre, chk["cre"], chk["dp"][1])):
+        peak = np.max(np.abs(r), axis=1, keepdims=True)
+        m = np.abs(r) > 1e-12 * peak
+        if m.any():
+            rels.append((np.abs(g - r)[m] / np.abs(r)[m]))
+        ng, nr = g @ dp, r @ dp
+        ok = nr != 0
+        if ok.any():
+            drift = max(drift, float(np.max(np.abs(ng[ok] - nr[ok]) / np.abs(nr[ok]))))
+    rel = np.concatenate(rels) if rels else np.zeros(1)
+    return {"vs": f"reference CPU ({chk['kind']}) on the CPU baseline's sample", "tracers": n,
+            "max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
+            "max_particle_number_drift": drift, "nsub_mismatches": int(np.sum(g_nsub != chk["nsub"])),
+            "bar": 1e-6}
 
 
 def run_reference_arm(args):
@@ -178,7 +218,7 @@ def run_reference_arm(args):
     vals = []
     first = None
     for _ in range(args.warmup + args.steps):
-        res, dt, n = cpu_reference_rate(cfg, budget_s=max(2.0, 60.0 / max(1, args.steps + args.warmup)))
+        res, dt, n, _ = cpu_reference_rate(cfg, budget_s=max(2.0, 60.0 / max(1, args.steps + args.warmup)))
         vals.append(res["value"])
         first = first or res
     timed = vals[args.warmup:] or vals
@@ -419,12 +459,18 @@ def run_gpu_arm(args):
         from croma_fp_b200 import serve_bench
         serving = serve_bench.run(nrequests=args.serving_requests)
     cpu = None
+    accuracy = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu, _, _ = cpu_reference_rate(cfg, budget_s=args.cpu_budget)
+            cpu, _, _, chk = cpu_reference_rate(cfg, budget_s=args.cpu_budget)
         except Exception as e:  # the checker library may be absent
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "unavailable",
                    "sample": f"{type(e).__name__}: {e}"}
+        else:
+            try:
+                accuracy = accuracy_vs_reference(cfg, args.path, chk)
+            except (RuntimeError, ValueError) as e:  # native.CromaError is a RuntimeError
+                accuracy = {"error": f"{type(e).__name__}: {e}"}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -438,6 +484,7 @@ def run_gpu_arm(args):
                                    "api": "croma_b200_set_state/snapshot/get_state in turn"}},
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "accuracy": accuracy,
             "serving": serving,
             "clocks": clocks.summary(),
             "gpu_launches": int(launches),
