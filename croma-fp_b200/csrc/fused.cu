@@ -304,22 +304,25 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
     // sum is kappa times a grid factor, so the division becomes a product with
     // the tabulated dx / (g_j + g_j+1) and 1 / kappa (equal to a few ulp).
     const double inv_kappa = T.dpp_fill ? 1.0 / (T.dpp_inv * T.dpp_scale) : 0.0;
+    // The division form is taken only when a lane of the warp needs it (the
+    // vote keeps it from being computed predicated on every face).  Face
+    // nb - 1 does not exist: its position swz(nb) is a padding word, read but
+    // never used.
 #pragma unroll 2
     for (int k = 0; k < kR; k++) {
         const int j = k * 32 + lane;
         const int s0 = sb0 + k * kStep, s1 = sb1 + k * kStep;
         double wp = 0.0, wm = 0.0;
-        if (j <= NB - 2) {
-            const double cl = sm.C[s0];
-            if (fabs(cl) > 1.0e-200) {
-                const double bsum = sm.B[s0] + sm.B[s1];
-                const double rf = tab[TB_RF * kTabStride + j] * inv_kappa;
-                const double w = (T.dpp_fill && isfinite(rf))
-                                     ? bsum * rf
-                                     : bsum / (cl + sm.C[s1]) * tab[TB_DXF * kTabStride + j];
-                face_weights_fast(w, wp, wm);
-            }
+        const double cl = sm.C[s0];
+        const bool live = (j <= NB - 2) && fabs(cl) > 1.0e-200;
+        const double bsum = sm.B[s0] + sm.B[s1];
+        const double rf = tab[TB_RF * kTabStride + j] * inv_kappa;
+        const bool divide = live && !(T.dpp_fill && isfinite(rf));
+        double w = bsum * rf;
+        if (__any_sync(kFull, divide)) {
+            if (divide) w = bsum / (cl + sm.C[s1]) * tab[TB_DXF * kTabStride + j];
         }
+        if (live) face_weights_fast(w, wp, wm);
         sm.Wp[s0] = wp;
         sm.Wm[s0] = wm;
     }
@@ -392,7 +395,9 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
 // src/fp_shared_core.c:226-257).  The chain of Moebius maps d -> b - e/d is
 // composed per lane as 2x2 matrices and combined by a warp scan, after which
 // each lane re-runs the exact recurrence on its rows from the scanned
-// incoming pivot.
+// incoming pivot.  The lane's own matrix is rescaled to a largest entry in
+// [1, 2); the scan's products then stay below 2^63 over its five levels, so
+// they are not rescaled (powers of two are exact either way: same pivots).
 __device__ __forceinline__ unsigned pivot_rows(double A[kR], double Bd[kR], double Cc[kR], int lane)
 {
     unsigned err = 0;
@@ -420,7 +425,6 @@ __device__ __forceinline__ unsigned pivot_rows(double A[kR], double Bd[kR], doub
             const double n00 = t00 * u00 + t01 * u10, n01 = t00 * u01 + t01 * u11;
             const double n10 = t10 * u00 + t11 * u10, n11 = t10 * u01 + t11 * u11;
             t00 = n00; t01 = n01; t10 = n10; t11 = n11;
-            rescale2(t00, t01, t10, t11);
         }
     }
     double vp = sup(t00, 1), vq = sup(t10, 1);
