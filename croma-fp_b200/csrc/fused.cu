@@ -54,7 +54,9 @@ constexpr int kSw = kPitch * kR;     // swizzled row-array length
 constexpr int kWarps = 1;            // warps per block
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kFacDoubles = 3 * NB;  // 1/d, a/d, c/d of one system
-constexpr int kFacWarps = 8;         // warps per factor-kernel block
+// warps per factor-kernel block: at nb = 256 two 9-warp blocks (106 KB of
+// shared memory each, at most 113 registers a thread) fill an SM
+constexpr int kFacWarps = 9;
 
 // Grid tables of one species staged in shared memory by the factor kernel.
 // X0..X3: protons expE, cp_Ep, cp_inv2mpkin, cp_inv_betap2; electrons
