@@ -40,7 +40,7 @@ UNIT = "tracer-snapshot updates/s"
 # proton and electron launches of an ncu capture of this workload at 32,768
 # tracers (profiles/steps_factor_secondary_batching_e_p_256.txt); traffic
 # scales with the tracer count (every tracer moves its own rows).
-NCU_DRAM_BYTES_PER_TRACER_STEPS_LAUNCH = (3.348338e9 + 1.122072e9 + 4.433178e9 + 0.076386e9) / 2 / 32768
+NCU_DRAM_BYTES_PER_TRACER_STEPS_LAUNCH = (3.347485e9 + 1.122321e9 + 4.431413e9 + 0.077046e9) / 2 / 32768
 # plain_steps_kernel DRAM read + write per tracer per launch (one segment slot
 # of 31.25 sub-steps), mean of the proton and electron launches, from one ncu
 # capture at 32,768 tracers of the same workload
