@@ -75,6 +75,16 @@ def workload_desc(ntracer):
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clock and throttle reasons of one GPU while it runs the timed
+    region: polled in-process through NVML every few milliseconds (the device
+    matched by PCI bus id), else read from an `nvidia-smi -lms 50` child."""
+
+    NVML_POLL_S = 0.005
+    NVML_REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+                    ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+                    ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+                    ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
+
     def __init__(self, device_index=0):
         self.samples = []
         self.reasons = set()
@@ -82,8 +92,42 @@ class ClockSampler:
         self._stop = threading.Event()
         self.dev = device_index
         self.proc = None
+        self.t = None
+        self.nvml = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            try:
+                pr = torch.cuda.get_device_properties(device_index)
+                bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.nvml = (pynvml, h)
+        except Exception:
+            self.nvml = None
+
+    def _poll(self):
+        pynvml, h = self.nvml
+        bits = [(n, getattr(pynvml, c, 0)) for n, c in self.NVML_REASONS]
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for n, bit in bits:
+                    if bit and (r & bit):
+                        self.reasons.add(n)
+            except Exception:
+                pass
+            self._stop.wait(self.NVML_POLL_S)
 
     def start(self):
+        if self.nvml:
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -113,6 +157,11 @@ class ClockSampler:
                     self.reasons.add(n)
 
     def stop(self):
+        if self.nvml:
+            self._stop.set()
+            if self.t:
+                self.t.join(timeout=5)
+            return
         if self.proc:
             self.proc.terminate()
             try:
@@ -124,7 +173,8 @@ class ClockSampler:
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
         return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
-                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+                "reasons": sorted(self.reasons), "samples": len(self.samples),
+                "source": "nvml" if self.nvml else "nvidia-smi"}
 
 
 # ---------------------------------------------------------------- CPU baseline
