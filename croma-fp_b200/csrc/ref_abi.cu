@@ -22,6 +22,7 @@
 // croma_b200_set_model() otherwise.
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -379,13 +380,9 @@ struct Scratch {
     }
 };
 
-int emission_hadronic(int ncell, int nbins, double emin, double emax, const double *crp_batch,
-                      const double *n_gas, const double *beta_p, const double *kern,
-                      const CRspectrum *grid, double *out, double *elapsed_ms)
+// Band energies as the reference accumulates them (fp_shared_core.c:2178-2188).
+std::vector<double> hadronic_energies(int nbins, double emin, double emax)
 {
-    if (ncell <= 0 || nbins <= 0 || !crp_batch || !n_gas || !beta_p || !kern || !grid || !out)
-        return fail(-1, "invalid emission arguments");
-    // E grid as the reference accumulates it (fp_shared_core.c:2178-2188)
     std::vector<double> E(nbins);
     const double d = (emax - emin) / (double)nbins;
     double a = emin - d;
@@ -393,6 +390,16 @@ int emission_hadronic(int ncell, int nbins, double emin, double emax, const doub
         a += d;
         E[i] = pow(10.0, a);
     }
+    return E;
+}
+
+int emission_hadronic(int ncell, int nbins, double emin, double emax, const double *crp_batch,
+                      const double *n_gas, const double *beta_p, const double *kern,
+                      const CRspectrum *grid, double *out, double *elapsed_ms)
+{
+    if (ncell <= 0 || nbins <= 0 || !crp_batch || !n_gas || !beta_p || !kern || !grid || !out)
+        return fail(-1, "invalid emission arguments");
+    const std::vector<double> E = hadronic_energies(nbins, emin, emax);
     Scratch s;
     double *d_crp, *d_n, *d_bp, *d_dp, *d_k, *d_E, *d_out;
     CROMA_CUDA(s.get((void **)&d_crp, (size_t)ncell * NB * sizeof(double)));
@@ -1021,3 +1028,131 @@ int synch_emission_theta(const FpSynchEmissionBatchInput *in, const CRspectrum *
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Emissivities of a native context's resident spectra (include/croma_b200.h).
+// The same kernels as the reference-ABI entry points above, reading the
+// spectra where the snapshots left them: only the kernel tables and per-cell
+// inputs go up and the emissivities come back.
+
+struct CromaB200Context {
+    croma::Context impl;
+};
+
+namespace {
+
+struct HostIn {
+    const void *src;
+    size_t bytes;
+};
+
+// One emission call on the context stream: uploads ins into one
+// stream-ordered device block, launch(inputs, spectra, dp, out, ncell,
+// stream), then the [ntracer][ncols] emissivities to out.
+template <class Launch>
+int ctx_emission(CromaB200Context *h, int species, int ncols, std::initializer_list<HostIn> ins, double *out,
+                 double *elapsed_ms, Launch launch)
+{
+    if (!h || ncols <= 0 || !out) return fail(-1, "invalid emission arguments");
+    Context &c = h->impl;
+    const double *spec = species ? c.d_cre : c.d_crp;
+    if (c.ntracer <= 0 || !spec) return fail(-1, "no resident spectra: call croma_b200_set_state first");
+    if (!(c.mp.species_mask & (species ? CROMA_SPECIES_ELECTRON : CROMA_SPECIES_PROTON)))
+        return fail(-1, "emission of a species this context does not evolve");
+    for (const HostIn &in : ins)
+        if (!in.src || in.bytes == 0) return fail(-1, "missing emission input");
+    CROMA_CUDA(cudaSetDevice(c.device));
+    const int ncell = c.ntracer;
+    auto align = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t out_bytes = (size_t)ncell * ncols * sizeof(double);
+    size_t total = align(out_bytes);
+    for (const HostIn &in : ins) total += align(in.bytes);
+    struct Block {
+        Context &c;
+        void *p = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ~Block()
+        {
+            if (p) dev_free(c, p);
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } blk{c};
+    CROMA_CUDA(dev_alloc_bytes(c, &blk.p, total));
+    CROMA_CUDA(cudaEventCreate(&blk.e0));
+    CROMA_CUDA(cudaEventCreate(&blk.e1));
+    CROMA_CUDA(cudaEventRecord(blk.e0, c.stream));
+    char *p = static_cast<char *>(blk.p);
+    double *d_out = reinterpret_cast<double *>(p);
+    p += align(out_bytes);
+    std::vector<const double *> d_in;
+    for (const HostIn &in : ins) {
+        CROMA_CUDA(cudaMemcpyAsync(p, in.src, in.bytes, cudaMemcpyHostToDevice, c.stream));
+        d_in.push_back(reinterpret_cast<const double *>(p));
+        p += align(in.bytes);
+    }
+    launch(d_in, spec, c.gt.s[species].dp, d_out, ncell, c.stream);
+    CROMA_CUDA(cudaGetLastError());
+    CROMA_CUDA(cudaMemcpyAsync(out, d_out, out_bytes, cudaMemcpyDeviceToHost, c.stream));
+    CROMA_CUDA(cudaEventRecord(blk.e1, c.stream));
+    CROMA_CUDA(cudaEventSynchronize(blk.e1));
+    if (elapsed_ms) *elapsed_ms = elapsed(blk.e0, blk.e1);
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int croma_b200_emission_ic(CromaB200Context *ctx, int nbands, const double *fic, double *eps_out,
+                           double *elapsed_ms)
+{
+    return ctx_emission(ctx, 1, nbands, {{fic, (size_t)nbands * NB * sizeof(double)}}, eps_out, elapsed_ms,
+                        [&](const std::vector<const double *> &in, const double *cre, const double *dp,
+                            double *out, int ncell, cudaStream_t st) {
+                            dim3 blk(32, 4), grd((ncell + 31) / 32, (nbands + 3) / 4);
+                            ic_emission_kernel<<<grd, blk, 0, st>>>(ncell, nbands, cre, in[0], dp, out);
+                        });
+}
+
+int croma_b200_emission_hadronic(CromaB200Context *ctx, int nbins, double e_min, double e_max,
+                                 const double *n_gas, const double *beta_p, const double *kernel,
+                                 double *eps_out, double *elapsed_ms)
+{
+    if (!ctx || nbins <= 0) return fail(-1, "invalid emission arguments");
+    const std::vector<double> E = hadronic_energies(nbins, e_min, e_max);
+    const size_t ncell = (size_t)(ctx->impl.ntracer > 0 ? ctx->impl.ntracer : 0);
+    return ctx_emission(ctx, 0, nbins,
+                        {{n_gas, ncell * sizeof(double)}, {beta_p, NB * sizeof(double)},
+                         {kernel, (size_t)nbins * NB * sizeof(double)}, {E.data(), (size_t)nbins * sizeof(double)}},
+                        eps_out, elapsed_ms,
+                        [&](const std::vector<const double *> &in, const double *crp, const double *dp,
+                            double *out, int nc, cudaStream_t st) {
+                            dim3 blk(32, 4), grd((nc + 31) / 32, (nbins + 3) / 4);
+                            hadronic_emission_kernel<<<grd, blk, 0, st>>>(nc, nbins, crp, in[0], in[1], dp, in[2],
+                                                                           in[3], out);
+                        });
+}
+
+int croma_b200_emission_synch(CromaB200Context *ctx, int nfreq, int nlogb, double logb_min, double inv_dlogb,
+                              const double *table, const double *b_dyn, const double *logb, double *eps_out,
+                              double *elapsed_ms)
+{
+    if (!ctx || nfreq <= 0) return fail(-1, "invalid emission arguments");
+    if (nlogb <= 1 || !(inv_dlogb > 0.0)) return fail(-1, "synchrotron emission needs a pitch-kernel table");
+    const size_t ncell = (size_t)(ctx->impl.ntracer > 0 ? ctx->impl.ntracer : 0);
+    const double a0 = sqrt(3.0) * pow(4.8e-10, 3.0);
+    const double den1 = 2.0 * 9.11e-28 * kC * kC, den2 = 4.0 * kPi;
+    return ctx_emission(ctx, 1, nfreq,
+                        {{table, (size_t)nlogb * nfreq * NB * sizeof(double)}, {b_dyn, ncell * sizeof(double)},
+                         {logb, ncell * sizeof(double)}},
+                        eps_out, elapsed_ms,
+                        [&](const std::vector<const double *> &in, const double *cre, const double *dp,
+                            double *out, int nc, cudaStream_t st) {
+                            dim3 blk(32, 4), grd((nc + 31) / 32, (nfreq + 3) / 4);
+                            synch_table_kernel<<<grd, blk, 0, st>>>(nc, nfreq, nlogb, logb_min, inv_dlogb, a0, den1,
+                                                                    den2, in[0], in[1], in[2], cre, dp, out);
+                        });
+}
+
+}  // extern "C"

@@ -10,8 +10,11 @@ contract is the reference's: host arrays in, host arrays out, so each call
 copies the spectra to the device and the emissivities back.  Reported per
 entry point: the call's own elapsed time (device events around copies and
 kernel), the bytes it moves between host and device, and those bytes over
-that time.  Inputs are seeded synthetic spectra, backgrounds and kernel
-tables of the reference's shapes.
+that time.  `resident` times the same integrals through the native
+context (croma_b200_emission_ic / _hadronic / _synch) on spectra already on
+the device: only the tables, per-cell inputs and emissivities move.  Inputs
+are seeded synthetic spectra, backgrounds and kernel tables of the
+reference's shapes.
 
     python croma-fp_b200/emission_bench.py [--cells 65536] [--calls 5]
 """
@@ -48,7 +51,6 @@ def run(ncell=65536, calls=5, seed=11):
     nb = cfg.nb
     fp = native.TracerFP(cfg, path="fused")
     gp, ge = fp.grid(0), fp.grid(1)
-    fp.close()
     crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), ncell, cfg.species)
     w = synth.Workload(cfg, ncell, 100, seed=seed)
     bg = w.background(20)
@@ -107,7 +109,28 @@ def run(ncell=65536, calls=5, seed=11):
         C.byref(sin), C.byref(cg_e), ref_abi.dptr(out_s), ms),
         spec_bytes + table.nbytes + b_dyn.nbytes + logb.nbytes + out_s.nbytes)
 
+    # the same integrals on spectra already resident in a context
+    fp.set_state(crp, cre, mass=w.mass)
+
+    def resident(name, call, bytes_moved):
+        call()
+        t = [call()[1] for _ in range(calls)]
+        med = statistics.median(t)
+        return {"ms_per_call": round(med, 3), "host_device_bytes": bytes_moved,
+                "cells_per_s": round(ncell / (med / 1e3)),
+                "speedup_vs_reference_contract": round(res[name]["ms_per_call"] / med, 1)}
+
+    nb_b = ncell * 8
+    resident_res = {
+        "ic": resident("ic", lambda: fp.emission_ic(fic), fic.nbytes + out_ic.nbytes),
+        "gamma": resident("gamma", lambda: fp.emission_hadronic(kern, n_gas, beta_p, -1.0, 3.0),
+                          nb_b + beta_p.nbytes + kern.nbytes + out_h.nbytes),
+        "synch_table": resident("synch_table", lambda: fp.emission_synch(table, b_dyn, logb, -9.0, nlogb / 5.0),
+                                table.nbytes + 2 * nb_b + out_s.nbytes),
+    }
+    fp.close()
     return {"metric": "emission entry points, host buffers in and out (reference contract)",
+            "resident": resident_res,
             "cells": ncell, "bins_per_species": nb, "bands": nband, "synch_frequencies": nfreq,
             "synch_logb_rows": nlogb, "calls": calls, "host_buffers": "pageable (numpy)",
             "data": "synthetic (seeded)", "results": res}

@@ -78,6 +78,9 @@ def load_library(nb: int) -> C.CDLL:
     L.croma_b200_set_state_broadcast.argtypes = [_vp, _i, _vp, _vp, _d]
     L.croma_b200_set_dsa.argtypes = [_vp, P(CromaB200DsaParams)]
     L.croma_b200_dsa_inject.argtypes = [_vp, P(CromaB200Shocks), _d, _d, _i, _i, P(_i)]
+    L.croma_b200_emission_ic.argtypes = [_vp, _i, _vp, _vp, P(_d)]
+    L.croma_b200_emission_hadronic.argtypes = [_vp, _i, _d, _d, _vp, _vp, _vp, _vp, P(_d)]
+    L.croma_b200_emission_synch.argtypes = [_vp, _i, _i, _d, _d, _vp, _vp, _vp, _vp, P(_d)]
     _LIBS[nb] = L
     return L
 
@@ -287,6 +290,43 @@ class TracerFP:
 
     def last_launch_count(self) -> int:
         return self.lib.croma_b200_last_launch_count(self.h)
+
+    # -- emissivities of the resident spectra ---------------------------
+    def emission_ic(self, fic):
+        """IC emissivity [ntracer][nbands] of the resident electron spectra;
+        fic [nbands][nb].  Returns (eps, device ms)."""
+        f = _c(fic)
+        if f.ndim != 2 or f.shape[1] != self.nb:
+            raise ValueError("fic must be [nbands][nb]")
+        eps, ms = np.empty((self.ntracer, f.shape[0])), _d()
+        self._check(self.lib.croma_b200_emission_ic(self.h, f.shape[0], _p(f), _p(eps), C.byref(ms)))
+        return eps, ms.value
+
+    def emission_hadronic(self, kernel, n_gas, beta_p, e_min, e_max):
+        """Gamma or neutrino emissivity [ntracer][nbins] of the resident
+        proton spectra (kernel [nbins][nb] chooses which).  Returns (eps, ms)."""
+        k, n, b = _c(kernel), _c(n_gas), _c(beta_p)
+        if k.ndim != 2 or k.shape[1] != self.nb:
+            raise ValueError("kernel must be [nbins][nb]")
+        if n.shape != (self.ntracer,) or b.shape != (self.nb,):
+            raise ValueError("n_gas must be [ntracer] and beta_p [nb]")
+        eps, ms = np.empty((self.ntracer, k.shape[0])), _d()
+        self._check(self.lib.croma_b200_emission_hadronic(self.h, k.shape[0], e_min, e_max, _p(n), _p(b), _p(k),
+                                                          _p(eps), C.byref(ms)))
+        return eps, ms.value
+
+    def emission_synch(self, table, b_dyn, logb, logb_min, inv_dlogb):
+        """Synchrotron emissivity [ntracer][nfreq] of the resident electron
+        spectra through the pitch-kernel table [nlogb][nfreq][nb]."""
+        t, bd, lb = _c(table), _c(b_dyn), _c(logb)
+        if t.ndim != 3 or t.shape[2] != self.nb:
+            raise ValueError("table must be [nlogb][nfreq][nb]")
+        if bd.shape != (self.ntracer,) or lb.shape != (self.ntracer,):
+            raise ValueError("b_dyn and logb must be [ntracer]")
+        eps, ms = np.empty((self.ntracer, t.shape[1])), _d()
+        self._check(self.lib.croma_b200_emission_synch(self.h, t.shape[1], t.shape[0], logb_min, inv_dlogb, _p(t),
+                                                       _p(bd), _p(lb), _p(eps), C.byref(ms)))
+        return eps, ms.value
 
     KERNEL_KINDS = {"evolve": 0, "coeff": 1, "secondary": 2}
 

@@ -208,6 +208,40 @@ int croma_b200_set_dsa(CromaB200Context *ctx, const CromaB200DsaParams *params);
 int croma_b200_dsa_inject(CromaB200Context *ctx, const CromaB200Shocks *shocks, double density_unit,
                           double dt_gyr, int mode, int reacc_mode, int *ninjected);
 
+/* ---- Emissivities of the resident spectra ----
+ * The per-snapshot emission integrals of the reference ABI
+ * (prepare_ic_emission_cuda_batch, prepare_gamma/neutrino_emission_cuda_batch,
+ * prepare_synch_emission_cuda_batch with a pitch-kernel table; include/
+ * fp_cuda_backend.h:97-110 of the reference) computed on the spectra the
+ * context already holds on the device, one row per tracer in the context's
+ * tracer order, with the same kernels and results bit for bit.  Only the
+ * kernel tables and per-tracer inputs (host arrays) go to the device and the
+ * emissivities (host arrays [ntracer][ncols]) come back: the spectra
+ * themselves do not cross PCIe.  Synchronous; *elapsed_ms (may be NULL)
+ * receives the device time of the call, copies included.  Errors: -1 invalid
+ * (no resident state, a species the context does not evolve, missing
+ * inputs), -3 CUDA. */
+
+/* eps[t][band] = sum_je fic[band][je] N_e[t][je] dp_e[je]; fic [nbands][nb]. */
+int croma_b200_emission_ic(CromaB200Context *ctx, int nbands, const double *fic, double *eps_out,
+                           double *elapsed_ms);
+
+/* Hadronic gamma or neutrino emission of the proton spectra:
+ * eps[t][bin] = E_bin n_gas[t] 1/2 sum_i (f_{i-1} + f_i) dp_i,
+ * f_i = beta_p[i] N_p[t][i] kernel[bin][i], E_bin log-spaced over
+ * [e_min, e_max] as the reference accumulates it; kernel is the gamma or the
+ * neutrino table [nbins][nb]; n_gas [ntracer], beta_p [nb]. */
+int croma_b200_emission_hadronic(CromaB200Context *ctx, int nbins, double e_min, double e_max,
+                                 const double *n_gas, const double *beta_p, const double *kernel,
+                                 double *eps_out, double *elapsed_ms);
+
+/* Synchrotron emission of the electron spectra through the pitch-kernel
+ * table [nlogb][nfreq][nb] (log-K interpolation in log B, nlogb > 1,
+ * inv_dlogb > 0); b_dyn and logb [ntracer]. */
+int croma_b200_emission_synch(CromaB200Context *ctx, int nfreq, int nlogb, double logb_min, double inv_dlogb,
+                              const double *table, const double *b_dyn, const double *logb, double *eps_out,
+                              double *elapsed_ms);
+
 /* FP64 FMA throughput of the current device, measured by a kernel of
  * independent fused multiply-add chains on every SM (TFLOP/s, FMA = 2 flops);
  * the denominator of the fused evolve's roofline. */
