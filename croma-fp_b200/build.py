@@ -22,7 +22,7 @@ LIBDIR = os.path.join(HERE, "lib")
 OBJROOT = os.path.join(HERE, "_build")
 NBS = (128, 256, 512)
 SOURCES = ("api.cu", "tables.cu", "schedule.cu", "fused.cu", "dsa.cu", "serve.cu",
-           "ref_abi.cu", "noalloc.cu", "output.cu")
+           "ref_abi.cu", "noalloc.cu", "output.cu", "emission.cu")
 NO_FMAD = {"schedule.cu"}
 
 

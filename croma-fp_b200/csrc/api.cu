@@ -225,6 +225,7 @@ void croma_b200_destroy(CromaB200Context *h)
     dev_free(c, c.d_err);
     free_ic_stage(c);
     free_dsa(c);
+    free_emission(c);
     for (auto e : c.pipe_up) cudaEventDestroy(e);
     for (auto e : c.pipe_done) cudaEventDestroy(e);
     for (auto e : c.pipe_done_p) cudaEventDestroy(e);
@@ -542,6 +543,111 @@ int croma_b200_snapshot_host(CromaB200Context *h, const CromaB200Snapshot *s, in
     return check_err(c);
 }
 
+int croma_b200_step_host(CromaB200Context *h, const CromaB200Snapshot *s, const CromaB200StepHost *io)
+{
+    if (!h || !s || !s->bg_curr || !io || s->bg_on_device) {
+        set_error("invalid step_host arguments (host backgrounds required)");
+        return -1;
+    }
+    Context &c = h->impl;
+    CROMA_CUDA(cudaSetDevice(c.device));
+    if (c.cap <= 0 || c.ntracer != c.cap) { set_error("set_state or reserve before step_host"); return -1; }
+    if (c.fused_chunk <= 0) { set_error("fused workspace not reserved"); return -1; }
+    const size_t n = (size_t)c.cap;
+    const bool want_emis = io->eps_syn || io->eps_ic || io->eps_gamma || io->eps_nu;
+    if (want_emis && !c.emission) { set_error("emission outputs requested without croma_b200_emission_setup"); return -1; }
+    if (!c.h2d_stream) CROMA_CUDA(cudaStreamCreateWithFlags(&c.h2d_stream, cudaStreamNonBlocking));
+    if (!c.d2h_stream) CROMA_CUDA(cudaStreamCreateWithFlags(&c.d2h_stream, cudaStreamNonBlocking));
+    // 1. the snapshot's backgrounds into the staging block (both slots)
+    const int allow = s->allow_interp ? 1 : 0;
+    CROMA_CUDA(cudaMemcpyAsync(c.d_bg, s->bg_curr, kNbg * n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    const double *bg_next = c.d_bg;
+    if (allow && s->bg_next && s->bg_next != s->bg_curr) {
+        CROMA_CUDA(cudaMemcpyAsync(c.d_bg + kNbg * n, s->bg_next, kNbg * n * sizeof(double), cudaMemcpyHostToDevice,
+                                   c.stream));
+        bg_next = c.d_bg + kNbg * n;
+    }
+    // 2. DSA injection from the host shock fields (synchronous)
+    int launches = 0;
+    if (io->shocks && io->dsa_mode != CROMA_DSA_OFF) {
+        int nin = 0;
+        const int rc = dsa_inject(c, io->shocks, io->density_unit, s->dt_snap, io->dsa_mode, io->dsa_reacc, &nin);
+        if (rc) return rc;
+        launches += c.last_launches;
+    }
+    // 3. emission of the spectra the snapshot starts from, downloaded on the
+    //    copy stream while the evolve runs
+    double *d_emis = nullptr;
+    struct Guard {
+        Context &c;
+        double *&p;
+        ~Guard()
+        {
+            if (p) dev_free(c, p);
+        }
+    } guard{c, d_emis};
+    if (want_emis) {
+        const CromaB200EmissionSetup &es = emission_config(c);
+        double *host[4] = {io->eps_syn, io->eps_ic, io->eps_gamma, io->eps_nu};
+        const int cols[4] = {host[0] ? es.nfreq : 0, host[1] ? es.nbins_ic : 0, host[2] ? es.nbins_gamma : 0,
+                             host[3] ? es.nbins_nu : 0};
+        size_t total = 0;
+        for (int k = 0; k < 4; k++) total += n * (size_t)cols[k];
+        CROMA_CUDA(dev_alloc(c, &d_emis, (total ? total : 1) * sizeof(double)));
+        double *dev[4];
+        double *q = d_emis;
+        for (int k = 0; k < 4; k++) {
+            dev[k] = cols[k] ? q : nullptr;
+            q += n * (size_t)cols[k];
+        }
+        const int rc = emission_run(c, c.d_bg, s->z_curr, dev[0], dev[1], dev[2], dev[3]);
+        if (rc) return rc;
+        launches += emission_launches(c, dev[0] != nullptr, dev[1] != nullptr, dev[2] != nullptr, dev[3] != nullptr);
+        if (!c.pipe_start) CROMA_CUDA(cudaEventCreateWithFlags(&c.pipe_start, cudaEventDisableTiming));
+        CROMA_CUDA(cudaEventRecord(c.pipe_start, c.stream));
+        CROMA_CUDA(cudaStreamWaitEvent(c.d2h_stream, c.pipe_start, 0));
+        for (int k = 0; k < 4; k++)
+            if (cols[k])
+                CROMA_CUDA(cudaMemcpyAsync(host[k], dev[k], n * cols[k] * sizeof(double), cudaMemcpyDeviceToHost,
+                                           c.d2h_stream));
+    }
+    // 4. the evolve; each workspace chunk's rows go back as soon as it is done
+    HostPipe pipe;
+    pipe.crp = io->crp_out;
+    pipe.cre = io->cre_out;
+    pipe.down_p = io->crp_out && (c.mp.species_mask & CROMA_SPECIES_PROTON) != 0;
+    pipe.down_e = io->cre_out && (c.mp.species_mask & CROMA_SPECIES_ELECTRON) != 0;
+    pipe.bounds.push_back(0);
+    push_split(pipe.bounds, 0, (int)n, c.fused_chunk);
+    const int nchunk = (int)pipe.bounds.size() - 1;
+    while ((int)c.pipe_up.size() < nchunk) {
+        cudaEvent_t u = nullptr, d = nullptr, dp = nullptr;
+        CROMA_CUDA(cudaEventCreateWithFlags(&u, cudaEventDisableTiming));
+        c.pipe_up.push_back(u);
+        CROMA_CUDA(cudaEventCreateWithFlags(&d, cudaEventDisableTiming));
+        c.pipe_done.push_back(d);
+        CROMA_CUDA(cudaEventCreateWithFlags(&dp, cudaEventDisableTiming));
+        c.pipe_done_p.push_back(dp);
+    }
+    // nothing to upload: every chunk's gate is already open
+    for (int k = 0; k < nchunk; k++) CROMA_CUDA(cudaEventRecord(c.pipe_up[k], c.stream));
+    CromaB200Snapshot sd = *s;
+    sd.bg_curr = c.d_bg;
+    sd.bg_next = bg_next;
+    sd.bg_on_device = 1;
+    c.pipe = &pipe;
+    int rc = snapshot_impl(c, &sd, 0);
+    c.pipe = nullptr;
+    launches += c.last_launches;
+    const cudaError_t e1 = cudaStreamSynchronize(c.stream);
+    const cudaError_t e2 = cudaStreamSynchronize(c.d2h_stream);
+    c.last_launches = launches;
+    if (rc) return rc;
+    if (e1 != cudaSuccess) return cuda_fail(e1, "step_host compute");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "step_host downloads");
+    return check_err(c);
+}
+
 int croma_b200_set_dsa(CromaB200Context *h, const CromaB200DsaParams *params)
 {
     if (!h) { set_error("null context"); return -1; }
@@ -711,6 +817,20 @@ __global__ void fp64_fma_probe(int iters, double seed, double *out)
 }  // namespace croma_probe
 
 extern "C" {
+
+int croma_b200_host_alloc(size_t bytes, void **out)
+{
+    if (!out || bytes == 0) { set_error("invalid host_alloc arguments"); return -1; }
+    *out = nullptr;
+    CROMA_CUDA(cudaHostAlloc(out, bytes, cudaHostAllocPortable));
+    return 0;
+}
+
+int croma_b200_host_free(void *p)
+{
+    if (p) CROMA_CUDA(cudaFreeHost(p));
+    return 0;
+}
 
 int croma_b200_fp64_peak(double *tflops)
 {

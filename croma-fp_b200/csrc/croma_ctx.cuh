@@ -16,6 +16,8 @@
 
 namespace croma {
 
+struct EmissionState;   // emission.cu
+
 constexpr int NB = CROMA_NB;
 static_assert(NB == 128 || NB == 256 || NB == 512, "supported bin counts: 128, 256, 512");
 
@@ -149,6 +151,9 @@ struct Context {
     cudaEvent_t pipe_start = nullptr;   // compute stream's earlier work, gating the uploads
     const HostPipe *pipe = nullptr;
 
+    // resident emission tables (croma_b200_emission_setup)
+    EmissionState *emission = nullptr;
+
     unsigned *d_err = nullptr;
     int last_launches = 0;
     int last_nsub_max = 0;
@@ -213,5 +218,14 @@ int set_dsa(Context &ctx, const CromaB200DsaParams *prm);
 int dsa_inject(Context &ctx, const CromaB200Shocks *sh, double density_unit, double dt_gyr, int mode,
                int reacc_mode, int *ninjected);
 void free_dsa(Context &ctx);
+// emission.cu
+int emission_setup(Context &c, const CromaB200EmissionSetup *s);
+int emission_run(Context &c, const double *bg_dev, double z, double *eps_syn, double *eps_ic, double *eps_gamma,
+                 double *eps_nu);
+int emission_tables(Context &c, int which, double *out);
+const CromaB200EmissionSetup &emission_config(const Context &c);
+// kernels one emission_run call launches for the requested kinds
+int emission_launches(const Context &c, bool syn, bool ic, bool gamma, bool nu);
+void free_emission(Context &c);
 
 }  // namespace croma

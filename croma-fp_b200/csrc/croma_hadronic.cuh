@@ -148,4 +148,130 @@ CROMA_HD double qe_kernel(double Ee, double p)
     return 8.0 * bmu * kMpiCh * kMpiCh * (kC * kMe) * integral / (kMpiCh * kMpiCh - kMmu * kMmu);
 }
 
+// ----------------------------------------------------------------------
+// Emission kernels of the pp interaction (the gamma and neutrino tables of
+// prepare_gamma_kernel_flat / prepare_neutrino_kernel_flat,
+// src/fp_shared_core.c:1724-1778).  Kelner (2006) energy distributions over
+// the same pion spectrum and cross sections as the secondaries above; the
+// step counts are include/HADRONIC.h:6-12 (200 pion-energy / x steps,
+// thresholds 0.285 / 0.289 / 0.29 GeV).
+// ----------------------------------------------------------------------
+constexpr double kMpi0 = 1.35e-1;          // pion0_mass_gev, src/CONSTANTS.c:21
+constexpr int kHadronSteps = 200;          // HADRON_KERNEL_EPI_STEPS = HADRON_ELECTRON_X_STEPS
+
+// gammaKernel, src/HADRONIC.c:139-177: pi0 -> 2 gamma, trapezoid over a
+// log-spaced pion energy from E_g + m_pi0^2 / (4 E_g) to E_p.
+CROMA_HD double gamma_kernel(double Eg, double p)
+{
+    const double gp = sqrt(p * p + 1.0), Ep = gp * kMp;
+    const double Emax = Ep;
+    double Emin = Eg + kMpi0 * kMpi0 / (4.0 * Eg);
+    if (Emax < Emin) return 0.0;
+    if (Emin < kMpi0) Emin = kMpi0;
+    if ((Ep - kMp) < 0.285) return 0.0;
+    const double amin = log10(Emin), amax = log10(Emax), da = (amax - amin) / (double)kHadronSteps;
+    double a = amin, Epi = pow(10.0, a);
+    double f = dsigma(0, Epi, Ep) / sqrt(Epi * Epi - kMpi0 * kMpi0), integral = 0.0;
+    for (int i = 1; i < kHadronSteps; i++) {
+        const double Epipre = Epi, fpre = f;
+        a += da;
+        Epi = pow(10.0, a);
+        const double dEpi = Epi - Epipre;
+        f = dsigma(0, Epi, Ep) / sqrt(Epi * Epi - kMpi0 * kMpi0);
+        integral += 0.5 * (f + fpre) * dEpi;
+    }
+    return 2.0 * kC * integral / (4.0 * kPi);
+}
+
+// Kelner (2006) eq. (36): electron / muon-neutrino spectrum from muon decay
+// in the pion frame (fe, src/HADRONIC.c:302-310).
+CROMA_HD double kelner_fe(double x)
+{
+    const double r = kMmu * kMmu / (kMpiCh * kMpiCh), x2 = x * x, r2 = r * r;
+    if (x > r) return (3.0 - 2.0 * r) * (9.0 * x2 - 6.0 * log(x) - 4.0 * x2 * x - 5.0) / (9.0 * pow(1.0 - r, 2.0));
+    const double h1 = (3.0 - 2.0 * r) * (9.0 * r2 - 6.0 * log(r) - 4.0 * r2 * r - 5.0) / (9.0 * pow(1.0 - r, 2.0));
+    const double h2 = (1.0 + 2.0 * r) * (r - x) * (9.0 * (r + x) - 4.0 * (r2 + r * x + x2)) / (9.0 * r2);
+    return h1 + h2;
+}
+
+// Kelner (2006) eq. (40): electron-neutrino spectrum, r = 0.573
+// (fnue, src/HADRONIC.c:311-320).
+CROMA_HD double kelner_fnue(double x)
+{
+    const double r = 0.573, x2 = x * x, r2 = r * r;
+    if (x > r)
+        return 2.0 * (1.0 - x) * (6.0 * pow(1.0 - x, 2.0) + r * (5.0 + 5.0 * x - 4.0 * x2) + 6.0 * r * log(x) / (1.0 - x)) /
+               (3.0 * pow(1.0 - r, 2.0));
+    const double h1 = 2.0 * ((1.0 - r) * (6.0 - 7.0 * r + 11.0 * r2 - 4.0 * r2 * r) + 6.0 * r * log(r)) /
+                      (3.0 * pow(1.0 - r, 2.0));
+    const double h2 = 2.0 * (r - x) * (7.0 * r2 - 4.0 * r2 * r + 7.0 * x * r - 4.0 * x * r2 - 2.0 * x2 - 4.0 * x2 * r) /
+                      (3.0 * r2);
+    return h1 + h2;
+}
+
+enum LeptonKind { kLeptonElectron = 0, kLeptonNue = 1, kLeptonNumu = 2 };   // HadronLeptonKernel
+
+// One charge of eKernel's sum: trapezoid in x = E / E_pi on (0, 1) with the
+// first interval taken as a rectangle (src/HADRONIC.c:200-236).
+template <int KIND>
+CROMA_HD double lepton_x_integral(int charge, double E, double Ep)
+{
+    const double dx = 1.0 / (double)kHadronSteps;
+    double x = 0.0, f = 0.0, integral = 0.0;
+    for (int i = 1; i < kHadronSteps; i++) {
+        x += dx;
+        const double Epi = E / x, fpre = f;
+        f = dsigma(charge, Epi, Ep) * (KIND == kLeptonNue ? kelner_fnue(x) : kelner_fe(x)) / x;
+        integral += (i == 1) ? f * dx : 0.5 * (f + fpre) * dx;
+    }
+    return integral;
+}
+
+// eKernel, src/HADRONIC.c:181-236, for the neutrino kinds (the electron kind
+// is the secondary source, qe_kernel above).
+template <int KIND>
+CROMA_HD double lepton_kernel(double E, double p)
+{
+    const double gp = sqrt(p * p + 1.0), Ep = gp * kMp;
+    const double Emax = gp * kMp;
+    const double Emin = 2.0 * E * kMpiCh * kMpiCh / (kMpiCh * kMpiCh + kMmu * kMmu);
+    if (Emax < Emin) return 0.0;
+    if ((Ep - kMp) < 0.289) return 0.0;
+    const double i1 = lepton_x_integral<KIND>(1, E, Ep);
+    const double i2 = lepton_x_integral<KIND>(-1, E, Ep);
+    return kC * (i1 + i2) / (4.0 * kPi);
+}
+
+// numu1Kernel, src/HADRONIC.c:240-289: muon neutrinos of the pion decay
+// itself, x = E / E_pi on (0, lambda).
+CROMA_HD double numu_pion_kernel(double Enu, double p)
+{
+    const double lambda = 1.0 - kMmu * kMmu / (kMpiCh * kMpiCh);
+    const double gp = sqrt(p * p + 1.0), Ep = gp * kMp, Emax = gp * kMp, Emin = Enu / lambda;
+    if (Emax < Emin) return 0.0;
+    if ((Ep - kMp) < 0.29) return 0.0;
+    const double dx = lambda / (double)kHadronSteps;
+    double sum[2];
+    for (int s = 0; s < 2; s++) {
+        const int charge = s ? -1 : 1;
+        double x = 0.0, f = 0.0, integral = 0.0;
+        for (int i = 1; i < kHadronSteps; i++) {
+            x += dx;
+            const double Epi = Enu / x, fpre = f;
+            f = dsigma(charge, Epi, Ep) / x;
+            integral += (i == 1) ? f * dx : 0.5 * (f + fpre) * dx;
+        }
+        sum[s] = integral;
+    }
+    return kC * (sum[0] + sum[1]) / lambda / (4.0 * kPi);
+}
+
+// One entry of the neutrino table: muon + electron neutrinos of muon decay
+// plus the muon neutrino of the pion decay (prepare_neutrino_kernel_flat,
+// src/fp_shared_core.c:1771-1773, in that order).
+CROMA_HD double neutrino_kernel(double Enu, double p)
+{
+    return lepton_kernel<kLeptonNumu>(Enu, p) + lepton_kernel<kLeptonNue>(Enu, p) + numu_pion_kernel(Enu, p);
+}
+
 }  // namespace croma

@@ -305,4 +305,35 @@ CROMA_HD double b_ic_integrand(double eps0, double gamma, double emin, double em
     return integral;
 }
 
+// IC_emissivity_kernel, FP_Coef.c:553-584: the inverse-Compton emissivity of
+// one electron of Lorentz factor gamma at frequency nu (Hz), a 400-step
+// log-spaced trapezoid over the seed CMB photon energy.  The photon energy
+// is normalised with the routine's own c = 3.0e10.
+CROMA_HD double ic_emissivity(const IcConsts &k, double nu, double gamma, double z)
+{
+    const int N = 400;
+    const double meg = 9.11e-28, c_local = 3.0e+10;
+    const double eps = kHPlanck * nu / (meg * c_local * c_local);
+    const double e0max = eps;
+    double e0min = eps / (4.0 * gamma * (gamma - eps));
+    if (e0min < 0) e0min = eps / (gamma * gamma);
+    const double da = (log10(e0max) - log10(e0min)) / (double)N;
+    double a = log10(e0min);
+    double eps0new = pow(10.0, a);
+    double Cnew = ic_kernel(eps0new, gamma, eps);
+    double n0new = cmb_density(k, eps0new, z);
+    double integral = 0.0;
+    for (int i = 0; i < N; i++) {
+        a = a + da;
+        const double eps0 = eps0new;
+        eps0new = pow(10.0, a);
+        const double deps0 = eps0new - eps0;
+        const double C = Cnew, n = n0new;
+        n0new = cmb_density(k, eps0new, z);
+        Cnew = ic_kernel(eps0new, gamma, eps);
+        integral = integral + 0.5 * (C * n + Cnew * n0new) * deps0;
+    }
+    return kHPlanck * eps * integral / (4.0 * kPi);
+}
+
 }  // namespace croma

@@ -31,6 +31,7 @@
 #define npe CROMA_NB
 #include "../../include/fp_cuda_backend.h"
 #include "croma_segment.cuh"
+#include "croma_emission.cuh"
 
 // CROMA's parameter globals (include/params.h): bound when present.
 extern "C" {
@@ -210,155 +211,6 @@ __global__ void cc_thomas_kernel(int nsys, int nrow, double dt, const double *a,
         x[i] = ((dt * src[o + i] + x_in[o + i]) + a[o + i] * x[i - 1]) / den;
     }
     for (int i = nrow - 2; i >= 0; i--) x[i] -= cp[i] * x[i + 1];
-}
-
-// ---- emission kernels ----
-// Q_one (src/EMISSION.c:297-308) times E n_gas, one thread per (cell, bin).
-__global__ void hadronic_emission_kernel(int ncell, int nbins, const double *crp, const double *n_gas,
-                                         const double *beta_p, const double *dp, const double *kern,
-                                         const double *E, double *out)
-{
-    const int ng = blockIdx.y * blockDim.y + threadIdx.y;
-    const int icell = blockIdx.x * blockDim.x + threadIdx.x;
-    if (icell >= ncell || ng >= nbins) return;
-    const double *N = crp + (size_t)icell * NB;
-    const double *f = kern + (size_t)ng * NB;
-    double fpre = beta_p[0] * N[0] * f[0], integral = 0.0;
-    for (int i = 1; i < NB; i++) {
-        const double fn = beta_p[i] * N[i] * f[i];
-        integral += (fpre + fn) * dp[i];
-        fpre = fn;
-    }
-    out[(size_t)icell * nbins + ng] = E[ng] * (integral * 0.5) * n_gas[icell];
-}
-
-// prepare_ic_emission_cell_major (src/fp_shared_core.c:2131-2157): per
-// (cell, band) the sum over electron bins of fic x N x dp, in bin order.
-__global__ void ic_emission_kernel(int ncell, int nbins, const double *cre, const double *fic,
-                                   const double *dp, double *out)
-{
-    const int nic = blockIdx.y * blockDim.y + threadIdx.y;
-    const int icell = blockIdx.x * blockDim.x + threadIdx.x;
-    if (icell >= ncell || nic >= nbins) return;
-    const double *N = cre + (size_t)icell * NB;
-    const double *f = fic + (size_t)nic * NB;
-    double integral = 0.0;
-    for (int je = 0; je < NB; je++) integral += f[je] * N[je] * dp[je];
-    out[(size_t)icell * nbins + nic] = integral;
-}
-
-// prepare_synch_emission_cell_major, pitch-kernel-table branch
-// (src/fp_shared_core.c:2070-2112 with tracer_fp_interp_synch_kernel_logk :2054-2068).
-__global__ void synch_table_kernel(int ncell, int nfreq, int nlogb, double logb_min, double inv_dlogb,
-                                   double a0, double den1, double den2, const double *table,
-                                   const double *b_dyn, const double *logb, const double *cre,
-                                   const double *dp, double *out)
-{
-    const int nf = blockIdx.y * blockDim.y + threadIdx.y;
-    const int icell = blockIdx.x * blockDim.x + threadIdx.x;
-    if (icell >= ncell || nf >= nfreq) return;
-    const double *N = cre + (size_t)icell * NB;
-    const double A = a0 * b_dyn[icell] / den1 / den2;
-    const double u = (logb[icell] - logb_min) * inv_dlogb;
-    int ib = (int)floor(u);
-    if (ib < 0) ib = 0;
-    if (ib > nlogb - 2) ib = nlogb - 2;
-    double t = u - (double)ib;
-    if (t < 0.0) t = 0.0;
-    if (t > 1.0) t = 1.0;
-    const double *k0 = table + ((size_t)ib * nfreq + nf) * NB;
-    const double *k1 = table + ((size_t)(ib + 1) * nfreq + nf) * NB;
-    double integral = 0.0;
-    for (int je = 2; je < NB - 1 && N[je + 1] > 0.0; je++) {
-        const double a = k0[je], b = k1[je];
-        double K;
-        if (t <= 0.0) K = a;
-        else if (t >= 1.0) K = b;
-        else if (a > 0.0 && b > 0.0) K = exp((1.0 - t) * log(a) + t * log(b));
-        else K = (1.0 - t) * a + t * b;
-        integral += N[je] * K * dp[je];
-    }
-    out[(size_t)icell * nfreq + nf] = A * integral;
-}
-
-// The synchrotron F(x) of the log-tabulated kernel at logx: 0 above the
-// table, 0 below its first cell, the last value past its last cell, else
-// 10^(log-linear interpolation) -- the lookup of SYN_emissivity_from_arrays
-// (src/Synchrotron.c:81-97) and prepare_synch_pitch_kernel_table
-// (src/fp_shared_core.c:2027-2042).
-struct SynchFx {
-    int nx;
-    double xmin, inv_dlogx, logx_last, fx_last;
-    const double *logx_tab, *logfx_tab;
-    __device__ double operator()(double logx) const
-    {
-        if (!(logx <= logx_last)) return 0.0;
-        const int ix = (int)floor((logx - xmin) * inv_dlogx);
-        if (ix < 0) return 0.0;
-        if (ix >= nx - 1) return fx_last;
-        const double frac = (logx - logx_tab[ix]) * inv_dlogx;
-        return pow(10.0, logfx_tab[ix] + frac * (logfx_tab[ix + 1] - logfx_tab[ix]));
-    }
-};
-
-// sum_k F(logy[nf][je][k] - logb) w_k, the pitch-angle integral of one
-// (frequency, electron bin) at one log B
-__device__ __forceinline__ double pitch_integral(const SynchFx &F, const double *logy_row, const double *w,
-                                                 int ntheta, double logb)
-{
-    double s = 0.0;
-    for (int k = 0; k < ntheta; k++) s += F(logy_row[k] - logb) * w[k];
-    return s;
-}
-
-// prepare_synch_pitch_kernel_table (src/fp_shared_core.c:2008-2052): table
-// [nlogb][nfreq][npe], one thread per entry.
-__global__ void synch_pitch_table_kernel(SynchFx F, int nfreq, int ntheta, int nlogb, double logb_min,
-                                         double inv_dlogb, const double *logy, const double *w, double *table)
-{
-    const long long total = (long long)nlogb * nfreq * NB;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int je = (int)(i % NB);
-        const long long r = i / NB;
-        const int nf = (int)(r % nfreq), ib = (int)(r / nfreq);
-        const double logb = logb_min + (double)ib / inv_dlogb;
-        table[i] = pitch_integral(F, logy + ((size_t)nf * NB + je) * ntheta, w, ntheta, logb);
-    }
-}
-
-// prepare_synch_emission_cell_major without a pitch-kernel table
-// (src/fp_shared_core.c:2113-2120 -> SYN_emissivity_from_arrays,
-// src/Synchrotron.c:62-103): one warp per (cell, frequency).  The bins run
-// from 2 up to the first je whose N[je+1] is not positive (found by a
-// ballot); lanes take strided bins and a shuffle tree sums them.
-__global__ void __launch_bounds__(128) synch_theta_kernel(SynchFx F, int ncell, int nfreq, int ntheta,
-                                                          double a0, double den1, double den2,
-                                                          const double *logy, const double *w,
-                                                          const double *b_dyn, const double *logb,
-                                                          const double *cre, const double *dp, double *out)
-{
-    const int lane = threadIdx.x & 31;
-    const long long idx = (long long)blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (idx >= (long long)ncell * nfreq) return;
-    const int icell = (int)(idx / nfreq), nf = (int)(idx % nfreq);
-    const double *N = cre + (size_t)icell * NB;
-    int stop = NB - 1;   // first je >= 2 with N[je+1] <= 0, else npe - 1
-    for (int j0 = 2; j0 < NB - 1; j0 += 32) {
-        const int je = j0 + lane;
-        const unsigned hit = __ballot_sync(0xffffffffu, je < NB - 1 && !(N[je + 1] > 0.0));
-        if (hit) {
-            stop = j0 + __ffs(hit) - 1;
-            break;
-        }
-    }
-    const double lb = logb[icell];
-    double s = 0.0;
-    for (int je = 2 + lane; je < stop; je += 32)
-        s += N[je] * pitch_integral(F, logy + ((size_t)nf * NB + je) * ntheta, w, ntheta, lb) * dp[je];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    if (lane == 0) out[idx] = a0 * b_dyn[icell] / den1 / den2 * s;
 }
 
 // One-shot device buffers of the stateless entry points (grow-only, guarded).
@@ -969,10 +821,9 @@ int prepare_synch_emission_cuda_batch(const FpSynchEmissionBatchInput *in, const
     CROMA_CUDA(cudaMemcpy(d_lb, in->logb, ncell * sizeof(double), cudaMemcpyHostToDevice));
     CROMA_CUDA(cudaMemcpy(d_cre, in->cre_batch, (size_t)ncell * NB * sizeof(double), cudaMemcpyHostToDevice));
     CROMA_CUDA(cudaMemcpy(d_dp, cre_grid->dp, NB * sizeof(double), cudaMemcpyHostToDevice));
-    const double a0 = sqrt(3.0) * pow(4.8e-10, 3.0);
-    const double den1 = 2.0 * 9.11e-28 * kC * kC, den2 = 4.0 * kPi;
+    const SynchPrefactor sp = synch_prefactor();
     dim3 blk(32, 4), grd((ncell + 31) / 32, (nfreq + 3) / 4);
-    synch_table_kernel<<<grd, blk>>>(ncell, nfreq, nlogb, in->logb_min, in->inv_dlogb, a0, den1, den2,
+    synch_table_kernel<<<grd, blk>>>(ncell, nfreq, nlogb, in->logb_min, in->inv_dlogb, sp.a0, sp.den1, sp.den2,
                                      d_tab, d_b, d_lb, d_cre, d_dp, d_out);
     CROMA_CUDA(cudaGetLastError());
     CROMA_CUDA(cudaMemcpy(eps_syn_out, d_out, (size_t)ncell * nfreq * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1012,10 +863,9 @@ int synch_emission_theta(const FpSynchEmissionBatchInput *in, const CRspectrum *
     CROMA_CUDA(cudaMemcpy(d_lb, in->logb, ncell * sizeof(double), cudaMemcpyHostToDevice));
     CROMA_CUDA(cudaMemcpy(d_cre, in->cre_batch, (size_t)ncell * NB * sizeof(double), cudaMemcpyHostToDevice));
     CROMA_CUDA(cudaMemcpy(d_dp, cre_grid->dp, NB * sizeof(double), cudaMemcpyHostToDevice));
-    const double a0 = sqrt(3.0) * pow(4.8e-10, 3.0);
-    const double den1 = 2.0 * 9.11e-28 * kC * kC, den2 = 4.0 * kPi;
+    const SynchPrefactor sp = synch_prefactor();
     const long long warps = (long long)ncell * nfreq;
-    synch_theta_kernel<<<(unsigned)((warps + 3) / 4), 128>>>(t.F, ncell, nfreq, in->ntheta_pitch, a0, den1, den2,
+    synch_theta_kernel<<<(unsigned)((warps + 3) / 4), 128>>>(t.F, ncell, nfreq, in->ntheta_pitch, sp.a0, sp.den1, sp.den2,
                                                             t.d_logy, t.d_w, d_b, d_lb, d_cre, d_dp, d_out);
     CROMA_CUDA(cudaGetLastError());
     CROMA_CUDA(cudaMemcpy(eps_syn_out, d_out, (size_t)ncell * nfreq * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1141,8 +991,7 @@ int croma_b200_emission_synch(CromaB200Context *ctx, int nfreq, int nlogb, doubl
     if (!ctx || nfreq <= 0) return fail(-1, "invalid emission arguments");
     if (nlogb <= 1 || !(inv_dlogb > 0.0)) return fail(-1, "synchrotron emission needs a pitch-kernel table");
     const size_t ncell = (size_t)(ctx->impl.ntracer > 0 ? ctx->impl.ntracer : 0);
-    const double a0 = sqrt(3.0) * pow(4.8e-10, 3.0);
-    const double den1 = 2.0 * 9.11e-28 * kC * kC, den2 = 4.0 * kPi;
+    const SynchPrefactor sp = synch_prefactor();
     return ctx_emission(ctx, 1, nfreq,
                         {{table, (size_t)nlogb * nfreq * NB * sizeof(double)}, {b_dyn, ncell * sizeof(double)},
                          {logb, ncell * sizeof(double)}},
@@ -1150,8 +999,8 @@ int croma_b200_emission_synch(CromaB200Context *ctx, int nfreq, int nlogb, doubl
                         [&](const std::vector<const double *> &in, const double *cre, const double *dp,
                             double *out, int nc, cudaStream_t st) {
                             dim3 blk(32, 4), grd((nc + 31) / 32, (nfreq + 3) / 4);
-                            synch_table_kernel<<<grd, blk, 0, st>>>(nc, nfreq, nlogb, logb_min, inv_dlogb, a0, den1,
-                                                                    den2, in[0], in[1], in[2], cre, dp, out);
+                            synch_table_kernel<<<grd, blk, 0, st>>>(nc, nfreq, nlogb, logb_min, inv_dlogb, sp.a0, sp.den1,
+                                                                    sp.den2, in[0], in[1], in[2], cre, dp, out);
                         });
 }
 

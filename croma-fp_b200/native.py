@@ -81,8 +81,30 @@ def load_library(nb: int) -> C.CDLL:
     L.croma_b200_emission_ic.argtypes = [_vp, _i, _vp, _vp, P(_d)]
     L.croma_b200_emission_hadronic.argtypes = [_vp, _i, _d, _d, _vp, _vp, _vp, _vp, P(_d)]
     L.croma_b200_emission_synch.argtypes = [_vp, _i, _i, _d, _d, _vp, _vp, _vp, _vp, P(_d)]
+    L.croma_b200_emission_setup.argtypes = [_vp, P(CromaB200EmissionSetup)]
+    L.croma_b200_emission_run.argtypes = [_vp, _vp, _d, _vp, _vp, _vp, _vp, _i]
+    L.croma_b200_emission_table.argtypes = [_vp, _i, _vp]
+    L.croma_b200_step_host.argtypes = [_vp, P(CromaB200Snapshot), P(CromaB200StepHost)]
+    L.croma_b200_host_alloc.argtypes = [C.c_size_t, P(_vp)]
+    L.croma_b200_host_free.argtypes = [_vp]
     _LIBS[nb] = L
     return L
+
+
+class CromaB200EmissionSetup(C.Structure):
+    _fields_ = [("nfreq", _i), ("nu_min_s", _d), ("nu_max_s", _d), ("ntheta_pitch", _i), ("nlogb", _i),
+                ("logb_min", _d), ("logb_max", _d), ("nbins_ic", _i), ("nu_min_ic", _d), ("nu_max_ic", _d),
+                ("nbins_gamma", _i), ("egamma_min", _d), ("egamma_max", _d), ("nbins_nu", _i),
+                ("enu_min", _d), ("enu_max", _d)]
+
+
+# The emission bands of the full-pipeline workload: synchrotron at 64
+# frequencies over 10 MHz .. 10 GHz; IC, gamma and neutrinos at 64 energies
+# over 1 keV .. 1 PeV (IC in log10 Hz: E / h); the reference's default pitch
+# angles (512) and log-B table (512 planes over [-6, 2]).
+EMISSION_CONFIG4 = dict(nfreq=64, nu_min_s=7.0, nu_max_s=10.0, ntheta_pitch=512, nlogb=512, logb_min=-6.0,
+                        logb_max=2.0, nbins_ic=64, nu_min_ic=17.383, nu_max_ic=29.383, nbins_gamma=64,
+                        egamma_min=-6.0, egamma_max=6.0, nbins_nu=64, enu_min=-6.0, enu_max=6.0)
 
 
 class CromaB200DsaParams(C.Structure):
@@ -98,6 +120,12 @@ SHOCK_FIELDS = ("mach", "prestemp", "presden", "pre_density_cgs", "upstream_spee
 
 class CromaB200Shocks(C.Structure):
     _fields_ = [(n, _vp) for n in SHOCK_FIELDS] + [("has_dsa", _i), ("on_device", _i)]
+
+
+class CromaB200StepHost(C.Structure):
+    _fields_ = [("shocks", C.POINTER(CromaB200Shocks)), ("dsa_mode", _i), ("dsa_reacc", _i),
+                ("density_unit", _d), ("eps_syn", _vp), ("eps_ic", _vp), ("eps_gamma", _vp), ("eps_nu", _vp),
+                ("crp_out", _vp), ("cre_out", _vp)]
 
 
 class CromaError(RuntimeError):
@@ -128,12 +156,54 @@ def fp64_peak(nb: int = 256) -> float:
     return t.value
 
 
+def _shocks_struct(shocks: dict):
+    """CromaB200Shocks from a dict of SHOCK_FIELDS arrays (or device
+    addresses with shocks['on_device']); returns (struct, arrays to keep)."""
+    sh = CromaB200Shocks()
+    keep = []
+    on_dev = int(shocks.get("on_device", 0))
+    for n in SHOCK_FIELDS:
+        a = shocks.get(n)
+        if a is None:
+            continue
+        if on_dev:
+            setattr(sh, n, int(a))
+        else:
+            arr = np.ascontiguousarray(a, dtype=np.float64)
+            keep.append(arr)
+            setattr(sh, n, arr.ctypes.data)
+    sh.has_dsa = int(shocks.get("has_dsa", 0))
+    sh.on_device = on_dev
+    return sh, keep
+
+
 def _p(a):
     return None if a is None else a.ctypes.data_as(_vp)
 
 
 def _c(a, dtype=np.float64):
     return None if a is None else np.ascontiguousarray(a, dtype=dtype)
+
+
+class PinnedArray:
+    """A float64 numpy array in page-locked host memory of exactly its size
+    (croma_b200_host_alloc); .a is the array, .free() releases it."""
+
+    def __init__(self, shape, nb: int = 512):
+        self.lib = load_library(nb)
+        n = int(np.prod(shape))
+        ptr = _vp()
+        if self.lib.croma_b200_host_alloc(C.c_size_t(n * 8), C.byref(ptr)) != 0:
+            raise CromaError(self.lib.croma_b200_last_error().decode())
+        self.ptr = ptr.value
+        buf = (C.c_double * n).from_address(self.ptr)
+        self.a = np.frombuffer(buf, dtype=np.float64).reshape(shape)
+
+    def free(self):
+        if self.ptr:
+            self.a = None
+            self.lib.croma_b200_host_free(self.ptr)
+            self.ptr = None
 
 
 class TracerFP:
@@ -254,6 +324,37 @@ class TracerFP:
                                                       int(chunks)))
         self.ntracer = n
 
+    def step_host(self, bg_curr, bg_next, z_curr, z_next, allow, dt, elapsed, shocks=None, dsa_mode="off",
+                  dsa_reacc="off", density_unit=1.0, outputs=None):
+        """One snapshot step through host memory (croma_b200_step_host): DSA
+        from host shock fields, emission and evolve; outputs maps 'syn', 'ic',
+        'gamma', 'nu', 'crp', 'cre' to host arrays filled in place (page-locked
+        ones let the copies overlap)."""
+        outputs = outputs or {}
+        bc = _c(bg_curr)
+        bn = _c(bg_next) if bg_next is not None else bc
+        snap = CromaB200Snapshot()
+        snap.bg_curr, snap.bg_next, snap.bg_on_device = bc.ctypes.data, bn.ctypes.data, 0
+        snap.z_curr, snap.z_next, snap.allow_interp = z_curr, z_next, int(bool(allow))
+        snap.dt_snap, snap.elapsed_gyr = dt, elapsed
+        io = CromaB200StepHost()
+        keep = None
+        if shocks is not None:
+            sh, keep = _shocks_struct(shocks)
+            io.shocks = C.pointer(sh)
+        io.dsa_mode = self.DSA_MODES[dsa_mode] if isinstance(dsa_mode, str) else int(dsa_mode)
+        io.dsa_reacc = self.DSA_REACC[dsa_reacc] if isinstance(dsa_reacc, str) else int(dsa_reacc)
+        io.density_unit = float(density_unit)
+        for k, f in (("syn", "eps_syn"), ("ic", "eps_ic"), ("gamma", "eps_gamma"), ("nu", "eps_nu"),
+                     ("crp", "crp_out"), ("cre", "cre_out")):
+            a = outputs.get(k)
+            if a is not None:
+                if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape[0] != self.ntracer:
+                    raise ValueError(f"output {k} must be C-contiguous float64 with one row per tracer")
+                setattr(io, f, a.ctypes.data)
+        self._check(self.lib.croma_b200_step_host(self.h, C.byref(snap), C.byref(io)))
+        del keep
+
     def sync(self):
         self._check(self.lib.croma_b200_sync(self.h))
 
@@ -328,6 +429,39 @@ class TracerFP:
                                                        _p(bd), _p(lb), _p(eps), C.byref(ms)))
         return eps, ms.value
 
+    # -- emission into device or host memory ---------------------------
+    def emission_setup(self, **kw):
+        """Builds the emission tables on the device (croma_b200_emission_setup);
+        keywords are the CromaB200EmissionSetup fields, missing ones 0."""
+        st = CromaB200EmissionSetup()
+        for name, _ in CromaB200EmissionSetup._fields_:
+            setattr(st, name, kw.get(name, 0))
+        self._check(self.lib.croma_b200_emission_setup(self.h, C.byref(st)))
+        self._emis = {n: kw.get(n, 0) for n in ("nfreq", "nbins_ic", "nbins_gamma", "nbins_nu")}
+
+    def emission_run(self, bg, z, kinds=("syn", "ic", "gamma", "nu")):
+        """Emissivities of the resident spectra from a host background
+        [8][ntracer]: dict kind -> [ntracer][bins]."""
+        b = _c(bg)
+        if b.shape != (8, self.ntracer):
+            raise ValueError("bg must be [8][ntracer]")
+        cols = dict(syn=self._emis["nfreq"], ic=self._emis["nbins_ic"], gamma=self._emis["nbins_gamma"],
+                    nu=self._emis["nbins_nu"])
+        out = {k: np.empty((self.ntracer, cols[k])) for k in kinds if cols[k] > 0}
+        self._check(self.lib.croma_b200_emission_run(self.h, _p(b), float(z), _p(out.get("syn")), _p(out.get("ic")),
+                                                     _p(out.get("gamma")), _p(out.get("nu")), 0))
+        return out
+
+    def emission_run_device(self, bg_ptr: int, z, syn=0, ic=0, gamma=0, nu=0):
+        """Asynchronous emission on device pointers (ints, 0 skips a kind)."""
+        self._check(self.lib.croma_b200_emission_run(self.h, bg_ptr, float(z), syn or None, ic or None,
+                                                     gamma or None, nu or None, 1))
+
+    def emission_table(self, which: str, shape):
+        out = np.empty(shape)
+        self._check(self.lib.croma_b200_emission_table(self.h, {"synch": 0, "ic": 1}[which], _p(out)))
+        return out
+
     KERNEL_KINDS = {"evolve": 0, "coeff": 1, "secondary": 2}
 
     def set_kernel_timing(self, enable: bool):
@@ -360,21 +494,7 @@ class TracerFP:
         """One snapshot's shock injection; shocks maps SHOCK_FIELDS names to
         host arrays [ntracer] (or device addresses with shocks['on_device'])
         plus 'has_dsa'.  Returns the number of tracers injected."""
-        sh = CromaB200Shocks()
-        keep = []
-        on_dev = int(shocks.get("on_device", 0))
-        for n in SHOCK_FIELDS:
-            a = shocks.get(n)
-            if a is None:
-                continue
-            if on_dev:
-                setattr(sh, n, int(a))
-            else:
-                arr = np.ascontiguousarray(a, dtype=np.float64)
-                keep.append(arr)
-                setattr(sh, n, arr.ctypes.data)
-        sh.has_dsa = int(shocks.get("has_dsa", 0))
-        sh.on_device = on_dev
+        sh, keep = _shocks_struct(shocks)
         m = self.DSA_MODES[mode] if isinstance(mode, str) else int(mode)
         r = self.DSA_REACC[reacc] if isinstance(reacc, str) else int(reacc)
         nin = _i()

@@ -139,6 +139,22 @@ class RefAbi:
     def error(self) -> str:
         return self.lib.croma_b200_last_error().decode()
 
+    def kernel_table(self, fn: str, p, nbins: int, lo: float, hi: float, z: float = 0.0):
+        """A device-built emission kernel table through its reference-form
+        entry point (prepare_gamma_kernel_flat_cuda,
+        prepare_neutrino_kernel_flat_cuda, prepare_ic_kernel_flat_cuda) for
+        the momentum grid p: [nbins][nb]."""
+        f = getattr(self.lib, fn)
+        args = [C.POINTER(self.CRspectrum), _i, _d, _d] + ([_d] if fn == "prepare_ic_kernel_flat_cuda" else []) + [_D]
+        f.argtypes = args
+        zero = np.zeros(self.nb)
+        g = self.grid(p, zero, zero, 0.0, 0.0)
+        out = np.empty((nbins, self.nb))
+        extra = [z] if fn == "prepare_ic_kernel_flat_cuda" else []
+        if f(C.byref(g), nbins, lo, hi, *extra, dptr(out)) != 0:
+            raise RuntimeError(self.error())
+        return out
+
     def grid(self, p, dp, E, pm1, pp1):
         g = self.CRspectrum()
         g.p[:] = list(p)

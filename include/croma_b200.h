@@ -242,6 +242,84 @@ int croma_b200_emission_synch(CromaB200Context *ctx, int nfreq, int nlogb, doubl
                               const double *table, const double *b_dyn, const double *logb, double *eps_out,
                               double *elapsed_ms);
 
+/* ---- Emission of the resident spectra into device memory ----
+ * The per-snapshot emission of the reference's snapshot driver
+ * (include/tracer_fp_solve.inc:117-426: synchrotron, inverse Compton,
+ * hadronic gamma rays and neutrinos, from the spectra the snapshot starts
+ * from) with every kernel table built on the device:
+ *   F(x) = x int_x^inf K_5/3 from its integral definition (the reference
+ *   calls GNU GSL's gsl_sf_synchrotron_1 in SYN_logFx_table,
+ *   src/Synchrotron.c:31-41), the 2750-point log-x grid, pitch angles,
+ *   frequencies, logy and the log-B pitch-kernel table of
+ *   tracer_fp_synch_data_init_tables / tracer_fp_refresh_synch_kernel_table
+ *   (src/tracer_fp_synch.c:87-121, 175-240, fixed log-B range);
+ *   the gamma / neutrino tables of prepare_gamma/neutrino_kernel_flat
+ *   (src/fp_shared_core.c:1724-1778), once;
+ *   the IC table of prepare_ic_kernel_flat (:1780-1807), rebuilt when z changes.
+ * Band grids follow the reference: band k at 10^(lo + (k+1) d - d),
+ * d = (hi - lo) / nbins, lo / hi in log10 Hz (synchrotron, IC) or log10 GeV
+ * (gamma, neutrino).  A count of 0 disables that kind. */
+typedef struct {
+    int nfreq;                         /* synchrotron frequencies */
+    double nu_min_s, nu_max_s;         /* log10 Hz (params.c:116 defaults 5.5, 10.5) */
+    int ntheta_pitch;                  /* pitch angles (N_theta_pitch, params.h:12: 512) */
+    int nlogb;                         /* log-B planes (TRACER_FP_SYNCH_LOGB_BINS: 512) */
+    double logb_min, logb_max;         /* log10(B / 1 uG) range (params.c:117: -6, 2) */
+    int nbins_ic;
+    double nu_min_ic, nu_max_ic;       /* log10 Hz (params.c:120: 13, 28) */
+    int nbins_gamma;
+    double egamma_min, egamma_max;     /* log10 GeV (params.c:121: -2, 6) */
+    int nbins_nu;
+    double enu_min, enu_max;           /* log10 GeV (params.c:122: -2, 8) */
+} CromaB200EmissionSetup;
+
+/* Builds the tables on the device (synchronous).  Errors: -1 invalid setup
+ * (a kind whose species the context does not evolve), -3 CUDA. */
+int croma_b200_emission_setup(CromaB200Context *ctx, const CromaB200EmissionSetup *setup);
+
+/* Emissivities of the resident spectra at redshift z: eps_* [ntracer][bins of
+ * the kind], NULL skips a kind.  bg is the snapshot's background block
+ * ([8][ntracer] field-major as in CromaB200Snapshot): n_gas (field 0) scales
+ * the hadronic kinds, B (field 2) is the synchrotron b_dyn.  on_device = 1:
+ * bg and the outputs are device pointers and the call is asynchronous on the
+ * context stream (the outputs are ready when croma_b200_sync returns);
+ * on_device = 0: host pointers, synchronous.  Results agree with the
+ * reference's prepare_*_emission_cell_major on the same tables to rounding
+ * (the sums run in another order). */
+int croma_b200_emission_run(CromaB200Context *ctx, const double *bg, double z, double *eps_syn,
+                            double *eps_ic, double *eps_gamma, double *eps_nu, int on_device);
+
+/* A table of the emission setup, copied to host memory: which =
+ * CROMA_EMIS_TABLE_SYNCH the pitch-kernel table [nlogb][nfreq][nb],
+ * CROMA_EMIS_TABLE_IC the IC table [nbins_ic][nb] of the last run's z. */
+enum { CROMA_EMIS_TABLE_SYNCH = 0, CROMA_EMIS_TABLE_IC = 1 };
+int croma_b200_emission_table(CromaB200Context *ctx, int which, double *out);
+
+/* One snapshot step of the resident pipeline through host memory: the
+ * per-snapshot sequence of the reference's driver (include/tracer_fp_solve.inc:
+ * DSA injection :76-101, emission :117-426, evolve :677-1526) with the
+ * snapshot's inputs (backgrounds, shock fields) read from host memory and its
+ * outputs (emissivities, evolved spectra) written to host memory, while the
+ * spectra stay resident.  The emissivities come back on a copy stream while
+ * the evolve runs, the evolved spectra workspace chunk by workspace chunk as
+ * each finishes; page-locked host buffers let the copies overlap.
+ * snap: host backgrounds (bg_on_device = 0).  Synchronous. */
+typedef struct {
+    const CromaB200Shocks *shocks;     /* host shock fields; NULL or dsa_mode OFF: no injection */
+    int dsa_mode, dsa_reacc;           /* CROMA_DSA_*, CROMA_DSA_REACC_* */
+    double density_unit;
+    double *eps_syn, *eps_ic, *eps_gamma, *eps_nu;   /* host [ntracer][bins] or NULL */
+    double *crp_out, *cre_out;                        /* host [ntracer][nb] or NULL */
+} CromaB200StepHost;
+int croma_b200_step_host(CromaB200Context *ctx, const CromaB200Snapshot *snap, const CromaB200StepHost *io);
+
+/* Page-locked host memory of exactly `bytes` (cudaHostAlloc, portable), for
+ * the host-buffer calls above, whose copies overlap the kernels only from
+ * page-locked memory; released by croma_b200_host_free (which waits for the
+ * device). */
+int croma_b200_host_alloc(size_t bytes, void **out);
+int croma_b200_host_free(void *p);
+
 /* FP64 FMA throughput of the current device, measured by a kernel of
  * independent fused multiply-add chains on every SM (TFLOP/s, FMA = 2 flops);
  * the denominator of the fused evolve's roofline. */

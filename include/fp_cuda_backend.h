@@ -270,6 +270,28 @@ int prepare_ic_emission_cuda_batch(const FpIcEmissionBatchInput *in,
                                    const CRspectrum *cre_grid,
                                    double *eps_ic_out,
                                    double *elapsed_ms);
+/* Device forms of the host routines that build the emission kernel tables
+ * (no CUDA counterpart in the reference; its CPU code builds them once per
+ * run, the IC table once per emitted snapshot).  Host grid in, host table
+ * out, [nbins][np] (gamma, neutrino: proton grid) or [nbins][npe] (IC:
+ * electron grid), band k at 10^(lo + k d), d = (hi - lo) / nbins, accumulated
+ * as the reference does.
+ *   prepare_gamma_kernel_flat     src/fp_shared_core.c:1724-1749 (gammaKernel, src/HADRONIC.c:139-177)
+ *   prepare_neutrino_kernel_flat  src/fp_shared_core.c:1751-1778 (eKernel + numu1Kernel, src/HADRONIC.c:181-289)
+ *   prepare_ic_kernel_flat        src/fp_shared_core.c:1780-1807 (IC_emissivity_kernel, src/FP_Coef.c:553-584) */
+int prepare_gamma_kernel_flat_cuda(const CRspectrum *crp, int nbins, double egamma_min, double egamma_max,
+                                   double *fga_flat);
+int prepare_neutrino_kernel_flat_cuda(const CRspectrum *crp, int nbins, double enu_min, double enu_max,
+                                      double *fnu_flat);
+int prepare_ic_kernel_flat_cuda(const CRspectrum *cre, int nbins, double nu_min, double nu_max, double z,
+                                double *fic_flat);
+/* The log10 F(x) column of SYN_logFx_table (src/Synchrotron.c:31-41) on the
+ * device: F(x) = x int_x^inf K_5/3(s) ds for x <= 300 from the integral
+ * definition (the reference calls GNU GSL's gsl_sf_synchrotron_1 there; GSL
+ * is not part of this library), sqrt(pi/2) exp(-x) sqrt(x) above, as the
+ * reference does. */
+int synch_logfx_table_cuda(int nx, const double *logx, double *logfx_out);
+
 int prepare_gamma_emission_cuda_batch(const FpGammaEmissionBatchInput *in,   /* :102-105 */
                                       const CRspectrum *crp_grid,
                                       double *eps_gamma_out,

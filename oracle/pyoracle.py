@@ -368,6 +368,11 @@ class ReferenceCPU(_Common):
         L.ref_ckpt_read.argtypes = [_s, _i, _i, _i, _i, _i, _i, _l, _vp, _vp, _vp, _i, _i, C.POINTER(_i)]
         L.ref_synch_emission.argtypes = [_i, _i, _i, _i, _i, _d, _d, _d, _D, _D, _D, _D, _D, _vp, _D, _D,
                                          _D, _D]
+        L.ref_gamma_kernel_table.argtypes = [_i, _d, _d, _D]
+        L.ref_nu_kernel_table.argtypes = [_i, _d, _d, _D]
+        L.ref_ic_kernel_table.argtypes = [_i, _d, _d, _d, _D]
+        L.ref_hadronic_emission.argtypes = [_i, _i, _i, _d, _d, _D, _D, _D, _D]
+        L.ref_synch_run.argtypes = [_i, _d, _d, _i, _i, _d, _d, _i, _vp, _vp] + [_vp] * 9
         self.cfg = cfg
         self.nb = cfg.nb
         self.configure(threads)
@@ -424,6 +429,50 @@ class ReferenceCPU(_Common):
                                        _as_d(w), _ptr(tab), _as_d(b_dyn), _as_d(logb), cre, out) != 0:
             raise RuntimeError("ref_synch_emission failed")
         return out
+
+    def kernel_table(self, kind: str, nbins: int, lo: float, hi: float, z: float = 0.0):
+        """prepare_{gamma,neutrino,ic}_kernel_flat: [nbins][nb]."""
+        out = np.empty((nbins, self.nb))
+        if kind == "gamma":
+            rc = self.lib.ref_gamma_kernel_table(nbins, lo, hi, out)
+        elif kind == "nu":
+            rc = self.lib.ref_nu_kernel_table(nbins, lo, hi, out)
+        else:
+            rc = self.lib.ref_ic_kernel_table(nbins, lo, hi, z, out)
+        if rc != 0:
+            raise RuntimeError(f"ref kernel table {kind} failed")
+        return out
+
+    def hadronic_emission(self, kind: str, crp, n_gas, kern, lo: float, hi: float):
+        """prepare_{gamma,neutrino}_emission_cell_major: [ncell][nbins]."""
+        crp = np.ascontiguousarray(crp, np.float64)
+        kern = np.ascontiguousarray(kern, np.float64)
+        out = np.empty((crp.shape[0], kern.shape[0]))
+        if self.lib.ref_hadronic_emission(0 if kind == "gamma" else 1, crp.shape[0], kern.shape[0], lo, hi,
+                                          _as_d(n_gas), crp, kern, out) != 0:
+            raise RuntimeError("ref hadronic emission failed")
+        return out
+
+    def synch_run(self, nfreq, nu_min, nu_max, ntheta, nlogb=512, logb_min=-6.0, logb_max=2.0,
+                  b_field=None, cre=None, tables=True):
+        """The reference's synchrotron tables (tracer_fp_synch_data_init_tables,
+        tracer_fp_refresh_synch_kernel_table) and, given b_field and cre,
+        prepare_synch_emission_cell_major.  Returns a dict of arrays."""
+        nx = 2750
+        r = {k: np.empty(nx) for k in ("logx", "logfx", "fx")}
+        r["theta"], r["w"], r["nus"] = np.empty(ntheta), np.empty(ntheta), np.empty(nfreq)
+        r["logy"] = np.empty((nfreq, self.nb, ntheta)) if tables else None
+        r["table"] = np.empty((nlogb, nfreq, self.nb)) if tables else None
+        ncell = 0 if cre is None else cre.shape[0]
+        r["eps"] = np.empty((ncell, nfreq)) if ncell else None
+        cre_c = None if cre is None else np.ascontiguousarray(cre, np.float64)
+        b_c = None if b_field is None else np.ascontiguousarray(b_field, np.float64)
+        outs = [r[k] for k in ("logx", "logfx", "fx", "theta", "w", "nus", "logy", "table", "eps")]
+        rc = self.lib.ref_synch_run(nfreq, nu_min, nu_max, ntheta, nlogb, logb_min, logb_max, ncell,
+                                    _ptr(b_c), _ptr(cre_c), *[_ptr(o) for o in outs])
+        if rc != 0:
+            raise RuntimeError(f"ref_synch_run failed: {rc}")
+        return r
 
     def threads(self) -> int:
         return self.lib.ref_threads()

@@ -577,6 +577,135 @@ int ref_synch_emission(int ncell, int nfreq, int nx, int ntheta, int nlogb, doub
     return rc;
 }
 
+/* ---- emission kernel tables and full emission through the reference ----
+ * ref_gamma_kernel_table / ref_nu_kernel_table / ref_ic_kernel_table run
+ * prepare_{gamma,neutrino,ic}_kernel_flat (src/fp_shared_core.c:1724-1807);
+ * ref_hadronic_emission runs prepare_{gamma,neutrino}_emission_cell_major
+ * (:2166-2243) with the grid's beta_p.  ref_synch_run builds the reference's
+ * SynchData with tracer_fp_synch_data_init_tables (src/tracer_fp_synch.c:87-121;
+ * its F(x) column comes from oracle/synch_fx.c through the GSL stand-in), the
+ * pitch-kernel table of tracer_fp_refresh_synch_kernel_table (:175-240, fixed
+ * log-B range) and prepare_synch_emission_cell_major (:2070-2129) on b_dyn,
+ * as include/tracer_fp_solve.inc:117-186 does; every table is returned. */
+int ref_gamma_kernel_table(int nbins, double emin, double emax, double *out)
+{
+    if (!g_ready || nbins <= 0 || !out) return -1;
+    prepare_gamma_kernel_flat(&g_crp, nbins, emin, emax, out);
+    return 0;
+}
+
+int ref_nu_kernel_table(int nbins, double emin, double emax, double *out)
+{
+    if (!g_ready || nbins <= 0 || !out) return -1;
+    prepare_neutrino_kernel_flat(&g_crp, nbins, emin, emax, out);
+    return 0;
+}
+
+int ref_ic_kernel_table(int nbins, double nu_min, double nu_max, double z, double *out)
+{
+    if (!g_ready || nbins <= 0 || !out) return -1;
+    prepare_ic_kernel_flat(&g_cre, nbins, nu_min, nu_max, z, out);
+    return 0;
+}
+
+/* kind 0 gamma, 1 neutrino */
+int ref_hadronic_emission(int kind, int ncell, int nbins, double emin, double emax, const double *n_gas,
+                          const double *crp, const double *kern, double *eps_out)
+{
+    if (!g_ready || ncell <= 0 || nbins <= 0) return -1;
+    if (kind == 0) {
+        FpGammaEmissionBatchInput in;
+        memset(&in, 0, sizeof in);
+        in.ncell = ncell; in.nbins = nbins; in.egamma_min = emin; in.egamma_max = emax;
+        in.n_gas = n_gas; in.crp_batch = crp; in.beta_p = g_beta_p; in.fga_flat = kern;
+        return prepare_gamma_emission_cell_major(&in, &g_crp, eps_out);
+    } else {
+        FpNeutrinoEmissionBatchInput in;
+        memset(&in, 0, sizeof in);
+        in.ncell = ncell; in.nbins = nbins; in.enu_min = emin; in.enu_max = emax;
+        in.n_gas = n_gas; in.crp_batch = crp; in.beta_p = g_beta_p; in.fnu_flat = kern;
+        return prepare_neutrino_emission_cell_major(&in, &g_crp, eps_out);
+    }
+}
+
+/* Outputs (any may be NULL): logx/logfx/fx [2750], theta/w [ntheta],
+ * nus [nfreq], logy [nfreq][npe][ntheta], table [nlogb][nfreq][npe],
+ * eps [ncell][nfreq] (ncell > 0 with b_field and cre). */
+int ref_synch_run(int nfreq, double nu_min, double nu_max, int ntheta, int nlogb, double logb_min,
+                  double logb_max, int ncell, const double *b_field, const double *cre,
+                  double *logx, double *logfx, double *fx, double *theta, double *w, double *nus,
+                  double *logy, double *table, double *eps)
+{
+    SynchData sd;
+    int rc = 0, nlogb_saved = 0;
+    double *b_dyn = 0, *lb = 0, lbmin = 0.0, lbmax = 0.0;
+    int nout = 0;
+    (void)nlogb_saved;
+    if (!g_ready || nfreq <= 0 || ntheta <= 0) return -1;
+    if (nlogb != TRACER_FP_SYNCH_LOGB_BINS) return -2;   /* the reference's table has a fixed plane count */
+    nu_min_s = nu_min;
+    nu_max_s = nu_max;
+    tracer_synch_ntheta_pitch = ntheta;
+    tracer_synch_logb_min = logb_min;
+    tracer_synch_logb_max = logb_max;
+    adaptive_synch_logb = 0;
+    tracer_fp_synch_data_reset(&sd);
+    if (tracer_fp_synch_data_alloc(&sd, nfreq) != 0 ||
+        tracer_fp_synch_data_init_tables(&sd, nfreq, &g_cre) != 0) {
+        tracer_fp_synch_data_release(&sd);
+        return -1;
+    }
+    if (logx) memcpy(logx, sd.logx_tab, (size_t)sd.nx_tab * sizeof(double));
+    if (logfx) memcpy(logfx, sd.logfx_tab, (size_t)sd.nx_tab * sizeof(double));
+    if (fx) memcpy(fx, sd.fx_tab, (size_t)sd.nx_tab * sizeof(double));
+    if (theta) memcpy(theta, sd.theta, (size_t)ntheta * sizeof(double));
+    if (w) memcpy(w, sd.pitch_weight, (size_t)ntheta * sizeof(double));
+    if (nus) memcpy(nus, sd.nus, (size_t)nfreq * sizeof(double));
+    if (logy) memcpy(logy, sd.logy_storage, (size_t)nfreq * (size_t)npe * (size_t)ntheta * sizeof(double));
+    if (tracer_fp_refresh_synch_kernel_table(&sd, nfreq, 0.0, 0.0, &sd.kernel_table) != 0) {
+        tracer_fp_synch_data_release(&sd);
+        return -1;
+    }
+    if (table) memcpy(table, sd.kernel_table, (size_t)nlogb * (size_t)nfreq * (size_t)npe * sizeof(double));
+    if (ncell > 0 && b_field && cre && eps) {
+        FpSynchEmissionBatchInput in;
+        int i;
+        b_dyn = (double *)malloc((size_t)ncell * sizeof(double));
+        lb = (double *)malloc((size_t)ncell * sizeof(double));
+        if (!b_dyn || !lb) { rc = -1; goto done; }
+        for (i = 0; i < ncell; i++) b_dyn[i] = b_field[i];
+        tracer_fp_logb_range_from_snapshot(ncell, b_dyn, lb, &lbmin, &lbmax, &nout);
+        memset(&in, 0, sizeof in);
+        in.ncell = ncell;
+        in.nfreq = nfreq;
+        in.nx_tab = sd.nx_tab;
+        in.ntheta_pitch = sd.ntheta_pitch;
+        in.nlogb = TRACER_FP_SYNCH_LOGB_BINS;
+        in.xmin = sd.xmin;
+        in.logb_min = sd.table_logb_min;
+        in.inv_dlogb = (double)(TRACER_FP_SYNCH_LOGB_BINS - 1) / (sd.table_logb_max - sd.table_logb_min);
+        in.fx_tab = sd.fx_tab;
+        in.logfx_tab = sd.logfx_tab;
+        in.logx_tab = sd.logx_tab;
+        in.logy = sd.logy_planes;
+        in.pitch_kernel_table = sd.kernel_table;
+        in.b_dyn = b_dyn;
+        in.logb = lb;
+        in.cre_batch = cre;
+        in.gamma2e = g_gamma2e;
+        in.theta = sd.theta;
+        in.dtheta = sd.dtheta;
+        in.pitch_weight = sd.pitch_weight;
+        in.nus = sd.nus;
+        rc = prepare_synch_emission_cell_major(&in, &g_cre, eps);
+    }
+done:
+    free(b_dyn);
+    free(lb);
+    tracer_fp_synch_data_release(&sd);
+    return rc;
+}
+
 /* ---- output files and checkpoints (src/tracer_fp_output.c,
  * src/tracer_fp_restart.c) on caller arrays, for byte comparisons --------
  * Open writers live in a small table indexed by the returned handle. */

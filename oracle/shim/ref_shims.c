@@ -11,9 +11,9 @@
  *   (src/Chang_Cooper.c:257-269), an analytic test solution that the hot
  *   path never calls.  They return NaN.
  * - gsl_sf_synchrotron_1: only reached from SYN_logFx_table
- *   (src/Synchrotron.c:31-41) when synchrotron tables are built; the
- *   emission checks pass the same F(x) table to both sides, so this stub
- *   aborts if it is ever reached.
+ *   (src/Synchrotron.c:31-41) when synchrotron tables are built; it returns
+ *   the checker's F(x) = x int_x^inf K_5/3 restated from the integral
+ *   definition (oracle/synch_fx.c), so the reference's table code runs.
  * - luminosity_distance_mpc: only used by the file writers
  *   (src/EMISSION.c:152, 250), which the checker never calls.
  */
@@ -51,11 +51,7 @@ double gsl_sf_gamma(double x) { (void)x; return NAN; }
 double gsl_sf_hyperg_1F1(double a, double b, double x) { (void)a; (void)b; (void)x; return NAN; }
 double gsl_sf_hyperg_U(double a, double b, double x) { (void)a; (void)b; (void)x; return NAN; }
 
-double gsl_sf_synchrotron_1(double x)
-{
-    (void)x;
-    fprintf(stderr, "oracle/_ref: gsl_sf_synchrotron_1 is not available in this build\n");
-    abort();
-}
+double oracle_synch_fx(double x);
+double gsl_sf_synchrotron_1(double x) { return oracle_synch_fx(x); }
 
 double luminosity_distance_mpc(double z) { (void)z; return NAN; }

@@ -210,8 +210,57 @@ def make_synch_emission(name="emission_synch"):
     print(name, "written")
 
 
+# Emission tables of the config-4 kind at a small size: band grids as
+# config 4 states them (1 keV .. 1 PeV for gamma / neutrino in log10 GeV, the
+# same photon energies for IC in log10 Hz, synchrotron 10 MHz .. 10 GHz).
+EMIS_TABLES = dict(nb=128, nbins=16, egamma=(-6.0, 6.0), enu=(-6.0, 6.0),
+                   nu_ic=(17.383, 29.383), z_ic=0.5, nfreq=8, nu_s=(7.0, 10.0), ntheta=32, nlogb=512,
+                   logb=(-6.0, 2.0), plane_stride=16, ncell=12)
+
+
+def make_emission_tables(name="emission_tables"):
+    """The reference's own kernel tables (prepare_gamma/neutrino/ic_kernel_flat),
+    synchrotron tables (tracer_fp_synch_data_init_tables with the checker's
+    F(x) in place of GSL's, the pitch-kernel table of
+    tracer_fp_refresh_synch_kernel_table over the default log-B range) and
+    emissivities (prepare_*_emission_cell_major) on 128-bin e+p spectra,
+    some electron spectra cut off so that the synchrotron stop rule acts.
+    Every plane_stride-th log-B plane of the pitch table is kept."""
+    e = EMIS_TABLES
+    nb, nbins = e["nb"], e["nbins"]
+    cfg = config.config1(nb=nb)
+    ref = pyoracle.ReferenceCPU(cfg)
+    gp, ge = ref.grid(0), ref.grid(1)
+    crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), e["ncell"], cfg.species)
+    rng = np.random.default_rng(4401)
+    crp = crp * rng.uniform(0.5, 2.0, (e["ncell"], 1))
+    cre = cre * rng.uniform(0.5, 2.0, (e["ncell"], 1))
+    for i, cut in enumerate((100, 121, 3, 127)):
+        cre[i, cut:] = 0.0
+    bg = synth.background(e["ncell"], 7, 4402)
+    n_gas, b_field = bg[0].copy(), bg[2].copy()
+    b_field[5] = 0.0   # a non-positive field takes the 1e-30 G floor
+    out = dict(nb=nb, cre=cre, crp=crp, n_gas=n_gas, b_field=b_field, dp_e=ge[1], dp_p=gp[1], p_e=ge[0],
+               p_p=gp[0])
+    out["fga"] = ref.kernel_table("gamma", nbins, *e["egamma"])
+    out["fnu"] = ref.kernel_table("nu", nbins, *e["enu"])
+    out["fic"] = ref.kernel_table("ic", nbins, *e["nu_ic"], z=e["z_ic"])
+    out["eps_gamma"] = ref.hadronic_emission("gamma", crp, n_gas, out["fga"], *e["egamma"])
+    out["eps_nu"] = ref.hadronic_emission("nu", crp, n_gas, out["fnu"], *e["enu"])
+    fic2, out["eps_ic"] = ref.ic_emission(cre, nbins, e["z_ic"], *e["nu_ic"])
+    assert np.array_equal(fic2, out["fic"])
+    r = ref.synch_run(e["nfreq"], *e["nu_s"], e["ntheta"], e["nlogb"], *e["logb"], b_field=b_field, cre=cre)
+    for k in ("logx", "logfx", "fx", "theta", "w", "nus", "logy"):
+        out["syn_" + k] = r[k]
+    out["syn_table_planes"] = r["table"][::e["plane_stride"]].copy()
+    out["eps_syn"] = r["eps"]
+    out["params"] = json.dumps(e)
+    np.savez_compressed(os.path.join(HERE, f"golden_{name}.npz"), **out)
+    print(name, "written")
+
+
 if __name__ == "__main__":
-    names = sys.argv[1:] or list(CASES) + list(DSA_CASES) + ["emission_ic", "emission_synch"]
+    names = sys.argv[1:] or list(CASES) + list(DSA_CASES) + ["emission_ic", "emission_synch", "emission_tables"]
     for n in names:
         if n in DSA_CASES:
             make_dsa_case(n, DSA_CASES[n])
@@ -219,5 +268,7 @@ if __name__ == "__main__":
             make_ic_emission(n)
         elif n == "emission_synch":
             make_synch_emission(n)
+        elif n == "emission_tables":
+            make_emission_tables(n)
         else:
             make_case(n, CASES[n])
