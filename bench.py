@@ -347,34 +347,37 @@ def run_e2e(fp, cfg, nt, w, bgs, shocks, snaps, steps):
 
 
 # ---------------------------------------------------------------- accuracy and CPU baseline
-def accuracy_and_cpu(cfg, w, bgs, shocks, snaps, ntr, nsnap, threads=0):
+def accuracy_and_cpu(cfg, w, bgs, shocks, snaps, ntr, nsnap, paths=("fused", "fp32r"), threads=0):
     """The first ntr tracers of the workload through nsnap consecutive steps
     (DSA tracer_state + snapshot) on the reference's own CPU code (oracle/_ref,
     all host threads; the restatement where the reference was not built) and
-    on the GPU (fused path, same inputs): per snapshot the max and median
-    relative error over bins above 1e-12 of each tracer's peak, the largest
-    particle-number drift and the nsub mismatches; emission of the first
-    snapshot (IC with the reference's own table, gamma / neutrino integrals
-    of the reference on the device-built tables).  The reference's time per
-    step is the CPU baseline."""
+    on the GPU (each path in `paths`, same inputs, in lockstep): per
+    snapshot the max and median relative error over bins above 1e-12 of each
+    tracer's peak, the largest particle-number drift and the nsub mismatches;
+    emission of the first snapshot (fused path: IC with the reference's own
+    table, gamma / neutrino integrals of the reference on the device-built
+    kernel tables).  The reference's time per step is the CPU baseline."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    from croma_fp_b200 import config, native
+    from croma_fp_b200 import config, native, synth
     kind = "reference" if pyoracle.reference_available(cfg.nb) else "port"
     ref = pyoracle.ReferenceCPU(cfg, threads=threads) if kind == "reference" else pyoracle.Oracle(cfg)
     cores = ref.threads() if kind == "reference" else 1
     gp, ge = ref.grid(0), ref.grid(1)
-    from croma_fp_b200 import synth
     crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), ntr, cfg.species)
     qpi, qepri = np.zeros_like(crp), np.zeros_like(cre)
     dis = np.zeros(ntr, np.uint8)
     mass = np.full(ntr, 1.0e7)
-    fp = native.TracerFP(cfg, path="fused")
-    crp1, cre1 = seed_rows(fp, cfg)
-    fp.set_state_broadcast(ntr, crp1, cre1, 1.0e7)
-    fp.set_dsa(config.DsaParams())
-    fp.emission_setup(**native.EMISSION_CONFIG4)
-    per_snap, t_ref, emis = [], 0.0, None
+    fps = {}
+    for p in paths:
+        fp = native.TracerFP(cfg, path=p)
+        crp1, cre1 = seed_rows(fp, cfg)
+        fp.set_state_broadcast(ntr, crp1, cre1, 1.0e7)
+        fp.set_dsa(config.DsaParams())
+        fps[p] = fp
+    fps[paths[0]].emission_setup(**native.EMISSION_CONFIG4)
+    per_snap = {p: [] for p in paths}
+    t_ref, emis = 0.0, None
     try:
         for k in range(nsnap):
             isnap = snaps[k]
@@ -383,27 +386,31 @@ def accuracy_and_cpu(cfg, w, bgs, shocks, snaps, ntr, nsnap, threads=0):
             t0 = time.perf_counter()
             ref.dsa_inject(config.DsaParams(), sh, mass, 1.0, float(w.dt[isnap]), 1, 0, crp, cre, qpi, qepri, dis)
             t_dsa = time.perf_counter() - t0
-            fp.dsa_inject(sh, 1.0, float(w.dt[isnap]), "tracer_state")
+            for fp in fps.values():
+                fp.dsa_inject(sh, 1.0, float(w.dt[isnap]), "tracer_state")
             if k == 0:
-                emis = emission_check(ref, fp, cfg, bgc, cre, crp, float(w.z[isnap]), kind)
+                emis = emission_check(ref, fps[paths[0]], cfg, bgc, cre, crp, float(w.z[isnap]), kind)
             t0 = time.perf_counter()
             nsub, _, _, _ = ref.snapshot(bgc, bgn, float(w.z[isnap]), float(w.z[isnap + 1]), True, float(w.dt[isnap]),
                                          float(w.elapsed[isnap]), qpi, qepri, crp, cre, mass=mass, dis=dis)
             t_ref += t_dsa + time.perf_counter() - t0
-            fp.snapshot(bgc, bgn, float(w.z[isnap]), float(w.z[isnap + 1]), True, float(w.dt[isnap]),
-                        float(w.elapsed[isnap]), sync=True)
-            g_crp, g_cre = fp.get_state()
-            per_snap.append(compare_spectra(g_crp, g_cre, crp, cre, gp[1], ge[1], fp.schedule()["nsub"], nsub))
+            for p, fp in fps.items():
+                fp.snapshot(bgc, bgn, float(w.z[isnap]), float(w.z[isnap + 1]), True, float(w.dt[isnap]),
+                            float(w.elapsed[isnap]), sync=True)
+                g_crp, g_cre = fp.get_state()
+                per_snap[p].append(compare_spectra(g_crp, g_cre, crp, cre, gp[1], ge[1], fp.schedule()["nsub"], nsub))
     finally:
-        fp.close()
+        for fp in fps.values():
+            fp.close()
     acc = {"vs": f"reference CPU ({kind}) on the first {ntr} tracers, {nsnap} consecutive snapshots "
-                 f"(DSA tracer_state + snapshot)", "tracers": ntr, "snapshots": nsnap,
-           "max_rel_err": max(p["max_rel_err"] for p in per_snap),
-           "median_rel_err": float(np.median([p["median_rel_err"] for p in per_snap])),
-           "max_particle_number_drift": max(p["drift"] for p in per_snap),
-           "nsub_mismatches": int(sum(p["nsub_mismatches"] for p in per_snap)),
-           "per_snapshot_max_rel_err": [p["max_rel_err"] for p in per_snap],
-           "emission_first_snapshot": emis, "bar": 1e-6}
+                 f"(DSA tracer_state + snapshot)", "tracers": ntr, "snapshots": nsnap, "bar": 1e-6,
+           "emission_first_snapshot": emis}
+    for p, ps in per_snap.items():
+        acc[p] = {"max_rel_err": max(x["max_rel_err"] for x in ps),
+                  "median_rel_err": float(np.median([x["median_rel_err"] for x in ps])),
+                  "max_particle_number_drift": max(x["drift"] for x in ps),
+                  "nsub_mismatches": int(sum(x["nsub_mismatches"] for x in ps)),
+                  "per_snapshot_max_rel_err": [x["max_rel_err"] for x in ps]}
     cpu = {"value": ntr * nsnap / t_ref, "unit": UNIT, "cores": cores, "kind": kind,
            "sample": f"{ntr} tracers x {nsnap} consecutive snapshots (DSA tracer_state + IC rows + nsub + "
                      f"buckets + evolve; no emission) in {t_ref:.1f} s"}
@@ -652,6 +659,7 @@ def run_gpu_arm(args):
                       "down every step, copies overlapped with the kernels",
                "steps": len(r["times"]), "ms_per_step": e2e_s * 1e3}
     fp64_peak = native.fp64_peak(cfg.nb)
+    tuning = {"protons": fp.tuning(0), "electrons": fp.tuning(1)}
     fp.close()
     del _eps
     torch.cuda.empty_cache()
@@ -667,6 +675,17 @@ def run_gpu_arm(args):
                  "warmup": args.plain_warmup, "chosen_over_plain": value / pv,
                  "roofline": roofline_plain(cfg, nt, pr, args.plain_steps, peaks, peak_kind),
                  "note": "same steps, inputs and emission; the evolve runs the reference's per-step data contract"}
+    fp32r = None
+    if not args.no_fp32r:
+        fr = run_resident("fp32r", cfg, nt, w, bg_dev, sh_dev, snaps, 1, args.fp32r_steps,
+                          emission=not args.no_emission, kernel_timing=True)
+        fv = world * nt * args.fp32r_steps / (fr["ms"] / 1e3)
+        fp32r = {"value": fv, "ms_per_step": fr["ms"] / args.fp32r_steps, "steps": args.fp32r_steps, "warmup": 1,
+                 "over_fused_fp64": fv / value, "over_plain": (fv / plain["value"]) if plain else None,
+                 "steps_kernel_ms_per_step": fr["evolve"][0] / args.fp32r_steps,
+                 "fused_fp64_steps_kernel_ms_per_step": res["evolve"][0] / args.steps,
+                 "note": "each sub-step solved in FP32 and refined once with an FP64 residual; factors, CC "
+                         "weights, spectra and particle budget FP64; accuracy in accuracy.fp32r"}
     peaks, peak_kind = measured_peaks()
     roofline = roofline_fused(cfg, nt, res, args.steps, fp64_peak, peaks, peak_kind)
     del bg_dev, sh_dev
@@ -681,19 +700,18 @@ def run_gpu_arm(args):
                    "sample": f"{type(e).__name__}: {e}"}
     secondary = None
     if rank == 0 and world == 1 and not args.no_secondary:
-        secondary = {"config1": run_config1(args)}
+        secondary = {"config1": run_config1(args), "heavy_tail": run_heavy_tail(args)}
     serving = None
     if rank == 0 and world == 1 and args.serving_requests > 0:
-        from croma_fp_b200 import serve_bench
-        serving = serve_bench.run(nrequests=args.serving_requests)
+        serving = run_serving(args)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": dict(workload_desc(nt), parallelism=f"dp{world} (independent tracer shards)",
                            path="fused (on-chip FP64)"),
-            "e2e": e2e, "plain": plain, "roofline": roofline, "cpu_baseline": cpu, "accuracy": acc,
-            "clocks": res["clocks"], "gpu_launches": int(res["launches"]),
+            "e2e": e2e, "plain": plain, "fp32r": fp32r, "roofline": roofline, "cpu_baseline": cpu, "accuracy": acc,
+            "autotuner": tuning, "clocks": res["clocks"], "gpu_launches": int(res["launches"]),
             "kernel_ms": {"evolve": res["evolve"][0], "coeff": res["coeff"][0], "secondary": res["secondary"][0],
                           "emission": res["emission_ms"]},
             "dsa_injected_per_step": res["dsa_injected_per_step"], "nsub": res["nsub"], "nbuckets": res["nbuckets"],
@@ -703,6 +721,48 @@ def run_gpu_arm(args):
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def run_heavy_tail(args):
+    """Uneven sub-step counts: the config-0 background distributions on an
+    electron grid over p/(m_e c) in [10, 1000] (128 bins, electron-only,
+    direct t_acc), whose nsub spread from 11 to the cap of 500 with a heavy
+    tail (median ~12, 90th percentile ~200-370), against the same tracers on
+    the full [0.1, 1e6] grid where every nsub is 500.  Reported: throughput,
+    the nsub distribution, sub-step rate (sum of nsub x nb per second) and
+    its ratio to the uniform workload's (the balance of uneven work)."""
+    import torch
+    from croma_fp_b200 import config, synth
+    nt = args.heavy_tail_tracers
+    out = {}
+    for name, cfg in (("heavy_tail", config.config0(pemin=1.0, pemax=3.0, nsub_max=500)),
+                      ("uniform", config.config0(nsub_max=500))):
+        w = synth.Workload(cfg, nt, NSNAP_TIMELINE, seed=SEED + 17)
+        snaps = [45 + k for k in range(6)]
+        bg = torch.stack([torch.from_numpy(w.background(s_)) for s_ in range(snaps[0], snaps[-1] + 2)]).cuda()
+        r = run_resident("fused", cfg, nt, w, bg, None, snaps, 2, 4, emission=False, dsa=False)
+        nsub = r["sched"]["nsub"].astype(np.float64)
+        rate = float(np.sum(nsub)) * cfg.nb * 4 / (r["ms"] / 1e3)
+        out[name] = {"value": nt * 4 / (r["ms"] / 1e3), "ms_per_step": r["ms"] / 4,
+                     "nsub_percentiles_0_10_50_90_99_100": [float(x) for x in
+                                                            np.percentile(nsub, [0, 10, 50, 90, 99, 100])],
+                     "substep_row_rate": rate}
+        del bg
+    out["balance"] = out["heavy_tail"]["substep_row_rate"] / out["uniform"]["substep_row_rate"]
+    out["workload"] = (f"{nt} tracers, electron-only, 128 bins, direct t_acc 0.3 Gyr; heavy_tail: electron grid "
+                       f"[10, 1e3], uniform: [0.1, 1e6]; 4 timed snapshots after 2")
+    return out
+
+
+def run_serving(args):
+    """Config 3: a Poisson stream of requests through the request server,
+    once per evolve path on the same arrival stream; p50 / p99 latency and
+    throughput per path."""
+    from croma_fp_b200 import serve_bench
+    out = {}
+    for path in args.serving_paths.split(","):
+        out[path] = serve_bench.run(nrequests=args.serving_requests, path=path)
+    return out
 
 
 def run_config1(args):
@@ -737,15 +797,24 @@ def main():
     ap.add_argument("--accuracy-tracers", type=int, default=4096)
     ap.add_argument("--accuracy-snaps", type=int, default=5)
     ap.add_argument("--reference-tracers", type=int, default=4096)
+    ap.add_argument("--fp32r-steps", type=int, default=3)
+    ap.add_argument("--no-fp32r", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-emission", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--heavy-tail-tracers", type=int, default=262144)
     ap.add_argument("--serving-requests", type=int, default=48)
+    ap.add_argument("--serving-paths", default="fused", help="comma-separated: fused, fp32r, plain")
+    ap.add_argument("--serving-only", action="store_true", help="run only the serving workload, one JSON line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.serving_only:
+        load_package()
+        print(json.dumps({"serving": run_serving(args)}), flush=True)
+        return 0
     return run_gpu_arm(args)
 
 

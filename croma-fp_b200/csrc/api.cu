@@ -164,7 +164,10 @@ int croma_b200_create(const CromaB200Config *cfg, int device, CromaB200Context *
 {
     if (cfg == nullptr || out == nullptr) { set_error("null argument"); return -1; }
     if (cfg->nb != NB) { set_error("config nb does not match this library's bin count"); return -1; }
-    if (cfg->path != CROMA_PATH_PLAIN && cfg->path != CROMA_PATH_FUSED) { set_error("unknown path"); return -1; }
+    if (cfg->path != CROMA_PATH_PLAIN && cfg->path != CROMA_PATH_FUSED && cfg->path != CROMA_PATH_FUSED_FP32R) {
+        set_error("unknown path");
+        return -1;
+    }
     if (cfg->dpp_model < 1 || cfg->dpp_model > 4) { set_error("unknown dpp_model"); return -1; }
     if ((cfg->species_mask & 3) == 0) { set_error("empty species mask"); return -1; }
     int ndev = 0;
@@ -817,6 +820,18 @@ __global__ void fp64_fma_probe(int iters, double seed, double *out)
 }  // namespace croma_probe
 
 extern "C" {
+
+int croma_b200_get_tuning(CromaB200Context *h, int species, int *tuned, int *solver, int *warps_per_block,
+                          double *variant_ms)
+{
+    if (!h || species < 0 || species > 1) { set_error("invalid get_tuning arguments"); return -1; }
+    const Context &c = h->impl;
+    const int t = tuning_info(c, species, solver, warps_per_block);
+    if (tuned) *tuned = t;
+    if (variant_ms)
+        for (int v = 0; v < 4; v++) variant_ms[v] = c.tune[species].ms[v];
+    return 0;
+}
 
 int croma_b200_host_alloc(size_t bytes, void **out)
 {

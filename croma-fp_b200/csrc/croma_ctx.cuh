@@ -75,6 +75,16 @@ struct ModelParams {
     double f_eddy, t_off_gyr, t_acc_off_gyr;
 };
 
+// The steps-kernel autotuner's record for one species (fused.cu): the
+// variant chosen (solver and warps per block, index into the tuner's list)
+// and the calibration time of each variant (-1: not run).
+struct TuneState {
+    int tuned = 0;
+    int variant = 0;
+    int tracers = 0, steps = 0;
+    double ms[4] = {-1.0, -1.0, -1.0, -1.0};
+};
+
 struct Context {
     CromaB200Config cfg{};
     ModelParams mp{};
@@ -151,6 +161,9 @@ struct Context {
     cudaEvent_t pipe_start = nullptr;   // compute stream's earlier work, gating the uploads
     const HostPipe *pipe = nullptr;
 
+    // steps-kernel autotuner, per species
+    TuneState tune[2];
+
     // resident emission tables (croma_b200_emission_setup)
     EmissionState *emission = nullptr;
 
@@ -213,6 +226,9 @@ int fused_reserve(Context &ctx, int cap);
 // on path CROMA_PATH_*
 double fused_workspace_bytes(const ModelParams &mp, int cap, double workspace_cap, int path);
 int run_fused(Context &ctx, const SnapArgs &a);
+// the autotuner's choice for a species: solver (0 scan, 1 FP32-refined scan,
+// 2 PCR) and warps per block; returns 1 once tuned
+int tuning_info(const Context &ctx, int species, int *solver, int *wpb);
 // dsa.cu
 int set_dsa(Context &ctx, const CromaB200DsaParams *prm);
 int dsa_inject(Context &ctx, const CromaB200Shocks *sh, double density_unit, double dt_gyr, int mode,

@@ -36,6 +36,7 @@
 // results agree with the reference's divisions to an ulp per operation.
 // Spectra are cell-major [tracer][nb] so that a warp's rows are contiguous.
 #include <cstdlib>
+#include <cstring>
 
 #include "croma_segment.cuh"
 
@@ -100,6 +101,11 @@ struct FusedParams {
     double *np_seg;          // [g1 - g0][nt][nb] proton spectra at segment starts, or null
     double *inje;            // [g1 - g0][nt][nb] electron source per segment, or null
     const int *np_min_qe;    // [nb]
+    // solver calibration (the autotuner): when cal_spec is set, the steps
+    // kernel reads and writes the spectra rows of tracer tl at cal_spec + tl nb
+    // instead of the resident ones and stops after cal_steps sub-steps
+    double *cal_spec;
+    int cal_steps;
 };
 
 __device__ __forceinline__ SegInfo segment_of(const FusedParams &P, int t, int slot)
@@ -693,19 +699,264 @@ __device__ __forceinline__ void substep(const Coef<SRC> &F, double N[kR])
     }
 }
 
-// Steps kernel: warp w of block b runs every segment [g0, g1) of tracer
-// t0 + b * kWarps + w for species S.
-template <int S, bool SRC>
-__global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 16 : 8)) steps_kernel(FusedParams P)
+// ---------------------------------------------------------------------------
+// FP32-refined sub-step (the "precision" form of the chosen path): the solve
+// of each sub-step in FP32 followed by one iterative-refinement sweep whose
+// residual is formed in FP64, the result kept in FP64.
+//
+//   y   = N / d + dt src / d                       FP64 (the scaled right-hand side)
+//   x0  = M^-1 y                                   FP32, the same two recurrences
+//   rho = y - (u - h u_{-1}),  u = x0 - q x0_{+1}  FP64: r / d - M x0 / d with M = L U,
+//                                                  L = (d, -a), U = (1, -c/d) the
+//                                                  FP64 factors of the segment
+//   e   = M^-1 rho                                 FP32
+//   N   = x0 + e                                   FP64
+//
+// The FP32 solves see y scaled by a per-segment power of two s (exact), so
+// that the largest |y| of the tracer is near 1 and the spectra, which span
+// more decades than FP32 does, keep their dominant bins in range; rho is
+// scaled by s 2^20.  The factored rows stay FP64 (the residual needs them);
+// the multipliers of the FP32 recurrences are their FP32 roundings.
+struct Coef32 {
+    float h[kR], q[kR];
+    float hk[5], qk[5];
+    float hlo, hhi, qlo, qhi;
+};
+
+__device__ __forceinline__ float supf(float v, int d) { return __shfl_up_sync(kFull, v, d); }
+__device__ __forceinline__ float sdnf(float v, int d) { return __shfl_down_sync(kFull, v, d); }
+
+template <bool SRC>
+__device__ __forceinline__ void make_coef32(const Coef<SRC> &F, Coef32 &G, int lane)
 {
+#pragma unroll
+    for (int r = 0; r < kR; r++) {
+        G.h[r] = (float)F.h[r];
+        G.q[r] = (float)F.q[r];
+    }
+    float hlo = 1.0f, hhi = 1.0f, qlo = 1.0f, qhi = 1.0f;
+#pragma unroll
+    for (int r = 0; r < kR / 2; r++) {
+        hlo *= G.h[r];
+        qlo *= G.q[r];
+        hhi *= G.h[r + kR / 2];
+        qhi *= G.q[r + kR / 2];
+    }
+    G.hlo = hlo;
+    G.hhi = hhi;
+    G.qlo = qlo;
+    G.qhi = qhi;
+    float H = hlo * hhi, Q = qlo * qhi;
+#pragma unroll
+    for (int lv = 0; lv < 5; lv++) {
+        const int off = 1 << lv;
+        G.hk[lv] = (lane >= off) ? H : 0.0f;
+        G.qk[lv] = (lane + off < 32) ? Q : 0.0f;
+        const float Hu = supf(H, off), Qd = sdnf(Q, off);
+        if (lane >= off) H *= Hu;
+        if (lane + off < 32) Q *= Qd;
+    }
+}
+
+// x <- M^-1 x in FP32, x holding the scaled right-hand side (substep's two
+// recurrences without the 1/d and source step).
+__device__ __forceinline__ void solve32(const Coef32 &G, float x[kR])
+{
+    constexpr int H2 = kR / 2;
+    float alo = 0.0f, ahi = 0.0f;
+#pragma unroll
+    for (int r = 0; r < H2; r++) {
+        alo = fmaf(G.h[r], alo, x[r]);
+        ahi = fmaf(G.h[r + H2], ahi, x[r + H2]);
+    }
+    float acc = fmaf(G.hhi, alo, ahi);
+#pragma unroll
+    for (int lv = 0; lv < 5; lv++) acc = fmaf(G.hk[lv], supf(acc, 1 << lv), acc);
+    const float cin = supf(acc, 1);
+    float plo = cin, phi = fmaf(G.hlo, cin, alo);
+#pragma unroll
+    for (int r = 0; r < H2; r++) {
+        plo = fmaf(G.h[r], plo, x[r]);
+        phi = fmaf(G.h[r + H2], phi, x[r + H2]);
+        x[r] = plo;
+        x[r + H2] = phi;
+    }
+    alo = 0.0f;
+    ahi = 0.0f;
+#pragma unroll
+    for (int r = H2 - 1; r >= 0; r--) {
+        alo = fmaf(G.q[r], alo, x[r]);
+        ahi = fmaf(G.q[r + H2], ahi, x[r + H2]);
+    }
+    acc = fmaf(G.qlo, ahi, alo);
+#pragma unroll
+    for (int lv = 0; lv < 5; lv++) acc = fmaf(G.qk[lv], sdnf(acc, 1 << lv), acc);
+    const float cout = sdnf(acc, 1);
+    phi = cout;
+    plo = fmaf(G.qhi, cout, ahi);
+#pragma unroll
+    for (int r = H2 - 1; r >= 0; r--) {
+        phi = fmaf(G.q[r + H2], phi, x[r + H2]);
+        plo = fmaf(G.q[r], plo, x[r]);
+        x[r + H2] = phi;
+        x[r] = plo;
+    }
+}
+
+// Power-of-two scale that brings the tracer's largest scaled right-hand side
+// |N / d + dt src / d| near 1 (1 for an all-zero spectrum).
+template <bool SRC>
+__device__ __forceinline__ double refine_scale(const Coef<SRC> &F, const double N[kR])
+{
+    double m = 0.0;
+#pragma unroll
+    for (int r = 0; r < kR; r++) m = fmax(m, fabs(N[r] * F.inv[r]) + (SRC ? fabs(F.sd[r]) : 0.0));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(kFull, m, off));
+    if (!(m > 0.0) || !isfinite(m)) return 1.0;
+    int e = ilogb(m);
+    e = max(-1000, min(1000, e));
+    return ldexp(1.0, -e);
+}
+
+template <bool SRC>
+__device__ __forceinline__ void substep_refined(const Coef<SRC> &F, const Coef32 &G, double N[kR], double s)
+{
+    const double inv_s = 1.0 / s, s2 = s * 1048576.0, inv_s2 = inv_s * (1.0 / 1048576.0);
+    float x[kR], e[kR];
+#pragma unroll
+    for (int r = 0; r < kR; r++) {
+        const double y = SRC ? fma(N[r], F.inv[r], F.sd[r]) : N[r] * F.inv[r];
+        x[r] = (float)(y * s);
+    }
+    solve32(G, x);
+    // u_r = x0_r - q_r x0_{r+1}; the row after the lane's last is the next
+    // lane's first (the last lane's last q is zero, so its own value is harmless)
+    const double xnext = sdn((double)x[0] * inv_s, 1);
+    const double ulast = (double)x[kR - 1] * inv_s - F.q[kR - 1] * xnext;
+    double uprev = sup(ulast, 1);   // lane 0: h of row 0 is zero
+#pragma unroll
+    for (int r = 0; r < kR; r++) {
+        const double x0 = (double)x[r] * inv_s;
+        const double x1 = (r < kR - 1) ? (double)x[r + 1] * inv_s : xnext;
+        const double u = x0 - F.q[r] * x1;
+        const double y = SRC ? fma(N[r], F.inv[r], F.sd[r]) : N[r] * F.inv[r];
+        const double rho = (y - u) + F.h[r] * uprev;
+        e[r] = (float)(rho * s2);
+        uprev = u;
+    }
+    solve32(G, e);
+#pragma unroll
+    for (int r = 0; r < kR; r++) N[r] = (double)x[r] * inv_s + (double)e[r] * inv_s2;
+}
+
+// ---------------------------------------------------------------------------
+// Warp PCR sub-step: parallel cyclic reduction of the tridiagonal system
+// b_i x_i - a_i x_{i-1} - c_i x_{i+1} = N_i + dt src_i, the algorithm of the
+// reference's solve_cc_pcr_kernel (src/fp_cuda_solver.cu:144-206) with one
+// warp per system instead of one thread block: each lane keeps its R rows in
+// registers, and at stride s every row combines with rows i - s and i + s
+// read back from the warp's slice of shared memory (swizzled rows, so both
+// partners of a lane's row r sit in distinct banks):
+//   alpha = a_i / b_{i-s},  gamma = c_i / b_{i+s},
+//   b <- b - alpha c_{i-s} - gamma a_{i+s},  a <- alpha a_{i-s},
+//   c <- gamma c_{i+s},  d <- d + alpha d_{i-s} + gamma d_{i+s},
+// log2(nb) levels, then x_i = d_i / b_i.  The rows a, b, c are rebuilt from
+// the segment's factored rows (d = 1/inv, a = h d, c = q d,
+// b = d + a q_{i-1}).  It does O(nb log nb) work and data movement per
+// sub-step against the scan's O(nb); the autotuner times both.
+struct PcrSmem {
+    double a[kSw], b[kSw], c[kSw], d[kSw];
+};
+
+template <bool SRC>
+__device__ __forceinline__ void pcr_rows_from_factored(Coef<SRC> &F, double cc[kR], int lane)
+{
+    // in place: inv -> b, h -> a, sd -> dt src; c into cc (q is read as the
+    // previous row's multiplier, so it stays)
+    const double q_in = sup(F.q[kR - 1], 1);   // q of the row before this lane's first
+#pragma unroll
+    for (int r = 0; r < kR; r++) {
+        const double dd = 1.0 / F.inv[r];
+        const double qprev = (r > 0) ? F.q[r - 1] : (lane > 0 ? q_in : 0.0);
+        const double aa = F.h[r] * dd;
+        cc[r] = F.q[r] * dd;
+        F.inv[r] = dd + aa * qprev;
+        if (SRC) F.sd[r] = F.sd[r] * dd;
+        F.h[r] = aa;
+    }
+}
+
+template <bool SRC>
+__device__ __forceinline__ void substep_pcr(const Coef<SRC> &F, const double cc[kR], double N[kR], PcrSmem &sm,
+                                            int lane)
+{
+    double a[kR], b[kR], c[kR];
+#pragma unroll
+    for (int r = 0; r < kR; r++) {
+        a[r] = F.h[r];
+        b[r] = F.inv[r];
+        c[r] = cc[r];
+        N[r] = SRC ? N[r] + F.sd[r] : N[r];
+    }
+#pragma unroll 1
+    for (int st = 1; st < NB; st <<= 1) {
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < kR; r++) {
+            const int o = r * kPitch + lane;
+            sm.a[o] = a[r];
+            sm.b[o] = b[r];
+            sm.c[o] = c[r];
+            sm.d[o] = N[r];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < kR; r++) {
+            const int m = lane * kR + r;
+            double na = 0.0, nb = b[r], nc = 0.0, nd = N[r];
+            if (m - st >= 0) {
+                const int o = swz(m - st);
+                const double al = a[r] / sm.b[o];
+                na = al * sm.a[o];
+                nb -= al * sm.c[o];
+                nd += al * sm.d[o];
+            }
+            if (m + st < NB) {
+                const int o = swz(m + st);
+                const double ga = c[r] / sm.b[o];
+                nc = ga * sm.c[o];
+                nb -= ga * sm.a[o];
+                nd += ga * sm.d[o];
+            }
+            a[r] = na;
+            b[r] = nb;
+            c[r] = nc;
+            N[r] = nd;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < kR; r++) N[r] = N[r] / b[r];
+}
+
+// Sub-step solvers of the steps kernel: the FP64 warp-scan Thomas, the same
+// with FP32 solves refined by an FP64 residual, and warp PCR.
+enum { kSolveScan = 0, kSolveRefined = 1, kSolvePcr = 2 };
+
+// Steps kernel: warp w of block b runs every segment [g0, g1) of tracer
+// t0 + b * WPB + w for species S with sub-step solver SOLVER.
+template <int S, bool SRC, int SOLVER, int WPB>
+__global__ void __launch_bounds__(WPB * 32, (NB <= 256 ? 16 : 8) / WPB) steps_kernel(FusedParams P)
+{
+    extern __shared__ double4 steps_smem[];
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int tl = blockIdx.x * kWarps + w;
+    const int tl = blockIdx.x * WPB + w;
     if (tl >= P.nt) return;
     const int t = P.t0 + tl;
     const SnapArgs &a = P.a;
     const int row0 = lane * kR;
-    double *Nrow = (S == 0 ? a.crp : a.cre) + (size_t)t * NB + row0;
+    double *Nrow = (P.cal_spec ? P.cal_spec + (size_t)tl * NB : (S == 0 ? a.crp : a.cre) + (size_t)t * NB) + row0;
     double N[kR];
 #pragma unroll
     for (int r = 0; r < kR; r += 2) {
@@ -715,9 +966,14 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 16 : 8)) steps_kerne
     }
     const double *qsrc = (S == 0) ? a.qpi : a.qepri;
     Coef<SRC> F;
+    Coef32 G;
+    double cc[SOLVER == kSolvePcr ? kR : 1];
+    PcrSmem *pcr_sm = reinterpret_cast<PcrSmem *>(steps_smem) + w;
+    double scale = 1.0;
+    int budget = P.cal_steps > 0 ? P.cal_steps : 0x7fffffff;
     const int nslot = P.g1 - P.g0;
 #pragma unroll 1
-    for (int gi = 0; gi < nslot; gi++) {
+    for (int gi = 0; gi < nslot && budget > 0; gi++) {
         const SegPre *__restrict__ pre = P.pre + (size_t)gi * P.nt + tl;
         const int flags = pre->flags;
         if (!(flags & kPreActive)) continue;
@@ -736,7 +992,7 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 16 : 8)) steps_kerne
             prefetch_l2(nf + 2 * NB);
             if (SRC && S == 1 && P.inje) prefetch_l2(P.inje + ((size_t)(gi + 1) * P.nt + tl) * NB + row0);
         }
-        if (S == 0 && P.np_seg) {
+        if (S == 0 && P.np_seg && !P.cal_spec) {
             double *o = P.np_seg + ((size_t)gi * P.nt + tl) * NB + row0;
 #pragma unroll
             for (int r = 0; r < kR; r += 2)
@@ -755,20 +1011,34 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 16 : 8)) steps_kerne
 #pragma unroll 1
         for (int k = 0; k < 3; k++) {
             const int want = (k == 1) ? 0 : 1;
-            const int run_n = (k == 0) ? sl : (k == 1 ? el - sl : g.steps - el);
+            int run_n = (k == 0) ? sl : (k == 1 ? el - sl : g.steps - el);
             if (run_n <= 0) continue;
             if (want >= P.sets) {   // no off set in the workspace: report, leave N as it was
                 if (lane == 0) atomicOr(a.err, kErrBadInput);
                 return;
             }
+            run_n = min(run_n, budget);
+            budget -= run_n;
             if (want != cur) {
                 load_coef<SRC>(F, fac_ptr(P, S, gi, want, tl), src, g.dt, lane);
+                if (SOLVER == kSolveRefined) make_coef32<SRC>(F, G, lane);
+                if (SOLVER == kSolvePcr) pcr_rows_from_factored<SRC>(F, cc, lane);
                 cur = want;
             }
-            // two sub-steps per trip: the carried spectrum keeps its
-            // registers across the loop (fewer copies per sub-step)
+            if (SOLVER == kSolveRefined) {
+                scale = refine_scale<SRC>(F, N);
+#pragma unroll 1
+                for (int istep = 0; istep < run_n; istep++) substep_refined<SRC>(F, G, N, scale);
+            } else if (SOLVER == kSolvePcr) {
+#pragma unroll 1
+                for (int istep = 0; istep < run_n; istep++) substep_pcr<SRC>(F, cc, N, *pcr_sm, lane);
+            } else {
+                // two sub-steps per trip: the carried spectrum keeps its
+                // registers across the loop (fewer copies per sub-step)
 #pragma unroll 2
-            for (int istep = 0; istep < run_n; istep++) substep<SRC>(F, N);
+                for (int istep = 0; istep < run_n; istep++) substep<SRC>(F, N);
+            }
+            if (budget <= 0) break;
         }
     }
 #pragma unroll
@@ -1082,6 +1352,104 @@ cudaError_t launch_factor(Context &ctx, const FusedParams &P)
     return cudaGetLastError();
 }
 
+// One steps-kernel variant: solver and warps per block (1, 2 or 4), on the
+// first `tracers` tracers of the chunk (all when <= 0).
+template <int S, bool SRC, int SOLVER, int WPB>
+cudaError_t launch_steps_variant(cudaStream_t st, const FusedParams &P, int tracers)
+{
+    const int n = tracers > 0 ? min(tracers, P.nt) : P.nt;
+    const int blocks = (n + WPB - 1) / WPB;
+    const size_t smem = SOLVER == kSolvePcr ? WPB * sizeof(PcrSmem) : 0;
+    if (smem > 48 * 1024) {
+        static const cudaError_t attr = cudaFuncSetAttribute(steps_kernel<S, SRC, SOLVER, WPB>,
+                                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (attr != cudaSuccess) return attr;
+    }
+    steps_kernel<S, SRC, SOLVER, WPB><<<blocks, WPB * 32, smem, st>>>(P);
+    return cudaGetLastError();
+}
+
+// Variants the autotuner chooses between: (solver, warps per block).
+constexpr int kStepVariants = 4;
+constexpr int kVariantSolver[kStepVariants] = {kSolveScan, kSolveScan, kSolveScan, kSolvePcr};
+constexpr int kVariantWpb[kStepVariants] = {1, 2, 4, 1};
+
+template <int S, bool SRC>
+cudaError_t launch_variant(cudaStream_t st, const FusedParams &P, int v, int tracers)
+{
+    switch (v) {
+    case 1: return launch_steps_variant<S, SRC, kSolveScan, 2>(st, P, tracers);
+    case 2: return launch_steps_variant<S, SRC, kSolveScan, 4>(st, P, tracers);
+    case 3: return launch_steps_variant<S, SRC, kSolvePcr, 1>(st, P, tracers);
+    default: return launch_steps_variant<S, SRC, kSolveScan, 1>(st, P, tracers);
+    }
+}
+
+// CROMA_CUDA_TRIDIAG (src/fp_cuda_solver.cu:41-63 of the reference): "thomas"
+// keeps the scan solvers, "pcr" forces PCR, unset lets the tuner choose.
+int tridiag_env()
+{
+    const char *e = getenv("CROMA_CUDA_TRIDIAG");
+    if (!e) e = getenv("FP_GPU_CUDA_TRIDIAG");
+    if (!e) return 0;
+    if (strcmp(e, "thomas") == 0) return 1;
+    if (strcmp(e, "pcr") == 0) return 2;
+    return 0;
+}
+
+// The autotuner: on the first chunk a context evolves, each admissible
+// variant runs the chunk's first tracers (at most 2,048) for their first 16
+// sub-steps on a copy of their spectra, timed with CUDA events; the fastest
+// is kept for the context's species.  Results are recorded in ctx.tune.
+template <int S>
+int tune_steps(Context &ctx, const FusedParams &P, bool src)
+{
+    TuneState &tu = ctx.tune[S];
+    const int env = tridiag_env();
+    const int T = min(P.nt, 2048), steps = 16;
+    double *scratch = nullptr;
+    CROMA_CUDA(dev_alloc(ctx, &scratch, (size_t)T * NB * sizeof(double)));
+    struct Free {
+        Context &c;
+        double *p;
+        ~Free() { dev_free(c, p); }
+    } guard{ctx, scratch};
+    const double *real = (S == 0 ? P.a.crp : P.a.cre) + (size_t)P.t0 * NB;
+    FusedParams Q = P;
+    Q.cal_spec = scratch;
+    Q.cal_steps = steps;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CROMA_CUDA(cudaEventCreate(&e0));
+    CROMA_CUDA(cudaEventCreate(&e1));
+    int best = -1;
+    for (int v = 0; v < kStepVariants; v++) {
+        const bool pcr = kVariantSolver[v] == kSolvePcr;
+        tu.ms[v] = -1.0;
+        if ((env == 1 && pcr) || (env == 2 && !pcr)) continue;
+        double ms_best = 1e30;
+        for (int rep = 0; rep < 2; rep++) {   // the first run warms the code and L2
+            CROMA_CUDA(cudaMemcpyAsync(scratch, real, (size_t)T * NB * sizeof(double), cudaMemcpyDeviceToDevice,
+                                       ctx.stream));
+            CROMA_CUDA(cudaEventRecord(e0, ctx.stream));
+            CROMA_CUDA((src ? launch_variant<S, true>(ctx.stream, Q, v, T) : launch_variant<S, false>(ctx.stream, Q, v, T)));
+            CROMA_CUDA(cudaEventRecord(e1, ctx.stream));
+            CROMA_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            CROMA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (rep == 1) ms_best = ms;
+        }
+        tu.ms[v] = ms_best;
+        if (best < 0 || ms_best < tu.ms[best]) best = v;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    tu.variant = best < 0 ? 0 : best;
+    tu.tuned = 1;
+    tu.tracers = T;
+    tu.steps = steps;
+    return 0;
+}
+
 template <int S>
 cudaError_t launch_steps(Context &ctx, const FusedParams &P, bool src, bool perstep)
 {
@@ -1089,11 +1457,18 @@ cudaError_t launch_steps(Context &ctx, const FusedParams &P, bool src, bool pers
     if (perstep) {
         if (src) plain_steps_kernel<S, true><<<blocks, kWarps * 32, 0, ctx.stream>>>(P);
         else plain_steps_kernel<S, false><<<blocks, kWarps * 32, 0, ctx.stream>>>(P);
-    } else {
-        if (src) steps_kernel<S, true><<<blocks, kWarps * 32, 0, ctx.stream>>>(P);
-        else steps_kernel<S, false><<<blocks, kWarps * 32, 0, ctx.stream>>>(P);
+        return cudaGetLastError();
     }
-    return cudaGetLastError();
+    if (ctx.cfg.path == CROMA_PATH_FUSED_FP32R) {
+        if (src) return launch_steps_variant<S, true, kSolveRefined, 1>(ctx.stream, P, 0);
+        return launch_steps_variant<S, false, kSolveRefined, 1>(ctx.stream, P, 0);
+    }
+    if (!ctx.tune[S].tuned) {
+        const int rc = tune_steps<S>(ctx, P, src);
+        if (rc) return cudaErrorUnknown;
+    }
+    const int v = ctx.tune[S].variant;
+    return src ? launch_variant<S, true>(ctx.stream, P, v, 0) : launch_variant<S, false>(ctx.stream, P, v, 0);
 }
 
 // Workspace budget of the fused path (factored matrices, segment-start
@@ -1338,6 +1713,15 @@ int run_fused(Context &ctx, const SnapArgs &a)
     const int nslots = ctx.mp.interp_max_segments < 1 ? 1
                      : (ctx.mp.interp_max_segments > 64 ? 64 : ctx.mp.interp_max_segments);
     return fused_chunks(ctx, P, nslots, ctx.cfg.path == CROMA_PATH_PLAIN);
+}
+
+int tuning_info(const Context &ctx, int species, int *solver, int *wpb)
+{
+    if (species < 0 || species > 1) return -1;
+    const TuneState &t = ctx.tune[species];
+    if (solver) *solver = kVariantSolver[t.variant];
+    if (wpb) *wpb = kVariantWpb[t.variant];
+    return t.tuned;
 }
 
 int run_fused_segment(Context &ctx, const SnapArgs &a, const SegInfo &ex, int ic_stride)

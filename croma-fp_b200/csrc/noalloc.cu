@@ -25,10 +25,13 @@
 //     different host threads) race on the array and corrupt each other's
 //     results: serialise them, e.g. on one stream.
 //   * The first call on each device looks the array's device address up with
-//     cudaGetSymbolAddress (with that device current) and caches it; make
-//     that first call before any stream capture begins.
+//     cudaGetSymbolAddress (with that device current) and caches it.  The
+//     stream must belong to the current device (checked: -1 otherwise); a
+//     cudaDeviceReset on a device ends the cached address's validity, so the
+//     library is not used on that device after one.
 //   * The call waits for its stream to finish the solve so that it can report
-//     a singular pivot (-2).
+//     a singular pivot (-2); a stream that is being captured is refused (-1)
+//     before anything is launched, since the wait would break the capture.
 #include <mutex>
 
 #include "croma_ctx.cuh"
@@ -110,6 +113,20 @@ extern "C" int solve_cc_cuda_batch_noalloc(int nsys, int nrow, double dt, const 
         return -1;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CROMA_CUDA(cudaStreamIsCapturing(st, &cap));
+    if (cap != cudaStreamCaptureStatusNone) {
+        set_error("solve_cc_cuda_batch_noalloc: the stream is being captured; the call waits for its stream "
+                  "and cannot run inside a capture");
+        return -1;
+    }
+    int cur = 0, sdev = 0;
+    CROMA_CUDA(cudaGetDevice(&cur));
+    CROMA_CUDA(cudaStreamGetDevice(st, &sdev));
+    if (sdev != cur) {
+        set_error("solve_cc_cuda_batch_noalloc: the stream belongs to another device than the current one");
+        return -1;
+    }
     double *scratch = nullptr;
     CROMA_CUDA(scratch_address(&scratch));
     CROMA_CUDA(cudaMemsetAsync(scratch, 0, sizeof(double), st));

@@ -21,6 +21,7 @@
 // globals when the library is linked into CROMA (weak references) and from
 // croma_b200_set_model() otherwise.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <initializer_list>
 #include <mutex>
@@ -213,6 +214,59 @@ __global__ void cc_thomas_kernel(int nsys, int nrow, double dt, const double *a,
     for (int i = nrow - 2; i >= 0; i--) x[i] -= cp[i] * x[i + 1];
 }
 
+// solve_cc_pcr_kernel's algorithm (src/fp_cuda_solver.cu:144-206): one block
+// per system, one thread per row, parallel cyclic reduction over shared
+// memory -- at stride s row i absorbs rows i - s and i + s:
+// alpha = a_i / b_{i-s}, gamma = c_i / b_{i+s}; b <- b - alpha c_{i-s} -
+// gamma a_{i+s}; a <- alpha a_{i-s}; c <- gamma c_{i+s}; d <- d + alpha
+// d_{i-s} + gamma d_{i+s} -- for log2(nrow) levels, then x_i = d_i / b_i.
+// nrow is a power of two (checked by the caller); smem 8 nrow doubles.
+__global__ void cc_pcr_kernel(int nrow, double dt, const double *a, const double *b, const double *c,
+                              const double *src, const double *x_in, double *x_out, unsigned *err)
+{
+    extern __shared__ double pcr_sm[];
+    double *A = pcr_sm, *B = A + nrow, *Cc = B + nrow, *D = Cc + nrow;   // current level
+    double *A2 = D + nrow, *B2 = A2 + nrow, *C2 = B2 + nrow, *D2 = C2 + nrow;   // next level
+    const int i = threadIdx.x;
+    const size_t o = (size_t)blockIdx.x * nrow + i;
+    A[i] = a[o];
+    B[i] = b[o];
+    Cc[i] = c[o];
+    D[i] = dt * src[o] + x_in[o];
+    __syncthreads();
+    for (int st = 1; st < nrow; st <<= 1) {
+        double na = 0.0, nb = B[i], nc = 0.0, nd = D[i];
+        if (i - st >= 0) {
+            const double al = A[i] / B[i - st];
+            na = al * A[i - st];
+            nb -= al * Cc[i - st];
+            nd += al * D[i - st];
+        }
+        if (i + st < nrow) {
+            const double ga = Cc[i] / B[i + st];
+            nc = ga * Cc[i + st];
+            nb -= ga * A[i + st];
+            nd += ga * D[i + st];
+        }
+        A2[i] = na;
+        B2[i] = nb;
+        C2[i] = nc;
+        D2[i] = nd;
+        __syncthreads();
+        double *t;
+        t = A; A = A2; A2 = t;
+        t = B; B = B2; B2 = t;
+        t = Cc; Cc = C2; C2 = t;
+        t = D; D = D2; D2 = t;
+    }
+    if (fabs(B[i]) <= 1.0e-300) {
+        atomicOr(err, kErrSingular);
+        x_out[o] = 0.0;
+        return;
+    }
+    x_out[o] = D[i] / B[i];
+}
+
 // One-shot device buffers of the stateless entry points (grow-only, guarded).
 struct Scratch {
     std::vector<void *> ptrs;
@@ -334,15 +388,25 @@ int cuda_get_current_device_id(char *out, int len)
     return 0;
 }
 
+// CROMA_CUDA_TRIDIAG as the reference reads it (src/fp_cuda_solver.cu:41-72):
+// "pcr" selects PCR for power-of-two row counts up to 512 (-1 otherwise),
+// "thomas" selects Thomas.  Unset, this library's solvers are Thomas (the
+// stateless batch solve) and, in the pipeline, the steps-kernel autotuner's
+// choice, which has picked the warp-scan Thomas over warp PCR on every
+// configuration measured; the stateless query then reports Thomas.
 int fp_cuda_tridiag_uses_pcr(int nrow)
 {
-    (void)nrow;
-    return 0;
+    const char *e = getenv("CROMA_CUDA_TRIDIAG");
+    if (!e) e = getenv("FP_GPU_CUDA_TRIDIAG");
+    if (!e || strcmp(e, "pcr") != 0) return 0;
+    return (nrow > 0 && (nrow & (nrow - 1)) == 0 && nrow <= 512) ? 1 : -1;
 }
 
 const char *fp_cuda_tridiag_solver_name(int nrow)
 {
-    (void)nrow;
+    const int pcr = fp_cuda_tridiag_uses_pcr(nrow);
+    if (pcr > 0) return "PCR (parallel cyclic reduction, one block per system)";
+    if (pcr < 0) return "PCR requested for a row count it cannot take";
     return "Thomas (warp-scan LU, factor once per segment)";
 }
 
@@ -365,8 +429,15 @@ int solve_cc_cuda_batch(const FpChangCooperSolveBatchInput *in, const double *st
     cudaEventRecord(e0);
     const double *h[5] = {in->a_batch, in->b_batch, in->c_batch, in->source_batch, state_init};
     for (int k = 0; k < 5; k++) CROMA_CUDA(cudaMemcpy(d[k], h[k], bytes, cudaMemcpyHostToDevice));
-    cc_thomas_kernel<<<(in->nsys + 127) / 128, 128>>>(in->nsys, in->nrow, in->dt, d[0], d[1], d[2], d[3],
-                                                      d[4], d[5], d[6], d_err);
+    const int pcr = fp_cuda_tridiag_uses_pcr(in->nrow);
+    if (pcr < 0) return fail(-1, "CROMA_CUDA_TRIDIAG=pcr needs a power-of-two row count of at most 512");
+    if (pcr) {
+        cc_pcr_kernel<<<in->nsys, in->nrow, 8 * in->nrow * sizeof(double)>>>(in->nrow, in->dt, d[0], d[1], d[2],
+                                                                             d[3], d[4], d[5], d_err);
+    } else {
+        cc_thomas_kernel<<<(in->nsys + 127) / 128, 128>>>(in->nsys, in->nrow, in->dt, d[0], d[1], d[2], d[3],
+                                                          d[4], d[5], d[6], d_err);
+    }
     CROMA_CUDA(cudaGetLastError());
     CROMA_CUDA(cudaMemcpy(state_out, d[5], bytes, cudaMemcpyDeviceToHost));
     unsigned err = 0;
@@ -376,7 +447,7 @@ int solve_cc_cuda_batch(const FpChangCooperSolveBatchInput *in, const double *st
     if (elapsed_ms) *elapsed_ms = elapsed(e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (used_pcr_out) *used_pcr_out = 0;
+    if (used_pcr_out) *used_pcr_out = pcr;
     if (err) return fail(-2, "singular tridiagonal pivot in solve_cc_cuda_batch");
     return 0;
 }

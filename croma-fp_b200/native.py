@@ -17,7 +17,7 @@ from .config import RunConfig
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBDIR = os.path.join(HERE, "lib")
 
-PATHS = {"plain": 0, "fused": 1}
+PATHS = {"plain": 0, "fused": 1, "fp32r": 2}
 
 _d, _i, _vp = C.c_double, C.c_int, C.c_void_p
 
@@ -86,6 +86,7 @@ def load_library(nb: int) -> C.CDLL:
     L.croma_b200_emission_table.argtypes = [_vp, _i, _vp]
     L.croma_b200_step_host.argtypes = [_vp, P(CromaB200Snapshot), P(CromaB200StepHost)]
     L.croma_b200_host_alloc.argtypes = [C.c_size_t, P(_vp)]
+    L.croma_b200_get_tuning.argtypes = [_vp, _i, P(_i), P(_i), P(_i), P(_d)]
     L.croma_b200_host_free.argtypes = [_vp]
     _LIBS[nb] = L
     return L
@@ -354,6 +355,18 @@ class TracerFP:
                 setattr(io, f, a.ctypes.data)
         self._check(self.lib.croma_b200_step_host(self.h, C.byref(snap), C.byref(io)))
         del keep
+
+    SOLVERS = {0: "thomas-scan", 1: "thomas-scan-fp32-refined", 2: "pcr"}
+
+    def tuning(self, species: int):
+        """The steps-kernel autotuner's record for species 0 (protons) or 1
+        (electrons): dict(tuned, solver, warps_per_block, variant_ms)."""
+        t, so, w = _i(), _i(), _i()
+        ms = (_d * 4)()
+        self._check(self.lib.croma_b200_get_tuning(self.h, species, C.byref(t), C.byref(so), C.byref(w), ms))
+        names = ("scan x1", "scan x2", "scan x4", "pcr x1")
+        return {"tuned": t.value, "solver": self.SOLVERS.get(so.value, so.value), "warps_per_block": w.value,
+                "variant_ms": {n: (m if m >= 0 else None) for n, m in zip(names, list(ms))}}
 
     def sync(self):
         self._check(self.lib.croma_b200_sync(self.h))

@@ -40,7 +40,7 @@ def _package():
 
 
 def run(nrequests=48, load=0.7, budget_gb=120.0, max_concurrent=4, seed=20261203,
-        rate_tracer_snaps_per_s=1.7e6, pool_tracers=POOL_TRACERS, max_chunk=65536):
+        rate_tracer_snaps_per_s=1.7e6, pool_tracers=POOL_TRACERS, max_chunk=65536, path="fused"):
     """Runs the serving workload; returns a result dict."""
     _package()
     from croma_fp_b200 import config, serve, synth
@@ -65,7 +65,7 @@ def run(nrequests=48, load=0.7, budget_gb=120.0, max_concurrent=4, seed=20261203
     work = float(np.sum(sizes * nsnaps))
     mean_service = work / nrequests / rate_tracer_snaps_per_s
     gaps = rng.exponential(mean_service / load, nrequests)
-    srv = serve.Server(cfg, hbm_budget_gb=budget_gb, max_concurrent=max_concurrent)
+    srv = serve.Server(cfg, hbm_budget_gb=budget_gb, max_concurrent=max_concurrent, path=path)
     flat = pool.reshape(-1)
     ids = []
     t0 = time.perf_counter()
@@ -102,7 +102,7 @@ def run(nrequests=48, load=0.7, budget_gb=120.0, max_concurrent=4, seed=20261203
             "p50_s": pct(0.5), "p99_s": pct(0.99), "max_s": float(lat[-1]),
             "tracer_snapshots": work, "wall_s": t1 - t0,
             "throughput": work / (t1 - t0), "offered_load": load, "max_concurrent": max_concurrent,
-            "hbm_budget_gb": budget_gb, "server_p50_s": st["p50_s"], "server_p99_s": st["p99_s"],
+            "hbm_budget_gb": budget_gb, "server_p50_s": st["p50_s"], "server_p99_s": st["p99_s"], "path": path,
             "workload": "Poisson arrivals, chunk log-U[64, 65536], 20..200 snapshots, "
                         "seed species uniform {e, p, e+p}, 256 bins, ASA, nsub <= 500"}
 

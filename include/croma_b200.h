@@ -41,8 +41,11 @@ enum {
     CROMA_PATH_PLAIN = 0,   /* FP64, reference data contract: CC rows materialised per
                                segment, every sub-step reads them, the source and N
                                from memory, re-pivots and writes N (per-step) */
-    CROMA_PATH_FUSED = 1    /* FP64, on-chip: rows built, factored and swept per tracer
+    CROMA_PATH_FUSED = 1,   /* FP64, on-chip: rows built, factored and swept per tracer
                                inside one kernel, warp-cooperative substitution */
+    CROMA_PATH_FUSED_FP32R = 2  /* the on-chip path with each sub-step solved in FP32 and
+                               refined once with an FP64 residual (FP64 factors, CC
+                               weights, spectra and particle budget) */
 };
 
 /* Species bits: bit 0 protons, bit 1 electrons.  A species outside the mask
@@ -312,6 +315,20 @@ typedef struct {
     double *crp_out, *cre_out;                        /* host [ntracer][nb] or NULL */
 } CromaB200StepHost;
 int croma_b200_step_host(CromaB200Context *ctx, const CromaB200Snapshot *snap, const CromaB200StepHost *io);
+
+/* The steps-kernel autotuner (the on-chip FP64 path).  On the first
+ * workspace chunk a context evolves, per species, each admissible variant --
+ * the warp-scan Thomas at 1, 2 or 4 tracers (warps) per block, and warp PCR
+ * (one warp per tracer, parallel cyclic reduction in shared memory) -- runs
+ * the chunk's first tracers (up to 2,048) for 16 sub-steps on a copy of
+ * their spectra, timed with CUDA events, and the fastest is kept for the
+ * context.  CROMA_CUDA_TRIDIAG=thomas admits only the scan variants, =pcr
+ * only PCR (src/fp_cuda_solver.cu:41-72 of the reference).  Reported here:
+ * tuned (0 before the first snapshot), solver (0 scan, 1 FP32-refined scan,
+ * 2 PCR), tracers per block, and the calibration time of each variant in
+ * milliseconds (variant order: scan x1, scan x2, scan x4, PCR; -1 = not run). */
+int croma_b200_get_tuning(CromaB200Context *ctx, int species, int *tuned, int *solver, int *warps_per_block,
+                          double *variant_ms);
 
 /* Page-locked host memory of exactly `bytes` (cudaHostAlloc, portable), for
  * the host-buffer calls above, whose copies overlap the kernels only from

@@ -317,9 +317,12 @@ int solve_cc_cuda_batch(const FpChangCooperSolveBatchInput *in,             /* :
  * library, so nsys * nrow may not exceed 524288 (larger batches return -1);
  * every GPU that loads the library keeps that 4 MiB array until exit.  All
  * calls on a device share it: calls that overlap on the GPU race and must be
- * serialised.  The first call on a device looks the array up and should come
- * before any stream capture.  The call waits for its stream and returns -2
- * on a singular pivot. */
+ * serialised.  The first call on a device looks the array up and caches its
+ * address; the stream must belong to the current device (-1 otherwise), and
+ * after a cudaDeviceReset the library is not to be used on that device.  The
+ * call waits for its stream and returns -2 on a singular pivot; because of
+ * that wait it refuses (-1, nothing launched) a stream that is being
+ * captured. */
 int solve_cc_cuda_batch_noalloc(int nsys, int nrow, double dt,
                                 const double *a, const double *b, const double *c,
                                 const double *source, const double *state_in,

@@ -62,3 +62,25 @@ def test_tables_match_reference(name):
     assert np.array_equal(npmin, d["np_min_qe"])
     if "fqe" in d:
         assert rel_err(fqe, d["fqe"], 1e-30) <= 1e-12
+
+
+FP32R_RTOL = 1e-6   # the precision form's bar: max relative error vs the FP64 reference
+
+
+@pytest.mark.parametrize("name", case_names())
+def test_fp32_refined_path_matches_reference(name):
+    """The on-chip path with each sub-step solved in FP32 and refined once
+    with an FP64 residual: schedule bit-exact (it is the same FP64 schedule),
+    spectra within 1e-6 of the reference's FP64 result; the error is recorded
+    per case."""
+    c, fp, results = _run_case(name, "fp32r")
+    d = c.d
+    worst = 0.0
+    for k, (sched, crp, cre) in enumerate(results):
+        assert np.array_equal(sched["nsub"], d[f"nsub_{k}"])
+        assert np.array_equal(sched["bucket_ids"], d[f"bucket_ids_{k}"])
+        worst = max(worst, rel_err(cre, d[f"cre_{k}"]))
+        if np.any(d[f"crp_{k}"]):
+            worst = max(worst, rel_err(crp, d[f"crp_{k}"]))
+    print(f"{name}: fp32-refined max rel err {worst:.3e}")
+    assert worst <= FP32R_RTOL, f"fp32-refined spectra rel err {worst:.3e}"

@@ -275,3 +275,27 @@ def test_device_binding_entry_points():
     assert abi.lib.cuda_get_current_device_id(buf, 64) == 0 and len(buf.value) > 4
     assert abi.lib.fp_cuda_tridiag_uses_pcr(128) == 0
     assert b"Thomas" in abi.lib.fp_cuda_tridiag_solver_name(128)
+
+
+def test_solve_cc_cuda_batch_pcr_when_requested(monkeypatch):
+    """CROMA_CUDA_TRIDIAG=pcr (src/fp_cuda_solver.cu:41-72): the batch solve
+    runs parallel cyclic reduction and reports it; same result as Thomas."""
+    cfg, o, abi, w, gp, ge, crp, cre, qpi, qepri, dis = _setup(nt=16)
+    row, m1, p1 = o.ic_row(0.4)
+    ric = np.repeat(row[:, None], 16, axis=1)
+    _, cce_on, _, _ = o.cc_coeffs(3e-4, w.background(2), ric, np.full(16, m1), np.full(16, p1), mass=w.mass)
+    a, b, c = (np.ascontiguousarray(cce_on[k]) for k in range(3))
+    src, x0, dt = np.ascontiguousarray(qepri), np.ascontiguousarray(cre), 3e-4
+    ref = _thomas_np(a, b, c, dt * src + x0)
+    inp = ref_abi.FpChangCooperSolveBatchInput(16, 128, dt, ref_abi.dptr(a), ref_abi.dptr(b), ref_abi.dptr(c),
+                                               ref_abi.dptr(src))
+    monkeypatch.setenv("CROMA_CUDA_TRIDIAG", "pcr")
+    assert abi.lib.fp_cuda_tridiag_uses_pcr(128) == 1
+    assert abi.lib.fp_cuda_tridiag_uses_pcr(100) == -1
+    out, ms, pcr = np.empty_like(x0), C.c_double(), C.c_int(7)
+    assert abi.lib.solve_cc_cuda_batch(C.byref(inp), ref_abi.dptr(x0), ref_abi.dptr(out), C.byref(ms),
+                                       C.byref(pcr)) == 0, abi.error()
+    assert pcr.value == 1
+    assert rel_err(out, ref) <= 1e-12
+    monkeypatch.setenv("CROMA_CUDA_TRIDIAG", "thomas")
+    assert abi.lib.fp_cuda_tridiag_uses_pcr(128) == 0

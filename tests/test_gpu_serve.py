@@ -110,3 +110,53 @@ def test_server_budget_cancel_and_strides():
         assert rel_err(g_cre, o_cre) <= 1e-10
     finally:
         srv.close()
+
+
+@pytest.mark.parametrize("path", ["fused", "fp32r"])
+def test_result_alone_equals_result_in_the_mix_256_bins(path):
+    """Config 3's mix at 256 bins with all three seed species: requests that
+    run concurrently (admitted as slots free up, their kernels overlapping on
+    the device) give the same spectra as each request run alone, within the
+    FP64 bar 1e-10 (they are computed by the same kernels on their own
+    contexts, so in practice bit for bit)."""
+    base = config.config1(nb=256)
+    specs = [(48, 3, "electron_only", 2), (20, 2, "proton_only", 3), (64, 2, "electron_proton", 3),
+             (33, 4, "electron_only", 2), (16, 3, "proton_only", 3), (40, 3, "electron_proton", 3)]
+    reqs = []
+    for i, (n, nsnap, seed, mask) in enumerate(specs):
+        cfg = config.config1(nb=256, species=seed)
+        first = 12 + 5 * i
+        w, bg, z, dt = _inputs(cfg, n, nsnap, 900 + i, first)
+        import pyoracle
+        o = pyoracle.Oracle(cfg)
+        gp, ge = o.grid(0), o.grid(1)
+        crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), n, cfg.species)
+        reqs.append(dict(bg=bg, z=z, dt=dt, crp=crp, cre=cre, mass=w.mass, mask=mask, e0=float(w.elapsed[first])))
+
+    def submit(srv, r):
+        return srv.submit(r["bg"], r["z"], r["dt"], r["crp"], r["cre"], mass=r["mass"], species_mask=r["mask"],
+                          elapsed0=r["e0"])
+
+    mix = []
+    srv = serve.Server(base, hbm_budget_gb=20.0, max_concurrent=4, workspace_gb_per_request=0.5, path=path)
+    try:
+        ids = [submit(srv, r) for r in reqs]
+        for rid in ids:
+            assert srv.wait(rid, 300.0) == serve.DONE, srv.result(rid)
+            mix.append(srv.output(rid))
+        assert srv.stats()["completed"] == len(reqs)
+    finally:
+        srv.close()
+    srv = serve.Server(base, hbm_budget_gb=20.0, max_concurrent=1, workspace_gb_per_request=0.5, path=path)
+    try:
+        for r, (m_crp, m_cre) in zip(reqs, mix):
+            rid = submit(srv, r)
+            assert srv.wait(rid, 300.0) == serve.DONE, srv.result(rid)
+            a_crp, a_cre = srv.output(rid)
+            for alone, inmix in ((a_crp, m_crp), (a_cre, m_cre)):
+                if np.any(alone):
+                    assert rel_err(inmix, alone) <= 1e-10
+                else:
+                    assert not np.any(inmix)
+    finally:
+        srv.close()

@@ -78,3 +78,54 @@ def test_noalloc_rejects_batches_beyond_its_scratch():
     rc = lib.solve_cc_cuda_batch_noalloc(nsys, nrow, 1.0, 8, 8, 8, 8, 8, 8, None)
     assert rc == -1
     assert b"524288" in lib.croma_b200_last_error()
+
+
+def test_noalloc_singular_pivot_then_clean_call():
+    """A zero first diagonal in one system gives -2 (the error word at the
+    head of the shared scratch is set); the next, valid call clears it and
+    returns 0 with the same result as solve_cc_cuda_batch."""
+    import torch
+    lib = _lib()
+    abi = ref_abi.RefAbi(128)
+    stream = torch.cuda.current_stream()
+    nsys, nrow, dt = 64, 128, 1e-3
+    a, b, c, src, x0 = _systems(nsys, nrow, 21)
+    bad = b.copy()
+    bad[17, 0] = 0.0
+    dev = [torch.from_numpy(v).cuda() for v in (a, bad, c, src, x0)]
+    out = torch.empty_like(dev[4])
+    torch.cuda.synchronize()
+    rc = lib.solve_cc_cuda_batch_noalloc(nsys, nrow, dt, *[t.data_ptr() for t in dev], out.data_ptr(),
+                                         stream.cuda_stream)
+    assert rc == -2
+    assert b"singular" in lib.croma_b200_last_error()
+    dev[1] = torch.from_numpy(b).cuda()
+    torch.cuda.synchronize()
+    rc = lib.solve_cc_cuda_batch_noalloc(nsys, nrow, dt, *[t.data_ptr() for t in dev], out.data_ptr(),
+                                         stream.cuda_stream)
+    assert rc == 0, lib.croma_b200_last_error().decode()
+    inp = ref_abi.FpChangCooperSolveBatchInput(nsys, nrow, dt, ref_abi.dptr(a), ref_abi.dptr(b), ref_abi.dptr(c),
+                                               ref_abi.dptr(src))
+    ref = np.empty_like(x0)
+    assert abi.lib.solve_cc_cuda_batch(C.byref(inp), ref_abi.dptr(x0), ref_abi.dptr(ref), None, None) == 0
+    got = out.cpu().numpy()
+    assert np.max(np.abs(got - ref) / np.abs(ref)) <= 1e-12
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    import torch
+    lib = _lib()
+    nsys, nrow = 8, 128
+    a, b, c, src, x0 = _systems(nsys, nrow, 22)
+    dev = [torch.from_numpy(v).cuda() for v in (a, b, c, src, x0)]
+    out = torch.empty_like(dev[4])
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    rc = None
+    with torch.cuda.graph(g, stream=s):
+        out.add_(0.0)   # the captured graph is not empty
+        rc = lib.solve_cc_cuda_batch_noalloc(nsys, nrow, 1e-3, *[t.data_ptr() for t in dev], out.data_ptr(),
+                                             s.cuda_stream)
+    assert rc == -1
+    assert b"captured" in lib.croma_b200_last_error()
