@@ -23,13 +23,21 @@
 //   the trapezoid of Q_one, src/EMISSION.c:297-308, with beta_p and E_k / 2
 //   for the hadronic kinds) and s_t = n_gas of the tracer (1 for IC);
 //   synchrotron: one warp per tracer, the log-K interpolation of
-//   prepare_synch_emission_cell_major (src/fp_shared_core.c:2070-2112) over
-//   tables of K and log K, the bins split over the lanes.
+//   prepare_synch_emission_cell_major (src/fp_shared_core.c:2070-2112,
+//   tracer_fp_interp_synch_kernel_logk :2054-2068) over tables of K and
+//   log K, the bins split over the lanes, bins from 2 up to the first je
+//   whose N[je+1] is not positive; b_dyn = B of the snapshot's background
+//   (field 2), logb = log10(B / 1e-6 G) with a non-positive or non-finite B
+//   taken as 1e-30 (tracer_fp_logb_range_from_snapshot,
+//   src/tracer_fp_synch.c:123-152).  Tracers run sorted by their log-B
+//   plane so that a block shares each table row through shared memory.
 // The sums run in a different order from the reference's sequential loops:
 // the results agree to rounding, not bit for bit.
 #include <cstdio>
 #include <cstring>
 #include <vector>
+
+#include <cub/cub.cuh>
 
 #define np CROMA_NB
 #define npe CROMA_NB
@@ -271,23 +279,69 @@ __global__ void fold_weights_kernel(int nbins, int wpitch, const double *kern, c
     W[i] = w;
 }
 
-// Synchrotron emissivity of the resident electron spectra through the
-// pitch-kernel table, one warp per tracer: bin je = 32 r + lane (r < R) of
-// every frequency, N dp kept in registers, bins from 2 up to the first je
-// whose N[je+1] is not positive (prepare_synch_emission_cell_major,
-// src/fp_shared_core.c:2088-2108, tracer_fp_interp_synch_kernel_logk
-// :2054-2068).  b_dyn = B of the snapshot's background (field 2),
-// logb = log10(B / 1e-6 G) with a non-positive or non-finite B taken as
-// 1e-30 (tracer_fp_logb_range_from_snapshot, src/tracer_fp_synch.c:123-152).
-__global__ void __launch_bounds__(128) synch_resident_kernel(int ntracer, int nfreq, int nlogb, double logb_min,
-                                                             double inv_dlogb, SynchPrefactor sp, const double *K,
-                                                             const double *logK, const double *bfield,
-                                                             const double *cre, const double *dp, double *out)
+// The synchrotron emission with the table rows shared: tracers are sorted by
+// their lower log-B plane ib (synch_plane_kernel + a radix sort), and a block
+// of kSynWarps warps takes kSynWarps consecutive sorted tracers, one per
+// warp.  For each frequency the block stages the rows K and log K of the
+// planes its tracers interpolate between -- two or three planes when their
+// ib values span at most two, which the sort makes the common case -- in
+// shared memory, so each row is read once per block instead of once per
+// tracer.  A block whose tracers span more planes reads the table directly.
+// Per tracer: K = exp((1 - t) log K_ib + t log K_ib+1) where both ends are
+// positive, the linear blend otherwise, clamped ends at t = 0 and 1.
+constexpr int kSynWarps = 8;
+
+__device__ __forceinline__ void synch_plane(double bval_in, double logb_min, double inv_dlogb, int nlogb, int &ib,
+                                            double &tw)
+{
+    double bval = bval_in;
+    if (!(bval > 0.0) || !isfinite(bval)) bval = 1.0e-30;
+    const double lb = log10(bval / 1.0e-6);
+    const double u = (lb - logb_min) * inv_dlogb;
+    ib = (int)floor(u);
+    if (ib < 0) ib = 0;
+    if (ib > nlogb - 2) ib = nlogb - 2;
+    tw = u - (double)ib;
+    if (tw < 0.0) tw = 0.0;
+    if (tw > 1.0) tw = 1.0;
+}
+
+__global__ void synch_plane_kernel(int ntracer, int nlogb, double logb_min, double inv_dlogb, const double *bfield,
+                                   int *key, int *idx)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntracer) return;
+    int ib;
+    double tw;
+    synch_plane(bfield[t], logb_min, inv_dlogb, nlogb, ib, tw);
+    key[t] = ib;
+    idx[t] = t;
+}
+
+struct SynRows {
+    double K[3][NB], L[3][NB];
+};
+
+__global__ void __launch_bounds__(kSynWarps * 32, 3) synch_sorted_kernel(
+    int ntracer, int nfreq, int nlogb, double logb_min, double inv_dlogb, SynchPrefactor sp, const double *K,
+    const double *logK, const int *order, const double *bfield, const double *cre, const double *dp, double *out)
 {
     constexpr int R = NB / 32;
-    const int lane = threadIdx.x & 31;
-    const long long t = (long long)blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (t >= ntracer) return;
+    extern __shared__ double4 syn_smem[];
+    SynRows &rows = *reinterpret_cast<SynRows *>(syn_smem);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long first = (long long)blockIdx.x * kSynWarps;
+    const long long last = min((long long)ntracer, first + kSynWarps) - 1;
+    const long long pos = first + w;
+    const bool active = pos < ntracer;
+    // the block's plane range (sorted: first and last tracer bound it)
+    int ib_lo, ib_hi;
+    double tw_unused;
+    synch_plane(bfield[order[first]], logb_min, inv_dlogb, nlogb, ib_lo, tw_unused);
+    synch_plane(bfield[order[last]], logb_min, inv_dlogb, nlogb, ib_hi, tw_unused);
+    const bool staged = ib_hi - ib_lo <= 1;
+    const int nplanes = staged ? ib_hi - ib_lo + 2 : 0;
+    const int t = active ? order[pos] : 0;
     const double *N = cre + (size_t)t * NB;
     int stop = NB - 1;
     for (int j0 = 2; j0 < NB - 1; j0 += 32) {
@@ -302,43 +356,52 @@ __global__ void __launch_bounds__(128) synch_resident_kernel(int ntracer, int nf
 #pragma unroll
     for (int r = 0; r < R; r++) {
         const int je = 32 * r + lane;
-        nd[r] = (je >= 2 && je < stop) ? N[je] : 0.0;
+        nd[r] = (active && je >= 2 && je < stop) ? N[je] * dp[je] : 0.0;
     }
-    double bval = bfield[t];
-    if (!(bval > 0.0) || !isfinite(bval)) bval = 1.0e-30;
-    const double lb = log10(bval / 1.0e-6);
-    const double A = sp.a0 * bfield[t] / sp.den1 / sp.den2;
-    const double u = (lb - logb_min) * inv_dlogb;
-    int ib = (int)floor(u);
-    if (ib < 0) ib = 0;
-    if (ib > nlogb - 2) ib = nlogb - 2;
-    double tw = u - (double)ib;
-    if (tw < 0.0) tw = 0.0;
-    if (tw > 1.0) tw = 1.0;
+    int ib;
+    double tw;
+    synch_plane(active ? bfield[t] : 1.0, logb_min, inv_dlogb, nlogb, ib, tw);
+    const double A = active ? sp.a0 * bfield[t] / sp.den1 / sp.den2 : 0.0;
+    const int s0 = ib - ib_lo;   // staged row of plane ib
     for (int nf = 0; nf < nfreq; nf++) {
+        if (staged) {
+            __syncthreads();
+            for (int i = threadIdx.x; i < nplanes * NB; i += blockDim.x) {
+                const int pl = i / NB, je = i % NB;
+                const size_t o = ((size_t)(ib_lo + pl) * nfreq + nf) * NB + je;
+                rows.K[pl][je] = __ldg(K + o);
+                rows.L[pl][je] = __ldg(logK + o);
+            }
+            __syncthreads();
+        }
+        if (!active) continue;
         const size_t o0 = ((size_t)ib * nfreq + nf) * NB, o1 = ((size_t)(ib + 1) * nfreq + nf) * NB;
-        double s = 0.0;
+        double sum = 0.0;
 #pragma unroll
         for (int r = 0; r < R; r++) {
             const int je = 32 * r + lane;
             if (nd[r] == 0.0) continue;
             double Kv;
             if (tw <= 0.0) {
-                Kv = __ldg(K + o0 + je);
+                Kv = staged ? rows.K[s0][je] : __ldg(K + o0 + je);
             } else if (tw >= 1.0) {
-                Kv = __ldg(K + o1 + je);
+                Kv = staged ? rows.K[s0 + 1][je] : __ldg(K + o1 + je);
             } else {
-                const double la = __ldg(logK + o0 + je), lb = __ldg(logK + o1 + je);
-                if (!isnan(la) && !isnan(lb))
+                const double la = staged ? rows.L[s0][je] : __ldg(logK + o0 + je);
+                const double lb = staged ? rows.L[s0 + 1][je] : __ldg(logK + o1 + je);
+                if (!isnan(la) && !isnan(lb)) {
                     Kv = exp((1.0 - tw) * la + tw * lb);
-                else
-                    Kv = (1.0 - tw) * __ldg(K + o0 + je) + tw * __ldg(K + o1 + je);
+                } else {
+                    const double ka = staged ? rows.K[s0][je] : __ldg(K + o0 + je);
+                    const double kb = staged ? rows.K[s0 + 1][je] : __ldg(K + o1 + je);
+                    Kv = (1.0 - tw) * ka + tw * kb;
+                }
             }
-            s += nd[r] * Kv * dp[je];
+            sum += nd[r] * Kv;
         }
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(kFull, s, off);
-        if (lane == 0) out[(size_t)t * nfreq + nf] = A * s;
+        for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(kFull, sum, off);
+        if (lane == 0) out[(size_t)t * nfreq + nf] = A * sum;
     }
 }
 
@@ -454,7 +517,11 @@ struct EmissionState {
     int ic_rebuilt = 0;                       // the last run rebuilt the IC table (2 more launches)
     double inv_dlogb = 0.0;
     size_t bytes = 0;
-    double *h_tables = nullptr;               // host copy for croma_b200_emission_tables (on request)
+    // tracer order of the synchrotron kernel (sorted by log-B plane)
+    int *d_key = nullptr, *d_key_alt = nullptr, *d_idx = nullptr, *d_idx_alt = nullptr;
+    void *d_sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
+    int sort_cap = 0;
 };
 
 void free_emission(Context &c)
@@ -462,6 +529,8 @@ void free_emission(Context &c)
     if (!c.emission) return;
     EmissionState *e = c.emission;
     if (e->d_block) dev_free(c, e->d_block);
+    for (void *p : {(void *)e->d_key, (void *)e->d_key_alt, (void *)e->d_idx, (void *)e->d_idx_alt, e->d_sort_tmp})
+        if (p) dev_free(c, p);
     delete e;
     c.emission = nullptr;
 }
@@ -488,8 +557,8 @@ int setup_emission(Context &c, const CromaB200EmissionSetup *s)
     if (!s) return fail_msg(-1, "null emission setup");
     if (s->nfreq < 0 || s->nbins_ic < 0 || s->nbins_gamma < 0 || s->nbins_nu < 0)
         return fail_msg(-1, "negative band count");
-    if (s->nfreq > 0 && (s->ntheta_pitch <= 0 || s->nlogb < 2 || !(s->logb_max > s->logb_min)))
-        return fail_msg(-1, "synchrotron needs ntheta_pitch > 0, nlogb >= 2 and logb_max > logb_min");
+    if (s->nfreq > 0 && (s->ntheta_pitch <= 0 || s->nlogb < 2 || s->nlogb > 65536 || !(s->logb_max > s->logb_min)))
+        return fail_msg(-1, "synchrotron needs ntheta_pitch > 0, 2 <= nlogb <= 65536 and logb_max > logb_min");
     if ((s->nfreq > 0 || s->nbins_ic > 0) && !(c.mp.species_mask & CROMA_SPECIES_ELECTRON))
         return fail_msg(-1, "synchrotron / IC emission needs the electron species");
     if ((s->nbins_gamma > 0 || s->nbins_nu > 0) && !(c.mp.species_mask & CROMA_SPECIES_PROTON))
@@ -663,9 +732,39 @@ int emission_run(Context &c, const double *bg, double z, double *eps_syn, double
     if (eps_nu && s.nbins_nu > 0)
         CROMA_CUDA(launch_gemm(n, s.nbins_nu, e->wp_nu, c.d_crp, e->d_w_nu, bg, 1, eps_nu, st));
     if (eps_syn && s.nfreq > 0) {
-        synch_resident_kernel<<<(n + 3) / 4, 128, 0, st>>>(n, s.nfreq, s.nlogb, s.logb_min, e->inv_dlogb,
-                                                           synch_prefactor(), e->d_K, e->d_logK, bg + 2 * (size_t)n,
-                                                           c.d_cre, c.gt.s[1].dp, eps_syn);
+        const double *bfield = bg + 2 * (size_t)n;
+        if (e->sort_cap < n) {
+            for (void *p : {(void *)e->d_key, (void *)e->d_key_alt, (void *)e->d_idx, (void *)e->d_idx_alt,
+                            e->d_sort_tmp})
+                if (p) dev_free(c, p);
+            e->d_key = e->d_key_alt = e->d_idx = e->d_idx_alt = nullptr;
+            e->d_sort_tmp = nullptr;
+            e->sort_cap = 0;
+            CROMA_CUDA(dev_alloc(c, &e->d_key, (size_t)n * sizeof(int)));
+            CROMA_CUDA(dev_alloc(c, &e->d_key_alt, (size_t)n * sizeof(int)));
+            CROMA_CUDA(dev_alloc(c, &e->d_idx, (size_t)n * sizeof(int)));
+            CROMA_CUDA(dev_alloc(c, &e->d_idx_alt, (size_t)n * sizeof(int)));
+            cub::DoubleBuffer<int> kb(e->d_key, e->d_key_alt), vb(e->d_idx, e->d_idx_alt);
+            size_t bytes = 0;
+            CROMA_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kb, vb, n, 0, 16, st));
+            CROMA_CUDA(dev_alloc_bytes(c, &e->d_sort_tmp, bytes ? bytes : 16));
+            e->sort_tmp_bytes = bytes;
+            e->sort_cap = n;
+        }
+        synch_plane_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, s.nlogb, s.logb_min, e->inv_dlogb, bfield, e->d_key,
+                                                             e->d_idx);
+        CROMA_CUDA(cudaGetLastError());
+        // plane indices are below 2^16 (nlogb is bounded by the table's size)
+        cub::DoubleBuffer<int> kb(e->d_key, e->d_key_alt), vb(e->d_idx, e->d_idx_alt);
+        size_t bytes = e->sort_tmp_bytes;
+        CROMA_CUDA(cub::DeviceRadixSort::SortPairs(e->d_sort_tmp, bytes, kb, vb, n, 0, 16, st));
+        constexpr size_t smem = sizeof(SynRows);
+        static const cudaError_t attr =
+            cudaFuncSetAttribute(synch_sorted_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        CROMA_CUDA(attr);
+        synch_sorted_kernel<<<(n + kSynWarps - 1) / kSynWarps, kSynWarps * 32, smem, st>>>(
+            n, s.nfreq, s.nlogb, s.logb_min, e->inv_dlogb, synch_prefactor(), e->d_K, e->d_logK, vb.Current(),
+            bfield, c.d_cre, c.gt.s[1].dp, eps_syn);
         CROMA_CUDA(cudaGetLastError());
     }
     return 0;
@@ -679,7 +778,7 @@ int emission_launches(const Context &c, bool syn, bool ic, bool gamma, bool nu)
 {
     const EmissionState *e = c.emission;
     if (!e) return 0;
-    return (syn && e->cfg.nfreq > 0) + (ic && e->cfg.nbins_ic > 0) * (1 + 2 * e->ic_rebuilt) +
+    return 3 * (syn && e->cfg.nfreq > 0) + (ic && e->cfg.nbins_ic > 0) * (1 + 2 * e->ic_rebuilt) +
            (gamma && e->cfg.nbins_gamma > 0) + (nu && e->cfg.nbins_nu > 0);
 }
 
