@@ -580,15 +580,6 @@ int croma_b200_step_host(CromaB200Context *h, const CromaB200Snapshot *s, const 
     }
     // 3. emission of the spectra the snapshot starts from, downloaded on the
     //    copy stream while the evolve runs
-    double *d_emis = nullptr;
-    struct Guard {
-        Context &c;
-        double *&p;
-        ~Guard()
-        {
-            if (p) dev_free(c, p);
-        }
-    } guard{c, d_emis};
     if (want_emis) {
         const CromaB200EmissionSetup &es = emission_config(c);
         double *host[4] = {io->eps_syn, io->eps_ic, io->eps_gamma, io->eps_nu};
@@ -596,7 +587,10 @@ int croma_b200_step_host(CromaB200Context *h, const CromaB200Snapshot *s, const 
                              host[3] ? es.nbins_nu : 0};
         size_t total = 0;
         for (int k = 0; k < 4; k++) total += n * (size_t)cols[k];
-        CROMA_CUDA(dev_alloc(c, &d_emis, (total ? total : 1) * sizeof(double)));
+        // the device outputs stay allocated across calls (grow-only), so a
+        // step does not map and unmap gigabytes of device memory each time
+        double *d_emis = nullptr;
+        CROMA_CUDA(emission_out_block(c, (total ? total : 1) * sizeof(double), &d_emis));
         double *dev[4];
         double *q = d_emis;
         for (int k = 0; k < 4; k++) {

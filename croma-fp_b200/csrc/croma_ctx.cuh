@@ -240,6 +240,8 @@ int emission_run(Context &c, const double *bg_dev, double z, double *eps_syn, do
                  double *eps_nu);
 int emission_tables(Context &c, int which, double *out);
 const CromaB200EmissionSetup &emission_config(const Context &c);
+// a device block of at least `bytes` for step outputs, kept by the emission state
+cudaError_t emission_out_block(Context &c, size_t bytes, double **out);
 // kernels one emission_run call launches for the requested kinds
 int emission_launches(const Context &c, bool syn, bool ic, bool gamma, bool nu);
 void free_emission(Context &c);

@@ -517,6 +517,9 @@ struct EmissionState {
     int ic_rebuilt = 0;                       // the last run rebuilt the IC table (2 more launches)
     double inv_dlogb = 0.0;
     size_t bytes = 0;
+    // device outputs of croma_b200_step_host (grow-only)
+    double *d_out = nullptr;
+    size_t out_bytes = 0;
     // tracer order of the synchrotron kernel (sorted by log-B plane)
     int *d_key = nullptr, *d_key_alt = nullptr, *d_idx = nullptr, *d_idx_alt = nullptr;
     void *d_sort_tmp = nullptr;
@@ -529,7 +532,8 @@ void free_emission(Context &c)
     if (!c.emission) return;
     EmissionState *e = c.emission;
     if (e->d_block) dev_free(c, e->d_block);
-    for (void *p : {(void *)e->d_key, (void *)e->d_key_alt, (void *)e->d_idx, (void *)e->d_idx_alt, e->d_sort_tmp})
+    for (void *p : {(void *)e->d_key, (void *)e->d_key_alt, (void *)e->d_idx, (void *)e->d_idx_alt, e->d_sort_tmp,
+                    (void *)e->d_out})
         if (p) dev_free(c, p);
     delete e;
     c.emission = nullptr;
@@ -773,6 +777,22 @@ int emission_run(Context &c, const double *bg, double z, double *eps_syn, double
 int emission_setup(Context &c, const CromaB200EmissionSetup *s) { return setup_emission(c, s); }
 
 const CromaB200EmissionSetup &emission_config(const Context &c) { return c.emission->cfg; }
+
+cudaError_t emission_out_block(Context &c, size_t bytes, double **out)
+{
+    EmissionState *e = c.emission;
+    if (!e) return cudaErrorInvalidValue;
+    if (e->out_bytes < bytes) {
+        if (e->d_out) dev_free(c, e->d_out);
+        e->d_out = nullptr;
+        e->out_bytes = 0;
+        const cudaError_t er = dev_alloc(c, &e->d_out, bytes);
+        if (er != cudaSuccess) return er;
+        e->out_bytes = bytes;
+    }
+    *out = e->d_out;
+    return cudaSuccess;
+}
 
 int emission_launches(const Context &c, bool syn, bool ic, bool gamma, bool nu)
 {

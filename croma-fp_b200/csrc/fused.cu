@@ -55,9 +55,10 @@ constexpr int kSw = kPitch * kR;     // swizzled row-array length
 constexpr int kWarps = 1;            // warps per block
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kFacDoubles = 3 * NB;  // 1/d, a/d, c/d of one system
-// warps per factor-kernel block: at nb = 256 two 9-warp blocks (106 KB of
-// shared memory each, at most 113 registers a thread) fill an SM
-constexpr int kFacWarps = 9;
+// warps per factor-kernel block: at nb <= 256 two 9-warp blocks (at most 113
+// registers a thread) fill an SM; at nb = 512 one 12-warp block (at most 170
+// registers, 160 KB of shared memory: the tables and each warp's B and C)
+constexpr int kFacWarps = (NB <= 256 ? 8 : 12);
 
 // Grid tables of one species staged in shared memory by the factor kernel.
 // X0..X3: protons expE, cp_Ep, cp_inv2mpkin, cp_inv_betap2; electrons
@@ -277,7 +278,7 @@ __device__ __forceinline__ SegTerms<S> seg_terms_pre(const GridTables &gt, const
 }
 
 struct WarpSmem {
-    double B[kSw], C[kSw], Wp[kSw], Wm[kSw];
+    double B[kSw], C[kSw];
 };
 
 
@@ -307,43 +308,45 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
         sm.C[sb0 + k * kStep] = C;
     }
     __syncwarp();
-    // faces j (between bins j and j+1), lane-strided.  The drift / diffusion
-    // ratio (B_j + B_j+1) / (C_j + C_j+1) * dx: with the filled Dpp form the C
-    // sum is kappa times a grid factor, so the division becomes a product with
-    // the tabulated dx / (g_j + g_j+1) and 1 / kappa (equal to a few ulp).
+    // Faces j (between bins j and j+1), computed in registers where the rows
+    // use them: lane l's rows m = l R + r need faces m - 1 and m, so the lane
+    // evaluates faces l R - 1 .. l R + R - 1 (the first one its left
+    // neighbour evaluates too).  The drift / diffusion ratio
+    // (B_j + B_j+1) / (C_j + C_j+1) * dx: with the filled Dpp form the C sum
+    // is kappa times a grid factor, so the division becomes a product with the
+    // tabulated dx / (g_j + g_j+1) and 1 / kappa (equal to a few ulp).  The
+    // division form is taken only when a lane of the warp needs it (the vote
+    // keeps it from being computed predicated on every face).  Faces -1 and
+    // nb - 1 do not exist.
     const double inv_kappa = T.dpp_fill ? 1.0 / (T.dpp_inv * T.dpp_scale) : 0.0;
-    // The division form is taken only when a lane of the warp needs it (the
-    // vote keeps it from being computed predicated on every face).  Face
-    // nb - 1 does not exist: its position swz(nb) is a padding word, read but
-    // never used.
-#pragma unroll 2
-    for (int k = 0; k < kR; k++) {
-        const int j = k * 32 + lane;
-        const int s0 = sb0 + k * kStep, s1 = sb1 + k * kStep;
-        double wp = 0.0, wm = 0.0;
-        const double cl = sm.C[s0];
-        const bool live = (j <= NB - 2) && fabs(cl) > 1.0e-200;
-        const double bsum = sm.B[s0] + sm.B[s1];
-        const double rf = tab[TB_RF * kTabStride + j] * inv_kappa;
+    auto face = [&](int j, int sj, int sj1, double &wp, double &wm) {
+        wp = 0.0;
+        wm = 0.0;
+        const bool exists = j >= 0 && j <= NB - 2;
+        const double cl = exists ? sm.C[sj] : 0.0;
+        const bool live = exists && fabs(cl) > 1.0e-200;
+        const double bsum = exists ? sm.B[sj] + sm.B[sj1] : 0.0;
+        const double rf = exists ? tab[TB_RF * kTabStride + sj] * inv_kappa : 0.0;
         const bool divide = live && !(T.dpp_fill && isfinite(rf));
         double w = bsum * rf;
         if (__any_sync(kFull, divide)) {
-            if (divide) w = bsum / (cl + sm.C[s1]) * tab[TB_DXF * kTabStride + j];
+            if (divide) w = bsum / (cl + sm.C[sj1]) * tab[TB_DXF * kTabStride + sj];
         }
         if (live) face_weights_fast(w, wp, wm);
-        sm.Wp[s0] = wp;
-        sm.Wm[s0] = wm;
-    }
-    __syncwarp();
+    };
 
     // rows a, b, c of this lane (cc_build_{left,interior,right}, Chang_Cooper.c:66-184)
     const int row0 = lane * kR;
+    double wpm, wmm;   // face m - 1
+    face(row0 - 1, lane > 0 ? (kR - 1) * kPitch + lane - 1 : 0, lane, wpm, wmm);
 #pragma unroll
     for (int r = 0; r < kR; r++) {
         const int m = row0 + r;
         const int sm_m = r * kPitch + lane;
         const int sm_p = r > 0 ? (r - 1) * kPitch + lane : (kR - 1) * kPitch + lane - 1;   // swz(m - 1), m >= 1
         const int sm_n = r < kR - 1 ? (r + 1) * kPitch + lane : lane + 1;                  // swz(m + 1)
+        double wpc, wmc;   // face m
+        face(m, sm_m, sm_n, wpc, wmc);
         const double k = T.dt * tab[TB_IDX * kTabStride + r * kPitch + lane];
         const double Cm = sm.C[r * kPitch + lane], Bm = sm.B[r * kPitch + lane], Dm = T.row_dT(tab, r, lane);
         double av = 0.0, bv, cv = 0.0;
@@ -351,15 +354,14 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
             const double nC = sm.C[sm_n], nB = sm.B[sm_n];
             if (fabs(Cm) > 1.0e-200) {
                 const double cm12 = 0.5 * (Cm + nC) * tab[TB_IDXR * kTabStride + r * kPitch + lane];
-                bv = 1.0 + k * (0.0 + cm12 * sm.Wm[sm_m]) + Dm;
-                cv = k * cm12 * sm.Wp[sm_m];
+                bv = 1.0 + k * (0.0 + cm12 * wmc) + Dm;
+                cv = k * cm12 * wpc;
             } else {
                 bv = 1.0 + k * 0.0 + Dm;
                 cv = k * 1.0 * 0.5 * (Bm + nB);
             }
         } else {
             const double pC = sm.C[sm_p], pB = sm.B[sm_p];
-            const double wpm = sm.Wp[sm_p], wmm = sm.Wm[sm_p];
             if (m == NB - 1) {
                 if (fabs(Cm) > 1.0e-200) {
                     const double cm_12 = 0.5 * (Cm + pC) * tab[TB_IDXL * kTabStride + r * kPitch + lane];
@@ -379,8 +381,8 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
                     const double cm_12 = 0.5 * (Cm + pC) * tab[TB_IDXL * kTabStride + r * kPitch + lane];
                     const double cm12 = 0.5 * (Cm + nC) * tab[TB_IDXR * kTabStride + r * kPitch + lane];
                     av = k * cm_12 * wmm;
-                    bv = 1.0 + k * (cm_12 * wpm + cm12 * sm.Wm[sm_m]) + Dm;
-                    cv = k * cm12 * sm.Wp[sm_m];
+                    bv = 1.0 + k * (cm_12 * wpm + cm12 * wmc) + Dm;
+                    cv = k * cm12 * wpc;
                 } else {
                     // interior row below the diffusion floor: every delta the
                     // reference reads here is zero (Chang_Cooper.c:91-103)
@@ -389,6 +391,8 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
                 }
             }
         }
+        wpm = wpc;
+        wmm = wmc;
         A[r] = av;
         Bd[r] = bv;
         Cc[r] = cv;
@@ -504,8 +508,8 @@ __global__ void __launch_bounds__(kFacWarps * 32, (NB <= 256 ? 2 : 1)) factor_ke
         tab[TB_P2 * kTabStride + i] = st.p2[i];
         tab[TB_CUT * kTabStride + i] = st.exp_cut[i];
         tab[TB_2P * kTabStride + i] = st.two_over_p[i];
-        tab[TB_DXF * kTabStride + i] = st.dxf[i];
-        tab[TB_RF * kTabStride + i] = st.face_rf[i];
+        tab[TB_DXF * kTabStride + swz(i)] = st.dxf[i];
+        tab[TB_RF * kTabStride + swz(i)] = st.face_rf[i];
         if (S == 0) {
             tab[TB_X0 * kTabStride + i] = st.expE[i];
             tab[TB_X1 * kTabStride + i] = P.gt.cp_Ep[i];
@@ -1401,10 +1405,26 @@ int tridiag_env()
 // variant runs the chunk's first tracers (at most 2,048) for their first 16
 // sub-steps on a copy of their spectra, timed with CUDA events; the fastest
 // is kept for the context's species.  Results are recorded in ctx.tune.
+// CROMA_B200_STEPS_VARIANT = 0..3 fixes the variant (scan x1, x2, x4, PCR)
+// without calibrating, for reproducible profiles; unset or out of range: tune.
+int fixed_variant_env()
+{
+    const char *e = getenv("CROMA_B200_STEPS_VARIANT");
+    if (!e || !*e) return -1;
+    const int v = atoi(e);
+    return (v >= 0 && v < kStepVariants) ? v : -1;
+}
+
 template <int S>
 int tune_steps(Context &ctx, const FusedParams &P, bool src)
 {
     TuneState &tu = ctx.tune[S];
+    const int fixed = fixed_variant_env();
+    if (fixed >= 0) {
+        tu.variant = fixed;
+        tu.tuned = 1;
+        return 0;
+    }
     const int env = tridiag_env();
     const int T = min(P.nt, 2048), steps = 16;
     double *scratch = nullptr;

@@ -326,7 +326,9 @@ int croma_b200_step_host(CromaB200Context *ctx, const CromaB200Snapshot *snap, c
  * only PCR (src/fp_cuda_solver.cu:41-72 of the reference).  Reported here:
  * tuned (0 before the first snapshot), solver (0 scan, 1 FP32-refined scan,
  * 2 PCR), tracers per block, and the calibration time of each variant in
- * milliseconds (variant order: scan x1, scan x2, scan x4, PCR; -1 = not run). */
+ * milliseconds (variant order: scan x1, scan x2, scan x4, PCR; -1 = not run).
+ * CROMA_B200_STEPS_VARIANT=0..3 fixes the variant in that order without
+ * calibrating (reproducible profiles). */
 int croma_b200_get_tuning(CromaB200Context *ctx, int species, int *tuned, int *solver, int *warps_per_block,
                           double *variant_ms);
 
