@@ -49,10 +49,13 @@ DSA_FRACTION = 0.05
 METRIC = "tracer-snapshot updates/s at <=1e-6 rel err vs FP64, chosen vs plain; p50/p99 latency"
 UNIT = "tracer-snapshot updates/s"
 SHOCK_KEYS = ("mach", "prestemp", "presden", "shock_side_code")
-# DRAM bytes per tracer of one launch of each kernel, from the ncu captures
-# of this workload's kernels at 16,384 tracers (profiles/*_full_pipeline_e_p_512.txt;
-# every tracer moves its own rows, so traffic scales with the tracer count)
-NCU_DRAM_BYTES_PER_TRACER = {}
+# DRAM bytes (read + write) per tracer of one launch of each kernel, from the
+# ncu captures of this workload's kernels at 16,384 tracers
+# (profiles/*_full_pipeline_e_p_512.txt: DRAM rate x duration / 16,384).  Every
+# tracer moves its own rows, so a launch's traffic is this figure times the
+# tracers it processes.  steps: mean of the proton and electron launches;
+# plain_steps: the electron launch of one segment slot.
+NCU_DRAM_BYTES_PER_TRACER = {"steps": (272.35e3 + 270.86e3) / 2, "plain_steps": 23.79e3}
 
 
 def load_package():
@@ -555,12 +558,13 @@ def roofline_fused(cfg, nt, res, steps, fp64_peak, peaks, peak_kind):
     launches_per_snapshot = max(1, ev_n // steps)
     alg_bytes_snapshot = (float(np.sum(nseg)) * 3 * nb * 8 * 2 + nt * nb * 16 * 2 + float(np.sum(nseg)) * nb * 8)
     alg_bytes_launch = alg_bytes_snapshot / launches_per_snapshot
-    traffic = None
-    if "steps" in NCU_DRAM_BYTES_PER_TRACER:
-        traffic = NCU_DRAM_BYTES_PER_TRACER["steps"] * nt / launches_per_snapshot * 2
+    # tracer-launches per snapshot: both species over every chunk
+    traffic = NCU_DRAM_BYTES_PER_TRACER["steps"] * 2 * nt / launches_per_snapshot if cfg.nb == 512 else None
     ms_total = res["ms"]
     return {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
             "frac": achieved / fp64_peak, "traffic": traffic,
+            "traffic_source": "ncu DRAM bytes per tracer-launch (profiles/steps_kernel_*_full_pipeline_e_p_512.txt) "
+                              "x tracers per launch",
             "peak_source": "measured live: croma_b200_fp64_peak (FMA chains on every SM)",
             "kernel": "steps_kernel (proton and electron launches per workspace chunk)",
             "launches": ev_n, "kernel_ms_total": ev_ms, "share_of_step": ev_ms / ms_total,
@@ -585,11 +589,14 @@ def roofline_plain(cfg, nt, res, steps, peaks, peak_kind):
     avg_ms = ev_ms / max(1, ev_n)
     achieved = per_launch / (avg_ms / 1e3) / 1e9
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    traffic = None
-    if "plain_steps" in NCU_DRAM_BYTES_PER_TRACER:
-        traffic = NCU_DRAM_BYTES_PER_TRACER["plain_steps"] * nt * steps / max(1, ev_n)
+    # tracer-launches per snapshot: both species over every segment slot and chunk
+    nslot = 16
+    traffic = (NCU_DRAM_BYTES_PER_TRACER["plain_steps"] * 2 * nslot * nt * steps / max(1, ev_n)
+               if cfg.nb == 512 else None)
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "peak_source": peak_kind,
+            "traffic_source": "ncu DRAM bytes per tracer-launch (profiles/plain_steps_kernel_electrons_full_pipeline_"
+                              "e_p_512.txt) x tracers per launch",
             "frac_meaning": "contract bytes (the reference's per-step data contract) per second; each warp runs "
                             "its slot's sub-steps back to back, so the per-step re-reads hit L2 and DRAM itself "
                             "sees a few per cent of these bytes (traffic)",
@@ -729,26 +736,36 @@ def run_heavy_tail(args):
     direct t_acc), whose nsub spread from 11 to the cap of 500 with a heavy
     tail (median ~12, 90th percentile ~200-370), against the same tracers on
     the full [0.1, 1e6] grid where every nsub is 500.  Reported: throughput,
-    the nsub distribution, sub-step rate (sum of nsub x nb per second) and
-    its ratio to the uniform workload's (the balance of uneven work)."""
+    the nsub distribution, and the balance of the uneven run: the steps and
+    factor kernels' time predicted from the uniform run's cost per tracer
+    sub-step and per factored segment, divided by the time measured (1.0:
+    the uneven work costs exactly its share, no idle tail)."""
     import torch
     from croma_fp_b200 import config, synth
     nt = args.heavy_tail_tracers
     out = {}
-    for name, cfg in (("heavy_tail", config.config0(pemin=1.0, pemax=3.0, nsub_max=500)),
-                      ("uniform", config.config0(nsub_max=500))):
+    for name, cfg in (("uniform", config.config0(nsub_max=500)),
+                      ("heavy_tail", config.config0(pemin=1.0, pemax=3.0, nsub_max=500))):
         w = synth.Workload(cfg, nt, NSNAP_TIMELINE, seed=SEED + 17)
         snaps = [45 + k for k in range(6)]
         bg = torch.stack([torch.from_numpy(w.background(s_)) for s_ in range(snaps[0], snaps[-1] + 2)]).cuda()
-        r = run_resident("fused", cfg, nt, w, bg, None, snaps, 2, 4, emission=False, dsa=False)
+        r = run_resident("fused", cfg, nt, w, bg, None, snaps, 2, 4, emission=False, dsa=False, kernel_timing=True)
         nsub = r["sched"]["nsub"].astype(np.float64)
-        rate = float(np.sum(nsub)) * cfg.nb * 4 / (r["ms"] / 1e3)
+        nseg = np.array([coeff_segments(cfg, int(x)) for x in r["sched"]["nsub"]], dtype=np.float64)
         out[name] = {"value": nt * 4 / (r["ms"] / 1e3), "ms_per_step": r["ms"] / 4,
                      "nsub_percentiles_0_10_50_90_99_100": [float(x) for x in
                                                             np.percentile(nsub, [0, 10, 50, 90, 99, 100])],
-                     "substep_row_rate": rate}
+                     "steps_ms_per_step": r["evolve"][0] / 4, "factor_ms_per_step": r["coeff"][0] / 4,
+                     "sum_nsub": float(nsub.sum()), "sum_nseg": float(nseg.sum())}
         del bg
-    out["balance"] = out["heavy_tail"]["substep_row_rate"] / out["uniform"]["substep_row_rate"]
+    u, h = out["uniform"], out["heavy_tail"]
+    c_step = u["steps_ms_per_step"] / u["sum_nsub"]
+    c_fac = u["factor_ms_per_step"] / u["sum_nseg"]
+    predicted = c_step * h["sum_nsub"] + c_fac * h["sum_nseg"]
+    measured = h["steps_ms_per_step"] + h["factor_ms_per_step"]
+    out["balance"] = predicted / measured
+    out["balance_rule"] = ("(uniform run's steps ms per tracer sub-step x heavy-tail sum nsub + its factor ms per "
+                           "segment x heavy-tail sum nseg) / heavy-tail steps + factor ms")
     out["workload"] = (f"{nt} tracers, electron-only, 128 bins, direct t_acc 0.3 Gyr; heavy_tail: electron grid "
                        f"[10, 1e3], uniform: [0.1, 1e6]; 4 timed snapshots after 2")
     return out

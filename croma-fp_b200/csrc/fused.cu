@@ -1057,7 +1057,7 @@ __global__ void __launch_bounds__(WPB * 32, (NB <= 256 ? 16 : 8) / WPB) steps_ke
 // with the pivots recomputed (tracer_fp_cpu_evolve, src/tracer_fp_cpu.c:149-190;
 // fp_thomas_solve_ws, src/fp_shared_core.c:226-257) and writes N back.
 template <int S, bool SRC>
-__global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 20 : 10)) plain_steps_kernel(FusedParams P)
+__global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 20 : 12)) plain_steps_kernel(FusedParams P)
 {
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;

@@ -5,6 +5,7 @@ driven through ctypes exactly as CROMA's snapshot driver calls it
 Bar: spectra within 1e-10 relative on bins above 1e-12 of each tracer's
 peak; the emission and batch-solve entry points within 1e-12."""
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -299,3 +300,47 @@ def test_solve_cc_cuda_batch_pcr_when_requested(monkeypatch):
     assert rel_err(out, ref) <= 1e-12
     monkeypatch.setenv("CROMA_CUDA_TRIDIAG", "thomas")
     assert abi.lib.fp_cuda_tridiag_uses_pcr(128) == 0
+
+
+CALLER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                      "abi_caller_np128")
+
+
+@pytest.mark.skipif(not os.path.exists(CALLER), reason="C caller not built (needs the reference's headers)")
+def test_c_caller_compiled_against_reference_header():
+    """oracle/abi_caller.c, compiled against the reference's own
+    fp_cuda_backend.h / fp_shared_core.h / params.h and linked to
+    libcroma_b200_np128.so, runs cuda_rank_state_upload -> run_tracer_pipeline
+    (gather and scatter through the rank state) -> cuda_rank_state_download;
+    its spectra match the oracle's segment within 1e-10."""
+    import subprocess
+    import tempfile
+    cfg, o, abi, w, gp, ge, crp, cre, qpi, qepri, dis = _setup(nt=48, seed=33)
+    nt = crp.shape[0]
+    bg = w.background(9)
+    row, m1, p1 = o.ic_row(0.55)
+    ric = np.ascontiguousarray(np.repeat(row[:, None], nt, axis=1))
+    m1s, p1s = np.full(nt, m1), np.full(nt, p1)
+    nstep, dt, windowed, on0, on1 = 7, 3.0e-4, 1, 1, 5
+    o_crp, o_cre = crp.copy(), cre.copy()
+    o.evolve_segment(nstep, dt, windowed, on0, on1, bg, ric, m1s, p1s, qpi, qepri, o_crp, o_cre,
+                     mass=w.mass, dis=dis)
+    with tempfile.TemporaryDirectory() as d:
+        fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(np.array([nt, nstep, windowed, on0, on1, cfg.dpp_model_id(), cfg.ttd_tacc_model],
+                             np.int32).tobytes())
+            f.write(np.array([dt, cfg.t_acc_direct_gyr, cfg.eta_dpp_cap]).tobytes())
+            for g in (gp, ge):
+                f.write(np.concatenate([g[0], g[1], g[2], [g[3], g[4]]]).astype(np.float64).tobytes())
+            for a in (bg, ric, m1s, p1s, w.mass):
+                f.write(np.ascontiguousarray(a, np.float64).tobytes())
+            f.write(np.ascontiguousarray(dis, np.uint8).tobytes())
+            for a in (crp, cre, qpi, qepri):
+                f.write(np.ascontiguousarray(a, np.float64).tobytes())
+        r = subprocess.run([CALLER, fin, fout], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        out = np.fromfile(fout, np.float64)
+    g_crp, g_cre = out[:nt * 128].reshape(nt, 128), out[nt * 128:].reshape(nt, 128)
+    assert rel_err(g_crp, o_crp) <= RTOL
+    assert rel_err(g_cre, o_cre) <= RTOL
