@@ -253,7 +253,9 @@ def run_resident(path, cfg, nt, w, bg_dev, sh_dev, snaps, warmup, steps, emissio
             if timed:
                 e1.record(stream)
                 emis_events.append((e0, e1))
-            launches += 6   # 3 GEMMs, synchrotron, IC table + weights (z changes every snapshot)
+            # 3 GEMMs, the IC table and its weights (z changes every snapshot),
+            # the synchrotron plane keys, the radix sort's 4 kernels, the synchrotron
+            launches += 12
         fp.snapshot(bg_dev[k].data_ptr(), bg_dev[k + 1].data_ptr(), float(w.z[isnap]), float(w.z[isnap + 1]),
                     True, float(w.dt[isnap]), float(w.elapsed[isnap]), sync=False)
         launches += fp.last_launch_count()

@@ -823,7 +823,7 @@ int croma_b200_get_tuning(CromaB200Context *h, int species, int *tuned, int *sol
     const int t = tuning_info(c, species, solver, warps_per_block);
     if (tuned) *tuned = t;
     if (variant_ms)
-        for (int v = 0; v < 4; v++) variant_ms[v] = c.tune[species].ms[v];
+        for (int v = 0; v < 5; v++) variant_ms[v] = c.tune[species].ms[v];
     return 0;
 }
 

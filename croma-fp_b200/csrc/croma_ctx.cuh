@@ -82,7 +82,7 @@ struct TuneState {
     int tuned = 0;
     int variant = 0;
     int tracers = 0, steps = 0;
-    double ms[4] = {-1.0, -1.0, -1.0, -1.0};
+    double ms[5] = {-1.0, -1.0, -1.0, -1.0, -1.0};
 };
 
 struct Context {
@@ -227,7 +227,8 @@ int fused_reserve(Context &ctx, int cap);
 double fused_workspace_bytes(const ModelParams &mp, int cap, double workspace_cap, int path);
 int run_fused(Context &ctx, const SnapArgs &a);
 // the autotuner's choice for a species: solver (0 scan, 1 FP32-refined scan,
-// 2 PCR) and warps per block; returns 1 once tuned
+// 2 PCR, 3 scan with its constants in shared memory) and warps per block;
+// returns 1 once tuned
 int tuning_info(const Context &ctx, int species, int *solver, int *wpb);
 // dsa.cu
 int set_dsa(Context &ctx, const CromaB200DsaParams *prm);

@@ -703,6 +703,67 @@ __device__ __forceinline__ void substep(const Coef<SRC> &F, double N[kR])
     }
 }
 
+// The steps kernel's registers bound its occupancy: warps are spread over
+// the SM's four sub-partitions, each with a quarter of the register file, so
+// at 512 bins (16 rows a lane) 8 warps per SM allow 255 registers a thread
+// and 12 allow 168, at 256 bins 16 allow 128 and 20 allow 102.  The
+// kSolveScanShared variant keeps the per-segment constants that a sub-step
+// only reads -- dt src / d of each row and the ten scan multipliers -- in the
+// warp's slice of shared memory ([r][lane] and [level][lane], one
+// conflict-free 8-byte read each per sub-step) instead of registers, for the
+// larger warp count.
+constexpr int kCoefSmemDoubles = NB + 10 * 32;   // per warp: dt src / d, hk, qk
+
+// substep() with dt src / d read from sm[r * 32] (SRC) and the scan
+// multipliers from sm[NB + lv * 32] (hk) and sm[NB + (5 + lv) * 32] (qk),
+// sm already offset to the lane.
+template <bool SRC>
+__device__ __forceinline__ void substep_sm(const Coef<SRC> &F, const double *sm, double N[kR])
+{
+    constexpr int H2 = kR / 2;
+    const double *hk = sm + NB, *qk = sm + NB + 5 * 32;
+    double alo = 0.0, ahi = 0.0;
+#pragma unroll
+    for (int r = 0; r < H2; r++) {
+        N[r] = SRC ? fma(N[r], F.inv[r], sm[r * 32]) : N[r] * F.inv[r];
+        N[r + H2] = SRC ? fma(N[r + H2], F.inv[r + H2], sm[(r + H2) * 32]) : N[r + H2] * F.inv[r + H2];
+        alo = fma(F.h[r], alo, N[r]);
+        ahi = fma(F.h[r + H2], ahi, N[r + H2]);
+    }
+    double acc = fma(F.hhi, alo, ahi);
+#pragma unroll
+    for (int lv = 0; lv < 5; lv++) acc = fma(hk[lv * 32], sup(acc, 1 << lv), acc);
+    const double cin = sup(acc, 1);
+    double plo = cin, phi = fma(F.hlo, cin, alo);
+#pragma unroll
+    for (int r = 0; r < H2; r++) {
+        plo = fma(F.h[r], plo, N[r]);
+        phi = fma(F.h[r + H2], phi, N[r + H2]);
+        N[r] = plo;
+        N[r + H2] = phi;
+    }
+    alo = 0.0;
+    ahi = 0.0;
+#pragma unroll
+    for (int r = H2 - 1; r >= 0; r--) {
+        alo = fma(F.q[r], alo, N[r]);
+        ahi = fma(F.q[r + H2], ahi, N[r + H2]);
+    }
+    acc = fma(F.qlo, ahi, alo);
+#pragma unroll
+    for (int lv = 0; lv < 5; lv++) acc = fma(qk[lv * 32], sdn(acc, 1 << lv), acc);
+    const double cout = sdn(acc, 1);
+    phi = cout;
+    plo = fma(F.qhi, cout, ahi);
+#pragma unroll
+    for (int r = H2 - 1; r >= 0; r--) {
+        phi = fma(F.q[r + H2], phi, N[r + H2]);
+        plo = fma(F.q[r], plo, N[r]);
+        N[r + H2] = phi;
+        N[r] = plo;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // FP32-refined sub-step (the "precision" form of the chosen path): the solve
 // of each sub-step in FP32 followed by one iterative-refinement sweep whose
@@ -943,16 +1004,21 @@ __device__ __forceinline__ void substep_pcr(const Coef<SRC> &F, const double cc[
     for (int r = 0; r < kR; r++) N[r] = N[r] / b[r];
 }
 
-// Sub-step solvers of the steps kernel: the FP64 warp-scan Thomas, the same
-// with FP32 solves refined by an FP64 residual, and warp PCR.
-enum { kSolveScan = 0, kSolveRefined = 1, kSolvePcr = 2 };
+// Sub-step solvers of the steps kernel: the FP64 warp-scan Thomas (its
+// per-segment constants in registers, or in shared memory to leave registers
+// for more warps), the same with FP32 solves refined by an FP64 residual, and
+// warp PCR.
+enum { kSolveScan = 0, kSolveRefined = 1, kSolvePcr = 2, kSolveScanShared = 3 };
 
 // Steps kernel: warp w of block b runs every segment [g0, g1) of tracer
 // t0 + b * WPB + w for species S with sub-step solver SOLVER.
 template <int S, bool SRC, int SOLVER, int WPB>
-__global__ void __launch_bounds__(WPB * 32, (NB <= 256 ? 16 : 8) / WPB) steps_kernel(FusedParams P)
+__global__ void __launch_bounds__(WPB * 32,
+                                  (SOLVER == kSolveScanShared ? (NB <= 256 ? 20 : 12) : (NB <= 256 ? 16 : 8)) / WPB)
+    steps_kernel(FusedParams P)
 {
     extern __shared__ double4 steps_smem[];
+    constexpr bool kSm = SOLVER == kSolveScanShared;
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int tl = blockIdx.x * WPB + w;
@@ -973,6 +1039,7 @@ __global__ void __launch_bounds__(WPB * 32, (NB <= 256 ? 16 : 8) / WPB) steps_ke
     Coef32 G;
     double cc[SOLVER == kSolvePcr ? kR : 1];
     PcrSmem *pcr_sm = reinterpret_cast<PcrSmem *>(steps_smem) + w;
+    double *coef_sm = reinterpret_cast<double *>(steps_smem) + (size_t)w * kCoefSmemDoubles + lane;
     double scale = 1.0;
     int budget = P.cal_steps > 0 ? P.cal_steps : 0x7fffffff;
     const int nslot = P.g1 - P.g0;
@@ -1027,6 +1094,19 @@ __global__ void __launch_bounds__(WPB * 32, (NB <= 256 ? 16 : 8) / WPB) steps_ke
                 load_coef<SRC>(F, fac_ptr(P, S, gi, want, tl), src, g.dt, lane);
                 if (SOLVER == kSolveRefined) make_coef32<SRC>(F, G, lane);
                 if (SOLVER == kSolvePcr) pcr_rows_from_factored<SRC>(F, cc, lane);
+                if (kSm) {
+                    __syncwarp();   // the previous run's reads of the slice are done
+                    if (SRC) {
+#pragma unroll
+                        for (int r = 0; r < kR; r++) coef_sm[r * 32] = F.sd[r];
+                    }
+#pragma unroll
+                    for (int lv = 0; lv < 5; lv++) {
+                        coef_sm[NB + lv * 32] = F.hk[lv];
+                        coef_sm[NB + (5 + lv) * 32] = F.qk[lv];
+                    }
+                    __syncwarp();
+                }
                 cur = want;
             }
             if (SOLVER == kSolveRefined) {
@@ -1036,6 +1116,9 @@ __global__ void __launch_bounds__(WPB * 32, (NB <= 256 ? 16 : 8) / WPB) steps_ke
             } else if (SOLVER == kSolvePcr) {
 #pragma unroll 1
                 for (int istep = 0; istep < run_n; istep++) substep_pcr<SRC>(F, cc, N, *pcr_sm, lane);
+            } else if (kSm) {
+#pragma unroll 2
+                for (int istep = 0; istep < run_n; istep++) substep_sm<SRC>(F, coef_sm, N);
             } else {
                 // two sub-steps per trip: the carried spectrum keeps its
                 // registers across the loop (fewer copies per sub-step)
@@ -1363,7 +1446,8 @@ cudaError_t launch_steps_variant(cudaStream_t st, const FusedParams &P, int trac
 {
     const int n = tracers > 0 ? min(tracers, P.nt) : P.nt;
     const int blocks = (n + WPB - 1) / WPB;
-    const size_t smem = SOLVER == kSolvePcr ? WPB * sizeof(PcrSmem) : 0;
+    const size_t smem = SOLVER == kSolvePcr ? WPB * sizeof(PcrSmem)
+                      : (SOLVER == kSolveScanShared ? (size_t)WPB * kCoefSmemDoubles * sizeof(double) : 0);
     if (smem > 48 * 1024) {
         static const cudaError_t attr = cudaFuncSetAttribute(steps_kernel<S, SRC, SOLVER, WPB>,
                                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1374,17 +1458,19 @@ cudaError_t launch_steps_variant(cudaStream_t st, const FusedParams &P, int trac
 }
 
 // Variants the autotuner chooses between: (solver, warps per block).
-constexpr int kStepVariants = 4;
-constexpr int kVariantSolver[kStepVariants] = {kSolveScan, kSolveScan, kSolveScan, kSolvePcr};
-constexpr int kVariantWpb[kStepVariants] = {1, 2, 4, 1};
+constexpr int kStepVariants = 5;
+constexpr int kVariantSolver[kStepVariants] = {kSolveScan, kSolveScan, kSolveScanShared, kSolveScanShared,
+                                               kSolvePcr};
+constexpr int kVariantWpb[kStepVariants] = {1, 2, 1, 2, 1};
 
 template <int S, bool SRC>
 cudaError_t launch_variant(cudaStream_t st, const FusedParams &P, int v, int tracers)
 {
     switch (v) {
     case 1: return launch_steps_variant<S, SRC, kSolveScan, 2>(st, P, tracers);
-    case 2: return launch_steps_variant<S, SRC, kSolveScan, 4>(st, P, tracers);
-    case 3: return launch_steps_variant<S, SRC, kSolvePcr, 1>(st, P, tracers);
+    case 2: return launch_steps_variant<S, SRC, kSolveScanShared, 1>(st, P, tracers);
+    case 3: return launch_steps_variant<S, SRC, kSolveScanShared, 2>(st, P, tracers);
+    case 4: return launch_steps_variant<S, SRC, kSolvePcr, 1>(st, P, tracers);
     default: return launch_steps_variant<S, SRC, kSolveScan, 1>(st, P, tracers);
     }
 }
@@ -1405,7 +1491,8 @@ int tridiag_env()
 // variant runs the chunk's first tracers (at most 2,048) for their first 16
 // sub-steps on a copy of their spectra, timed with CUDA events; the fastest
 // is kept for the context's species.  Results are recorded in ctx.tune.
-// CROMA_B200_STEPS_VARIANT = 0..3 fixes the variant (scan x1, x2, x4, PCR)
+// CROMA_B200_STEPS_VARIANT = 0..4 fixes the variant (scan x1, scan x2, shared
+// scan x1, shared scan x2, PCR)
 // without calibrating, for reproducible profiles; unset or out of range: tune.
 int fixed_variant_env()
 {

@@ -356,15 +356,15 @@ class TracerFP:
         self._check(self.lib.croma_b200_step_host(self.h, C.byref(snap), C.byref(io)))
         del keep
 
-    SOLVERS = {0: "thomas-scan", 1: "thomas-scan-fp32-refined", 2: "pcr"}
+    SOLVERS = {0: "thomas-scan", 1: "thomas-scan-fp32-refined", 2: "pcr", 3: "thomas-scan-smem"}
 
     def tuning(self, species: int):
         """The steps-kernel autotuner's record for species 0 (protons) or 1
         (electrons): dict(tuned, solver, warps_per_block, variant_ms)."""
         t, so, w = _i(), _i(), _i()
-        ms = (_d * 4)()
+        ms = (_d * 5)()
         self._check(self.lib.croma_b200_get_tuning(self.h, species, C.byref(t), C.byref(so), C.byref(w), ms))
-        names = ("scan x1", "scan x2", "scan x4", "pcr x1")
+        names = ("scan x1", "scan x2", "smem scan x1", "smem scan x2", "pcr x1")
         return {"tuned": t.value, "solver": self.SOLVERS.get(so.value, so.value), "warps_per_block": w.value,
                 "variant_ms": {n: (m if m >= 0 else None) for n, m in zip(names, list(ms))}}
 

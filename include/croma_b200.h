@@ -318,17 +318,19 @@ int croma_b200_step_host(CromaB200Context *ctx, const CromaB200Snapshot *snap, c
 
 /* The steps-kernel autotuner (the on-chip FP64 path).  On the first
  * workspace chunk a context evolves, per species, each admissible variant --
- * the warp-scan Thomas at 1, 2 or 4 tracers (warps) per block, and warp PCR
- * (one warp per tracer, parallel cyclic reduction in shared memory) -- runs
- * the chunk's first tracers (up to 2,048) for 16 sub-steps on a copy of
- * their spectra, timed with CUDA events, and the fastest is kept for the
- * context.  CROMA_CUDA_TRIDIAG=thomas admits only the scan variants, =pcr
- * only PCR (src/fp_cuda_solver.cu:41-72 of the reference).  Reported here:
- * tuned (0 before the first snapshot), solver (0 scan, 1 FP32-refined scan,
- * 2 PCR), tracers per block, and the calibration time of each variant in
- * milliseconds (variant order: scan x1, scan x2, scan x4, PCR; -1 = not run).
- * CROMA_B200_STEPS_VARIANT=0..3 fixes the variant in that order without
- * calibrating (reproducible profiles). */
+ * the warp-scan Thomas with its per-segment constants in registers or in
+ * shared memory (fewer registers, more warps per SM), at 1 or 2 tracers
+ * (warps) per block, and warp PCR (one warp per tracer, parallel cyclic
+ * reduction in shared memory) -- runs the chunk's first tracers (up to 2,048)
+ * for 16 sub-steps on a copy of their spectra, timed with CUDA events, and
+ * the fastest is kept for the context.  CROMA_CUDA_TRIDIAG=thomas admits only
+ * the scan variants, =pcr only PCR (src/fp_cuda_solver.cu:41-72 of the
+ * reference).  Reported here: tuned (0 before the first snapshot), solver
+ * (0 scan, 1 FP32-refined scan, 2 PCR, 3 scan with shared-memory constants),
+ * tracers per block, and the calibration time of each variant in
+ * milliseconds, variant_ms[5] in the order scan x1, scan x2, shared scan x1,
+ * shared scan x2, PCR (-1 = not run).  CROMA_B200_STEPS_VARIANT=0..4 fixes
+ * the variant in that order without calibrating (reproducible profiles). */
 int croma_b200_get_tuning(CromaB200Context *ctx, int species, int *tuned, int *solver, int *warps_per_block,
                           double *variant_ms);
 

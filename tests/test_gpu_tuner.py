@@ -43,7 +43,8 @@ def test_tuner_chooses_and_records(name, monkeypatch):
         assert t["tuned"] == 1
         ms = t["variant_ms"]
         assert all(v is not None and v > 0 for v in ms.values()), ms
-        chosen = {("thomas-scan", 1): "scan x1", ("thomas-scan", 2): "scan x2", ("thomas-scan", 4): "scan x4",
+        chosen = {("thomas-scan", 1): "scan x1", ("thomas-scan", 2): "scan x2",
+                  ("thomas-scan-smem", 1): "smem scan x1", ("thomas-scan-smem", 2): "smem scan x2",
                   ("pcr", 1): "pcr x1"}[(t["solver"], t["warps_per_block"])]
         assert ms[chosen] == min(ms.values())
     print(name, tunes)
@@ -52,8 +53,15 @@ def test_tuner_chooses_and_records(name, monkeypatch):
 @pytest.mark.parametrize("env,solver", [("pcr", "pcr"), ("thomas", "thomas-scan")])
 def test_tridiag_env_restricts_the_tuner(env, solver, monkeypatch):
     for t in _run("c1_asa128", env, monkeypatch):
-        assert t["tuned"] == 1 and t["solver"] == solver
+        assert t["tuned"] == 1 and t["solver"].startswith(solver)
         if env == "pcr":
             assert t["variant_ms"]["scan x1"] is None
         else:
             assert t["variant_ms"]["pcr x1"] is None
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("name", ["c1_asa256", "c4_asa512"])
+def test_every_steps_variant_matches_reference(name, variant, monkeypatch):
+    monkeypatch.setenv("CROMA_B200_STEPS_VARIANT", str(variant))
+    _run(name, None, monkeypatch)
