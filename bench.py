@@ -795,11 +795,12 @@ def run_config1(args):
     from croma_fp_b200 import synth
     w = synth.Workload(cfg, nt, NSNAP_TIMELINE, seed=SEED)
     bg = torch.stack([torch.from_numpy(w.background(s)) for s in range(snaps[0], snaps[-1] + 2)]).cuda()
-    f = run_resident("fused", cfg, nt, w, bg, None, snaps, 3, 5, emission=False, dsa=False)
+    f = run_resident("fused", cfg, nt, w, bg, None, snaps, 3, 5, emission=False, dsa=False, kernel_timing=True)
     p = run_resident("plain", cfg, nt, w, bg, None, snaps, 1, 2, emission=False, dsa=False)
     vf, vp = nt * 5 / (f["ms"] / 1e3), nt * 2 / (p["ms"] / 1e3)
     return {"workload": "batching: 65,536 tracers, electron_proton, 256 bins, ASA, nsub <= 500 (no DSA, no "
                         "emission)", "fused": vf, "plain": vp, "chosen_over_plain": vf / vp,
+            "fused_kernel_ms_per_step": {k: f[k][0] / 5 for k in ("evolve", "coeff", "secondary")},
             "nsub": f["nsub"], "steps": {"fused": 5, "plain": 2}}
 
 

@@ -55,10 +55,14 @@ constexpr int kSw = kPitch * kR;     // swizzled row-array length
 constexpr int kWarps = 1;            // warps per block
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kFacDoubles = 3 * NB;  // 1/d, a/d, c/d of one system
-// warps per factor-kernel block: at nb <= 256 two 9-warp blocks (at most 113
-// registers a thread) fill an SM; at nb = 512 one 12-warp block (at most 170
-// registers, 160 KB of shared memory: the tables and each warp's B and C)
-constexpr int kFacWarps = (NB <= 256 ? 8 : 12);
+// Face weights of the factor kernel: at nb = 512 computed in registers where
+// the rows use them, so each warp's shared memory holds only B and C and one
+// 12-warp block (at most 168 registers, 160 KB of shared memory) fills an SM
+// instead of 9 warps; at nb <= 256, where registers and not shared memory
+// bound the warps, computed lane-strided into shared memory (two 9-warp
+// blocks per SM).
+constexpr bool kFacesInRegs = (NB >= 512);
+constexpr int kFacWarps = (NB <= 256 ? 9 : 12);
 
 // Grid tables of one species staged in shared memory by the factor kernel.
 // X0..X3: protons expE, cp_Ep, cp_inv2mpkin, cp_inv_betap2; electrons
@@ -279,6 +283,7 @@ __device__ __forceinline__ SegTerms<S> seg_terms_pre(const GridTables &gt, const
 
 struct WarpSmem {
     double B[kSw], C[kSw];
+    double Wp[kFacesInRegs ? 1 : kSw], Wm[kFacesInRegs ? 1 : kSw];
 };
 
 
@@ -308,10 +313,11 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
         sm.C[sb0 + k * kStep] = C;
     }
     __syncwarp();
-    // Faces j (between bins j and j+1), computed in registers where the rows
-    // use them: lane l's rows m = l R + r need faces m - 1 and m, so the lane
-    // evaluates faces l R - 1 .. l R + R - 1 (the first one its left
-    // neighbour evaluates too).  The drift / diffusion ratio
+    // Faces j (between bins j and j+1).  In registers (kFacesInRegs) where the
+    // rows use them: lane l's rows m = l R + r need faces m - 1 and m, so the
+    // lane evaluates faces l R - 1 .. l R + R - 1 (the first one its left
+    // neighbour evaluates too); else lane-strided into shared memory.  The
+    // drift / diffusion ratio
     // (B_j + B_j+1) / (C_j + C_j+1) * dx: with the filled Dpp form the C sum
     // is kappa times a grid factor, so the division becomes a product with the
     // tabulated dx / (g_j + g_j+1) and 1 / kappa (equal to a few ulp).  The
@@ -335,10 +341,34 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
         if (live) face_weights_fast(w, wp, wm);
     };
 
+    if (!kFacesInRegs) {
+        // faces lane-strided into shared memory (j = 32 k + lane); face nb - 1
+        // does not exist: its position swz(nb) is a padding word, never read
+#pragma unroll 2
+        for (int k = 0; k < kR; k++) {
+            const int j = k * 32 + lane;
+            const int s0 = sb0 + k * kStep, s1 = sb1 + k * kStep;
+            double wp = 0.0, wm = 0.0;
+            const double cl = sm.C[s0];
+            const bool live = (j <= NB - 2) && fabs(cl) > 1.0e-200;
+            const double bsum = sm.B[s0] + sm.B[s1];
+            const double rf = tab[TB_RF * kTabStride + j] * inv_kappa;
+            const bool divide = live && !(T.dpp_fill && isfinite(rf));
+            double w = bsum * rf;
+            if (__any_sync(kFull, divide)) {
+                if (divide) w = bsum / (cl + sm.C[s1]) * tab[TB_DXF * kTabStride + j];
+            }
+            if (live) face_weights_fast(w, wp, wm);
+            sm.Wp[kFacesInRegs ? 0 : s0] = wp;
+            sm.Wm[kFacesInRegs ? 0 : s0] = wm;
+        }
+        __syncwarp();
+    }
+
     // rows a, b, c of this lane (cc_build_{left,interior,right}, Chang_Cooper.c:66-184)
     const int row0 = lane * kR;
-    double wpm, wmm;   // face m - 1
-    face(row0 - 1, lane > 0 ? (kR - 1) * kPitch + lane - 1 : 0, lane, wpm, wmm);
+    double wpm = 0.0, wmm = 0.0;   // face m - 1
+    if (kFacesInRegs) face(row0 - 1, lane > 0 ? (kR - 1) * kPitch + lane - 1 : 0, lane, wpm, wmm);
 #pragma unroll
     for (int r = 0; r < kR; r++) {
         const int m = row0 + r;
@@ -346,7 +376,16 @@ __device__ unsigned build_rows(const SegTerms<S> &T, const double *tab, int lane
         const int sm_p = r > 0 ? (r - 1) * kPitch + lane : (kR - 1) * kPitch + lane - 1;   // swz(m - 1), m >= 1
         const int sm_n = r < kR - 1 ? (r + 1) * kPitch + lane : lane + 1;                  // swz(m + 1)
         double wpc, wmc;   // face m
-        face(m, sm_m, sm_n, wpc, wmc);
+        if (kFacesInRegs) {
+            face(m, sm_m, sm_n, wpc, wmc);
+        } else {
+            wpc = sm.Wp[kFacesInRegs ? 0 : sm_m];
+            wmc = sm.Wm[kFacesInRegs ? 0 : sm_m];
+            if (m > 0) {
+                wpm = sm.Wp[kFacesInRegs ? 0 : sm_p];
+                wmm = sm.Wm[kFacesInRegs ? 0 : sm_p];
+            }
+        }
         const double k = T.dt * tab[TB_IDX * kTabStride + r * kPitch + lane];
         const double Cm = sm.C[r * kPitch + lane], Bm = sm.B[r * kPitch + lane], Dm = T.row_dT(tab, r, lane);
         double av = 0.0, bv, cv = 0.0;
@@ -508,8 +547,8 @@ __global__ void __launch_bounds__(kFacWarps * 32, (NB <= 256 ? 2 : 1)) factor_ke
         tab[TB_P2 * kTabStride + i] = st.p2[i];
         tab[TB_CUT * kTabStride + i] = st.exp_cut[i];
         tab[TB_2P * kTabStride + i] = st.two_over_p[i];
-        tab[TB_DXF * kTabStride + swz(i)] = st.dxf[i];
-        tab[TB_RF * kTabStride + swz(i)] = st.face_rf[i];
+        tab[TB_DXF * kTabStride + (kFacesInRegs ? swz(i) : i)] = st.dxf[i];
+        tab[TB_RF * kTabStride + (kFacesInRegs ? swz(i) : i)] = st.face_rf[i];
         if (S == 0) {
             tab[TB_X0 * kTabStride + i] = st.expE[i];
             tab[TB_X1 * kTabStride + i] = P.gt.cp_Ep[i];
