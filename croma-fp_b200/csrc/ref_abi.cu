@@ -698,6 +698,10 @@ int run_tracer_pipeline(const FpCudaPipelineInput *in, const FpCudaOutputSchedul
         times->solve_ms = elapsed(e1, e2);
         times->d2h_ms = elapsed(e2, e3);
         times->total_ms = elapsed(e0, e3);
+        // which sub-step solver the steps-kernel autotuner runs for each species
+        int solver = 0;
+        if (tuning_info(c, 0, &solver, nullptr)) times->used_pcr_proton = solver == 2;
+        if (tuning_info(c, 1, &solver, nullptr)) times->used_pcr_electron = solver == 2;
     }
     cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
     if (err) {

@@ -172,3 +172,31 @@ def test_resident_emission_device_pointers_equal_host_call():
             assert np.array_equal(t.cpu().numpy(), host[k]), k
     finally:
         fp.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ntr", [1, 3, 9])
+def test_resident_emission_ragged_tracer_counts(ntr):
+    """Tracer counts below and across the synchrotron kernel's block of 8
+    sorted tracers (1, 3, 9), and a setup with only some kinds: each tracer's
+    emissivities equal the same tracer's from the 12-tracer run."""
+    full, bg = _resident_context()
+    try:
+        ref = full.emission_run(bg, PRM["z_ic"])
+    finally:
+        full.close()
+    cfg = config.config1(nb=PRM["nb"])
+    fp = native.TracerFP(cfg, path="fused")
+    try:
+        idx = np.arange(ntr) * 5 % FIX["crp"].shape[0]
+        fp.set_state(FIX["crp"][idx], FIX["cre"][idx])
+        fp.emission_setup(nfreq=PRM["nfreq"], nu_min_s=PRM["nu_s"][0], nu_max_s=PRM["nu_s"][1],
+                          ntheta_pitch=PRM["ntheta"], nlogb=PRM["nlogb"], logb_min=PRM["logb"][0],
+                          logb_max=PRM["logb"][1], nbins_gamma=PRM["nbins"], egamma_min=PRM["egamma"][0],
+                          egamma_max=PRM["egamma"][1])
+        eps = fp.emission_run(np.ascontiguousarray(bg[:, idx]), PRM["z_ic"], kinds=("syn", "gamma"))
+    finally:
+        fp.close()
+    assert set(eps) == {"syn", "gamma"}
+    for k in eps:
+        assert rel_to_max(eps[k], ref[k][idx]) <= 1e-13, k

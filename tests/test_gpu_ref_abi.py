@@ -344,3 +344,37 @@ def test_c_caller_compiled_against_reference_header():
     g_crp, g_cre = out[:nt * 128].reshape(nt, 128), out[nt * 128:].reshape(nt, 128)
     assert rel_err(g_crp, o_crp) <= RTOL
     assert rel_err(g_cre, o_cre) <= RTOL
+
+
+def test_run_tracer_pipeline_with_pcr_requested(monkeypatch):
+    """CROMA_CUDA_TRIDIAG=pcr in the pipeline: the steps kernel runs warp PCR,
+    FpCudaPipelineTimes reports it for both species, and the spectra still
+    match the oracle's segment within 1e-10."""
+    monkeypatch.setenv("CROMA_CUDA_TRIDIAG", "pcr")
+    cfg, o, abi, w, gp, ge, crp, cre, qpi, qepri, dis = _setup(nt=24, seed=41)
+    nt = crp.shape[0]
+    bg = w.background(11)
+    row, m1, p1 = o.ic_row(0.45)
+    ric = np.ascontiguousarray(np.repeat(row[:, None], nt, axis=1))
+    m1s, p1s = np.full(nt, m1), np.full(nt, p1)
+    nstep, dt = 6, 2.5e-4
+    o_crp, o_cre = crp.copy(), cre.copy()
+    o.evolve_segment(nstep, dt, False, 0, nstep, bg, ric, m1s, p1s, qpi, qepri, o_crp, o_cre, mass=w.mass, dis=dis)
+    cgp, cge = abi.grid(*gp), abi.grid(*ge)
+    ws = abi.lib.cuda_pipeline_workspace_create()
+    assert ws
+    try:
+        ci, keep = _coeff(bg, ric, m1s, p1s, w.mass, dis)
+        pin = _pipeline_input(abi, cgp, cge, ci, nstep, dt, False, 0, nstep, ws)
+        pin.crp_init, pin.cre_init = ref_abi.dptr(crp), ref_abi.dptr(cre)
+        pin.qpi_batch, pin.qepri_batch = ref_abi.dptr(qpi), ref_abi.dptr(qepri)
+        g_crp, g_cre = np.empty_like(crp), np.empty_like(cre)
+        times = ref_abi.FpCudaPipelineTimes()
+        rc = abi.lib.run_tracer_pipeline(C.byref(pin), None, ref_abi.dptr(g_crp), ref_abi.dptr(g_cre),
+                                         None, None, None, C.byref(times))
+        assert rc == 0, abi.error()
+        assert times.used_pcr_proton == 1 and times.used_pcr_electron == 1
+        assert rel_err(g_crp, o_crp) <= RTOL
+        assert rel_err(g_cre, o_cre) <= RTOL
+    finally:
+        abi.lib.cuda_pipeline_workspace_destroy(ws)

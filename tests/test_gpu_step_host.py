@@ -61,3 +61,35 @@ def test_step_host_equals_its_parts(path):
     finally:
         a.close()
         b.close()
+
+
+def test_step_host_spectra_only_and_no_shocks():
+    """Outputs may be partial: no emission set up, no shock fields (no
+    injection), only the electron spectra requested; the step equals
+    snapshot + get_state on a second context."""
+    cfg = config.config1(nb=128)
+    nt, seed = 33, 616
+    w = synth.Workload(cfg, nt, 100, seed=seed)
+    ctx = []
+    for _ in range(2):
+        fp = native.TracerFP(cfg, path="fused")
+        gp, ge = fp.grid(0), fp.grid(1)
+        crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), nt, cfg.species)
+        fp.set_state(crp, cre, mass=w.mass)
+        ctx.append(fp)
+    a, b = ctx
+    try:
+        for isnap in (40, 41):
+            args = w.snapshot_args(isnap)
+            out = {"cre": np.empty((nt, 128))}
+            a.step_host(*args, outputs=out)
+            b.snapshot(*args, sync=True)
+            g_crp, g_cre = b.get_state()
+            assert np.array_equal(out["cre"], g_cre)
+        a_crp, a_cre = a.get_state()
+        assert np.array_equal(a_crp, g_crp)
+        with pytest.raises(native.CromaError):
+            a.step_host(*args, outputs={"syn": np.empty((nt, 8))})   # emission never set up
+    finally:
+        a.close()
+        b.close()
