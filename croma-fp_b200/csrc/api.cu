@@ -811,6 +811,12 @@ __global__ void fp64_fma_probe(int iters, double seed, double *out)
     for (int k = 0; k < 8; k++) s += x[k];
     if (s == 12345.678) out[blockIdx.x] = s;
 }
+// rcp_nr (the factor and per-step kernels' reciprocal) element-wise.
+__global__ void rcp_probe(long long n, const double *x, double *out)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = croma::rcp_nr(x[i]);
+}
 }  // namespace croma_probe
 
 extern "C" {
@@ -823,7 +829,7 @@ int croma_b200_get_tuning(CromaB200Context *h, int species, int *tuned, int *sol
     const int t = tuning_info(c, species, solver, warps_per_block);
     if (tuned) *tuned = t;
     if (variant_ms)
-        for (int v = 0; v < 5; v++) variant_ms[v] = c.tune[species].ms[v];
+        for (int v = 0; v < CROMA_B200_STEPS_VARIANTS; v++) variant_ms[v] = c.tune[species].ms[v];
     return 0;
 }
 
@@ -838,6 +844,24 @@ int croma_b200_host_alloc(size_t bytes, void **out)
 int croma_b200_host_free(void *p)
 {
     if (p) CROMA_CUDA(cudaFreeHost(p));
+    return 0;
+}
+
+int croma_b200_rcp_check(long long n, const double *x, double *out)
+{
+    if (n < 0 || (n > 0 && (!x || !out))) { set_error("invalid rcp_check arguments"); return -1; }
+    if (n == 0) return 0;
+    double *d = nullptr;
+    CROMA_CUDA(cudaMalloc(&d, 2 * (size_t)n * sizeof(double)));
+    cudaError_t e = cudaMemcpy(d, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        const long long blocks = (n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096;
+        croma_probe::rcp_probe<<<(unsigned)blocks, 256>>>(n, d, d + n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + n, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "rcp_check");
     return 0;
 }
 

@@ -82,7 +82,7 @@ struct TuneState {
     int tuned = 0;
     int variant = 0;
     int tracers = 0, steps = 0;
-    double ms[5] = {-1.0, -1.0, -1.0, -1.0, -1.0};
+    double ms[CROMA_B200_STEPS_VARIANTS] = {-1.0, -1.0, -1.0, -1.0, -1.0, -1.0, -1.0, -1.0, -1.0};
 };
 
 struct Context {

@@ -210,11 +210,36 @@ CROMA_HD void face_weights(double w, double &wp, double &wm)
     }
 }
 
+// FP64 reciprocal for the factor and per-step kernels.  CUDA's IEEE division
+// is a called routine: on B200 one costs ~125-145 cycles of a warp's time and
+// two of them never overlap (measured: the same per-division time at 1, 4 or
+// 8 independent divisions per thread), so a chain of pivots or a row of
+// faces serialises on it.  This form is inline: the hardware approximation
+// (PTX rcp.approx.ftz.f64) and two Newton-Raphson steps for 1/x in FMA form,
+// e = 1 - x y, y <- y + y e (each step squares the relative error), which
+// reach the FP64 rounding level for normal x (tested against the exact
+// reciprocal in ulps).  Subnormal x is flushed (then 0 gives a NaN) and
+// 1/x below the normal range returns 0; the callers' operands are O(1)
+// denominators bounded away from both.  Host builds divide.
+CROMA_HD double rcp_nr(double x)
+{
+#ifdef __CUDA_ARCH__
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+#else
+    return 1.0 / x;
+#endif
+}
+
 // The same weights with one exponential and one division per face and no
 // divergent branch (the evolve kernels' form): exp(-w/2) is taken as
-// 1/exp(w/2), the two quotients by the denominator share one division and
-// the series constants are multiplied in.  Agrees with face_weights to a few
-// ulp.
+// 1/exp(w/2), the two quotients by the denominator share one reciprocal
+// (rcp_nr) and the series constants are multiplied in.  Agrees with
+// face_weights to a few ulp.
 CROMA_HD void face_weights_fast(double w, double &wp, double &wm)
 {
     const double aw = fabs(w);
@@ -222,7 +247,7 @@ CROMA_HD void face_weights_fast(double w, double &wp, double &wm)
     const double w2 = w * w;
     const double dser = 1.0 + w2 * (1.0 / 24.0) + (w2 * w2) * (1.0 / 1920.0);
     const double e = exp(series ? 0.5 * w : -aw);
-    const double q = (series ? 1.0 : aw) / (series ? e * dser : 1.0 - e);
+    const double q = (series ? 1.0 : aw) * rcp_nr(series ? e * dser : 1.0 - e);
     const double s = q * e;
     // series: wm = 1 / (e dser), wp = e / dser; otherwise big = q, small = q e
     wp = series ? s * e : ((w >= 0.0) ? q : s);

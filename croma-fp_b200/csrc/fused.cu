@@ -37,6 +37,7 @@
 // Spectra are cell-major [tracer][nb] so that a warp's rows are contiguous.
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 
 #include "croma_segment.cuh"
 
@@ -136,6 +137,33 @@ __device__ __forceinline__ int swz(int m) { return (m % kR) * kPitch + m / kR; }
 __device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 __device__ __forceinline__ double sup(double v, int d) { return __shfl_up_sync(kFull, v, d); }
 __device__ __forceinline__ double sdn(double v, int d) { return __shfl_down_sync(kFull, v, d); }
+// 32-byte accesses of four consecutive doubles (sm_100 256-bit vector
+// loads and stores).  The lanes of a warp own 128-byte row blocks, so a
+// 16-byte access per lane would touch 32 sectors and use half of each (a
+// scalar access a quarter); 32 bytes per lane use every sector fully.  The
+// asm is volatile so that the per-step path's re-reads stay in its loop.
+// ld4_cg: L2 only (rows and sources); ld4 / st4: the default caching.
+__device__ __forceinline__ void ld4_cg(const double *p, double *v)
+{
+    asm volatile("ld.global.cg.v4.f64 {%0,%1,%2,%3}, [%4];"
+                 : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
+}
+__device__ __forceinline__ void ld4(const double *p, double *v)
+{
+    asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
+                 : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p) : "memory");
+}
+__device__ __forceinline__ void st4(double *p, const double *v)
+{
+    asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]), "d"(v[2]), "d"(v[3])
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    const int n = valid ? 16 : 0;   // 0 source bytes: the 16 destination bytes are zero-filled
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
 
 // Exact power-of-two rescaling of a 2x2 matrix (projective maps are
 // unchanged by a common factor).
@@ -479,13 +507,13 @@ __device__ __forceinline__ unsigned pivot_rows(double A[kR], double Bd[kR], doub
         }
     }
     double vp = sup(t00, 1), vq = sup(t10, 1);
-    double cp_prev = (lane == 0) ? 0.0 : -c_in * vq / vp;
+    double cp_prev = (lane == 0) ? 0.0 : -c_in * vq * rcp_nr(vp);
 #pragma unroll
     for (int r = 0; r < kR; r++) {
         const int m = row0 + r;
         const double den = Bd[r] + A[r] * cp_prev;
         if (fabs(den) <= 1.0e-300) err |= kErrSingular;
-        const double inv = 1.0 / den;
+        const double inv = rcp_nr(den);
         const double cr = Cc[r];
         Bd[r] = inv;
         A[r] = A[r] * inv;
@@ -634,15 +662,15 @@ __device__ __forceinline__ void load_rows(const double *in, int lane, double X[k
 {
     const int row0 = lane * kR;
 #pragma unroll
-    for (int r = 0; r < kR; r += 2) {
-        const double2 vx = __ldcg(reinterpret_cast<const double2 *>(in + row0 + r));
-        const double2 vy = __ldcg(reinterpret_cast<const double2 *>(in + NB + row0 + r));
-        const double2 vz = __ldcg(reinterpret_cast<const double2 *>(in + 2 * NB + row0 + r));
-        X[r] = vx.x; X[r + 1] = vx.y;
-        Y[r] = vy.x; Y[r + 1] = vy.y;
-        Z[r] = vz.x; Z[r + 1] = vz.y;
+    for (int r = 0; r < kR; r += 4) {
+        ld4_cg(in + row0 + r, X + r);
+        ld4_cg(in + NB + row0 + r, Y + r);
+        ld4_cg(in + 2 * NB + row0 + r, Z + r);
     }
 }
+
+template <bool SRC>
+__device__ __forceinline__ void scan_multipliers(Coef<SRC> &F, int lane);
 
 // The rest of Coef once inv, h, q hold the lane's factored rows: the source
 // term and the scan multipliers.
@@ -654,8 +682,21 @@ __device__ __forceinline__ void finish_coef(Coef<SRC> &F, const double *src, dou
     if (lane == 31) F.q[kR - 1] = 0.0;
     if (SRC) {
 #pragma unroll
-        for (int r = 0; r < kR; r++) F.sd[r] = (dt * src[row0 + r]) * F.inv[r];
+        for (int r = 0; r < kR; r += 4) {
+            double v[4];
+            ld4_cg(src + row0 + r, v);
+#pragma unroll
+            for (int i = 0; i < 4; i++) F.sd[r + i] = (dt * v[i]) * F.inv[r + i];
+        }
     }
+    scan_multipliers<SRC>(F, lane);
+}
+
+// The half-chain products (hlo, hhi, qlo, qhi) and the warp-scan
+// multipliers (hk, qk) of the lane's h and q rows.
+template <bool SRC>
+__device__ __forceinline__ void scan_multipliers(Coef<SRC> &F, int lane)
+{
     double hlo = 1.0, hhi = 1.0, qlo = 1.0, qhi = 1.0;
 #pragma unroll
     for (int r = 0; r < kR / 2; r++) {
@@ -750,22 +791,38 @@ __device__ __forceinline__ void substep(const Coef<SRC> &F, double N[kR])
 // only reads -- dt src / d of each row and the ten scan multipliers -- in the
 // warp's slice of shared memory ([r][lane] and [level][lane], one
 // conflict-free 8-byte read each per sub-step) instead of registers, for the
-// larger warp count.
-constexpr int kCoefSmemDoubles = NB + 10 * 32;   // per warp: dt src / d, hk, qk
+// larger warp count.  The kSolveScanRhs variant also moves 1 / d of each
+// row there, as (1 / d, dt src / d) pairs ([r][lane], one conflict-free
+// 16-byte read per row and sub-step): the lane then holds only N, h and q
+// (about 100 registers at 512 bins), for 16 warps per SM at 512 bins and 24
+// at 256.
+constexpr int kCoefSmemDoubles = NB + 10 * 32;       // per warp: dt src / d, hk, qk
+constexpr int kRhsSmemDoubles = 2 * NB + 10 * 32;    // per warp: (1 / d, dt src / d), hk, qk
 
-// substep() with dt src / d read from sm[r * 32] (SRC) and the scan
-// multipliers from sm[NB + lv * 32] (hk) and sm[NB + (5 + lv) * 32] (qk),
-// sm already offset to the lane.
-template <bool SRC>
-__device__ __forceinline__ void substep_sm(const Coef<SRC> &F, const double *sm, double N[kR])
+// substep() with the per-segment constants of the warp's shared-memory slice
+// wsm.  RHS false (kSolveScanShared): dt src / d at wsm[r * 32 + lane] (SRC),
+// the scan multipliers at wsm[NB + lv * 32 + lane] (hk) and
+// wsm[NB + (5 + lv) * 32 + lane] (qk).  RHS true (kSolveScanRhs): the pair
+// (1 / d, dt src / d) of row r at double2 index r * 32 + lane, hk and qk
+// after the 2 NB doubles of pairs.  Same arithmetic as substep().
+template <bool SRC, bool RHS>
+__device__ __forceinline__ void substep_sm(const Coef<SRC> &F, const double *wsm, int lane, double N[kR])
 {
     constexpr int H2 = kR / 2;
-    const double *hk = sm + NB, *qk = sm + NB + 5 * 32;
+    const double *sm = wsm + lane;
+    const double2 *rhs = reinterpret_cast<const double2 *>(wsm) + lane;
+    const double *hk = sm + (RHS ? 2 * NB : NB), *qk = hk + 5 * 32;
     double alo = 0.0, ahi = 0.0;
 #pragma unroll
     for (int r = 0; r < H2; r++) {
-        N[r] = SRC ? fma(N[r], F.inv[r], sm[r * 32]) : N[r] * F.inv[r];
-        N[r + H2] = SRC ? fma(N[r + H2], F.inv[r + H2], sm[(r + H2) * 32]) : N[r + H2] * F.inv[r + H2];
+        if (RHS) {
+            const double2 u = rhs[r * 32], v = rhs[(r + H2) * 32];
+            N[r] = SRC ? fma(N[r], u.x, u.y) : N[r] * u.x;
+            N[r + H2] = SRC ? fma(N[r + H2], v.x, v.y) : N[r + H2] * v.x;
+        } else {
+            N[r] = SRC ? fma(N[r], F.inv[r], sm[r * 32]) : N[r] * F.inv[r];
+            N[r + H2] = SRC ? fma(N[r + H2], F.inv[r + H2], sm[(r + H2) * 32]) : N[r + H2] * F.inv[r + H2];
+        }
         alo = fma(F.h[r], alo, N[r]);
         ahi = fma(F.h[r + H2], ahi, N[r + H2]);
     }
@@ -794,6 +851,201 @@ __device__ __forceinline__ void substep_sm(const Coef<SRC> &F, const double *sm,
     const double cout = sdn(acc, 1);
     phi = cout;
     plo = fma(F.qhi, cout, ahi);
+#pragma unroll
+    for (int r = H2 - 1; r >= 0; r--) {
+        phi = fma(F.q[r + H2], phi, N[r + H2]);
+        plo = fma(F.q[r], plo, N[r]);
+        N[r + H2] = phi;
+        N[r] = plo;
+    }
+}
+
+// kSolveScanRhs's coefficient load: the (1 / d, dt src / d) pairs of the
+// lane's rows go from the factored rows (and the source) straight to the
+// warp's slice, h and q into registers, and the scan multipliers, formed as
+// load_coef forms them, into the slice after the pairs.
+template <bool SRC>
+__device__ __forceinline__ void load_coef_rhs(Coef<SRC> &F, const double *fac, const double *src, double dt,
+                                              int lane, double *wsm)
+{
+    const int row0 = lane * kR;
+    double2 *rhs = reinterpret_cast<double2 *>(wsm) + lane;
+    __syncwarp();   // the previous run's reads of the slice are done
+#pragma unroll
+    for (int r = 0; r < kR; r += 2) {
+        const double2 vi = __ldcg(reinterpret_cast<const double2 *>(fac + row0 + r));
+        const double s0 = SRC ? (dt * src[row0 + r]) * vi.x : 0.0;
+        const double s1 = SRC ? (dt * src[row0 + r + 1]) * vi.y : 0.0;
+        rhs[r * 32] = make_double2(vi.x, s0);
+        rhs[(r + 1) * 32] = make_double2(vi.y, s1);
+    }
+#pragma unroll
+    for (int r = 0; r < kR; r += 2) {
+        const double2 vh = __ldcg(reinterpret_cast<const double2 *>(fac + NB + row0 + r));
+        const double2 vq = __ldcg(reinterpret_cast<const double2 *>(fac + 2 * NB + row0 + r));
+        F.h[r] = vh.x; F.h[r + 1] = vh.y;
+        F.q[r] = vq.x; F.q[r + 1] = vq.y;
+    }
+    if (lane == 0) F.h[0] = 0.0;
+    if (lane == 31) F.q[kR - 1] = 0.0;
+    scan_multipliers<SRC>(F, lane);
+    double *hk = wsm + 2 * NB + lane;
+#pragma unroll
+    for (int lv = 0; lv < 5; lv++) {
+        hk[lv * 32] = F.hk[lv];
+        hk[(5 + lv) * 32] = F.qk[lv];
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// Short-chain sub-step (kSolveScan4).  substep() runs, per sub-step, the
+// forward recurrence (local pass, 5-level warp scan, carry shuffle, second
+// local pass) and then the back substitution the same way, one after the
+// other: two scans of six dependent shuffles each plus four dependent local
+// passes.  This form shortens that chain in two ways.
+//
+// * Radix-4 warp scans: the carry into lane i is gathered from the
+//   aggregates of lanes i-1..i-4 (four shuffles issued together), then from
+//   those partial carries at lanes i-4, i-8, i-12, then at i-16: three
+//   dependent shuffle levels instead of six, exclusive directly.
+// * The back substitution's local pass runs on the forward pass's raw
+//   (zero-carry) values while the forward scan is in flight.  Both
+//   recurrences are linear, so the true back aggregate of the lane is the raw
+//   one plus per-segment constants times the forward carry; the forward
+//   carry then reaches the rows as z = raw + (product of h) carry, a chain of
+//   multiplies that runs while the back scan is in flight.
+//
+// The sums are the same as substep()'s, regrouped (results agree to
+// rounding, not bit for bit).
+struct Scan4 {
+    double fw[3];    // forward level 1: weights of the aggregates of lanes i-2, i-3, i-4 (i-1: 1)
+    double fp[4];    // forward levels 2, 3: products of H over lanes i-4..i-1, i-8.., i-12.., i-16..
+    double bw[3];    // the same for the back substitution (lanes i+2, i+3, i+4)
+    double bp[4];
+    double kh;       // back aggregate of the upper half's carry response to z at its first row - 1
+    double qk, kc;   // qlo kh, and the full back aggregate's response to the forward carry
+};
+
+// Forward exclusive scan: the carry into this lane (z at the last row of the
+// lane below), from each lane's zero-carry aggregate a.  Weights outside the
+// warp are zero, so the shuffles need no lane predicates (a shuffle from
+// outside the warp returns the caller's own finite value).
+__device__ __forceinline__ double scan4_up(double a, const double fw[3], const double fp[4], int lane)
+{
+    const double s1 = sup(a, 1), s2 = sup(a, 2), s3 = sup(a, 3), s4 = sup(a, 4);
+    const double S = fma(fw[0], s2, lane >= 1 ? s1 : 0.0) + fma(fw[2], s4, fw[1] * s3);
+    const double t4 = sup(S, 4), t8 = sup(S, 8), t12 = sup(S, 12);
+    const double E = fma(fp[0], t4, S) + fma(fp[2], t12, fp[1] * t8);
+    return fma(fp[3], sup(E, 16), E);
+}
+
+// Back exclusive scan: the carry into this lane from above (x at the first
+// row of the lane above).
+__device__ __forceinline__ double scan4_down(double a, const double bw[3], const double bp[4], int lane)
+{
+    const double s1 = sdn(a, 1), s2 = sdn(a, 2), s3 = sdn(a, 3), s4 = sdn(a, 4);
+    const double S = fma(bw[0], s2, lane <= 30 ? s1 : 0.0) + fma(bw[2], s4, bw[1] * s3);
+    const double t4 = sdn(S, 4), t8 = sdn(S, 8), t12 = sdn(S, 12);
+    const double E = fma(bp[0], t4, S) + fma(bp[2], t12, bp[1] * t8);
+    return fma(bp[3], sdn(E, 16), E);
+}
+
+// The Scan4 constants of the lane's coefficients (after load_coef).
+template <bool SRC>
+__device__ __forceinline__ void make_scan4(const Coef<SRC> &F, Scan4 &R, int lane)
+{
+    const double H = F.hlo * F.hhi, Q = F.qlo * F.qhi;   // products over the lane's rows
+    {
+        const double h1 = sup(H, 1), h2 = sup(H, 2), h3 = sup(H, 3), h4 = sup(H, 4);
+        const double w3 = h1 * h2, w4 = w3 * h3, p4 = w4 * h4;
+        const double p8 = p4 * sup(p4, 4);
+        const double p12 = p8 * sup(p4, 8);
+        const double p16 = p8 * sup(p8, 8);
+        R.fw[0] = lane >= 2 ? h1 : 0.0;
+        R.fw[1] = lane >= 3 ? w3 : 0.0;
+        R.fw[2] = lane >= 4 ? w4 : 0.0;
+        R.fp[0] = lane >= 4 ? p4 : 0.0;
+        R.fp[1] = lane >= 8 ? p8 : 0.0;
+        R.fp[2] = lane >= 12 ? p12 : 0.0;
+        R.fp[3] = lane >= 16 ? p16 : 0.0;
+    }
+    {
+        const double q1 = sdn(Q, 1), q2 = sdn(Q, 2), q3 = sdn(Q, 3), q4 = sdn(Q, 4);
+        const double w3 = q1 * q2, w4 = w3 * q3, p4 = w4 * q4;
+        const double p8 = p4 * sdn(p4, 4);
+        const double p12 = p8 * sdn(p4, 8);
+        const double p16 = p8 * sdn(p8, 8);
+        R.bw[0] = lane <= 29 ? q1 : 0.0;
+        R.bw[1] = lane <= 28 ? w3 : 0.0;
+        R.bw[2] = lane <= 27 ? w4 : 0.0;
+        R.bp[0] = lane <= 27 ? p4 : 0.0;
+        R.bp[1] = lane <= 23 ? p8 : 0.0;
+        R.bp[2] = lane <= 19 ? p12 : 0.0;
+        R.bp[3] = lane <= 15 ? p16 : 0.0;
+    }
+    // the back aggregate of each half applied to the half's forward carry
+    // response (the running products of h from the half's first row)
+    constexpr int H2 = kR / 2;
+    double clo[H2], chi[H2];
+    double c0 = 1.0, c1 = 1.0;
+#pragma unroll
+    for (int r = 0; r < H2; r++) {
+        c0 *= F.h[r];
+        c1 *= F.h[r + H2];
+        clo[r] = c0;
+        chi[r] = c1;
+    }
+    double kl = 0.0, kh = 0.0;
+#pragma unroll
+    for (int r = H2 - 1; r >= 0; r--) {
+        kl = fma(F.q[r], kl, clo[r]);
+        kh = fma(F.q[r + H2], kh, chi[r]);
+    }
+    R.kh = kh;
+    R.qk = F.qlo * kh;
+    R.kc = fma(R.qk, F.hlo, kl);
+}
+
+template <bool SRC>
+__device__ __forceinline__ void substep4(const Coef<SRC> &F, const Scan4 &R, int lane, double N[kR])
+{
+    constexpr int H2 = kR / 2;
+    // forward, zero carry into each half: N <- the raw chain values
+    double alo = 0.0, ahi = 0.0;
+#pragma unroll
+    for (int r = 0; r < H2; r++) {
+        const double ylo = SRC ? fma(N[r], F.inv[r], F.sd[r]) : N[r] * F.inv[r];
+        const double yhi = SRC ? fma(N[r + H2], F.inv[r + H2], F.sd[r + H2]) : N[r + H2] * F.inv[r + H2];
+        alo = fma(F.h[r], alo, ylo);
+        ahi = fma(F.h[r + H2], ahi, yhi);
+        N[r] = alo;
+        N[r + H2] = ahi;
+    }
+    const double af = fma(F.hhi, alo, ahi);
+    // back aggregates of the raw values, independent of the forward scan
+    double blo = 0.0, bhi = 0.0;
+#pragma unroll
+    for (int r = H2 - 1; r >= 0; r--) {
+        blo = fma(F.q[r], blo, N[r]);
+        bhi = fma(F.q[r + H2], bhi, N[r + H2]);
+    }
+    const double bpre = fma(R.qk, alo, fma(F.qlo, bhi, blo));
+    const double cin = scan4_up(af, R.fw, R.fp, lane);
+    const double zh = fma(F.hlo, cin, alo);          // z at the lower half's last row
+    const double cout = scan4_down(fma(R.kc, cin, bpre), R.bw, R.bp, lane);
+    const double bhi_t = fma(R.kh, zh, bhi);         // the upper half's true back aggregate
+    // the forward carry's response: z = raw + (running product of h) carry
+    double d = cin, e = zh;
+#pragma unroll
+    for (int r = 0; r < H2; r++) {
+        d *= F.h[r];
+        e *= F.h[r + H2];
+        N[r] += d;
+        N[r + H2] += e;
+    }
+    // back substitution: x_i = z_i + q_i x_{i+1}
+    double phi = cout, plo = fma(F.qhi, cout, bhi_t);
 #pragma unroll
     for (int r = H2 - 1; r >= 0; r--) {
         phi = fma(F.q[r + H2], phi, N[r + H2]);
@@ -1047,17 +1299,21 @@ __device__ __forceinline__ void substep_pcr(const Coef<SRC> &F, const double cc[
 // per-segment constants in registers, or in shared memory to leave registers
 // for more warps), the same with FP32 solves refined by an FP64 residual, and
 // warp PCR.
-enum { kSolveScan = 0, kSolveRefined = 1, kSolvePcr = 2, kSolveScanShared = 3 };
+enum { kSolveScan = 0, kSolveRefined = 1, kSolvePcr = 2, kSolveScanShared = 3, kSolveScanRhs = 4,
+       kSolveScan4 = 5 };
 
 // Steps kernel: warp w of block b runs every segment [g0, g1) of tracer
 // t0 + b * WPB + w for species S with sub-step solver SOLVER.
 template <int S, bool SRC, int SOLVER, int WPB>
 __global__ void __launch_bounds__(WPB * 32,
-                                  (SOLVER == kSolveScanShared ? (NB <= 256 ? 20 : 12) : (NB <= 256 ? 16 : 8)) / WPB)
+                                  (SOLVER == kSolveScanShared ? (NB <= 256 ? 20 : 12)
+                                   : SOLVER == kSolveScanRhs  ? (WPB == 1 ? (NB <= 256 ? 24 : 16) : (NB <= 256 ? 20 : 12))
+                                                              : (NB <= 256 ? 16 : 8)) / WPB)
     steps_kernel(FusedParams P)
 {
     extern __shared__ double4 steps_smem[];
     constexpr bool kSm = SOLVER == kSolveScanShared;
+    constexpr bool kRhs = SOLVER == kSolveScanRhs;
     const int w = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int tl = blockIdx.x * WPB + w;
@@ -1068,17 +1324,14 @@ __global__ void __launch_bounds__(WPB * 32,
     double *Nrow = (P.cal_spec ? P.cal_spec + (size_t)tl * NB : (S == 0 ? a.crp : a.cre) + (size_t)t * NB) + row0;
     double N[kR];
 #pragma unroll
-    for (int r = 0; r < kR; r += 2) {
-        const double2 v = *reinterpret_cast<const double2 *>(Nrow + r);
-        N[r] = v.x;
-        N[r + 1] = v.y;
-    }
+    for (int r = 0; r < kR; r += 4) ld4(Nrow + r, N + r);
     const double *qsrc = (S == 0) ? a.qpi : a.qepri;
     Coef<SRC> F;
     Coef32 G;
+    Scan4 R4;
     double cc[SOLVER == kSolvePcr ? kR : 1];
     PcrSmem *pcr_sm = reinterpret_cast<PcrSmem *>(steps_smem) + w;
-    double *coef_sm = reinterpret_cast<double *>(steps_smem) + (size_t)w * kCoefSmemDoubles + lane;
+    double *coef_sm = reinterpret_cast<double *>(steps_smem) + (size_t)w * (kRhs ? kRhsSmemDoubles : kCoefSmemDoubles);
     double scale = 1.0;
     int budget = P.cal_steps > 0 ? P.cal_steps : 0x7fffffff;
     const int nslot = P.g1 - P.g0;
@@ -1130,19 +1383,21 @@ __global__ void __launch_bounds__(WPB * 32,
             run_n = min(run_n, budget);
             budget -= run_n;
             if (want != cur) {
-                load_coef<SRC>(F, fac_ptr(P, S, gi, want, tl), src, g.dt, lane);
+                if (kRhs) load_coef_rhs<SRC>(F, fac_ptr(P, S, gi, want, tl), src, g.dt, lane, coef_sm);
+                else load_coef<SRC>(F, fac_ptr(P, S, gi, want, tl), src, g.dt, lane);
                 if (SOLVER == kSolveRefined) make_coef32<SRC>(F, G, lane);
+                if (SOLVER == kSolveScan4) make_scan4<SRC>(F, R4, lane);
                 if (SOLVER == kSolvePcr) pcr_rows_from_factored<SRC>(F, cc, lane);
                 if (kSm) {
                     __syncwarp();   // the previous run's reads of the slice are done
                     if (SRC) {
 #pragma unroll
-                        for (int r = 0; r < kR; r++) coef_sm[r * 32] = F.sd[r];
+                        for (int r = 0; r < kR; r++) coef_sm[r * 32 + lane] = F.sd[r];
                     }
 #pragma unroll
                     for (int lv = 0; lv < 5; lv++) {
-                        coef_sm[NB + lv * 32] = F.hk[lv];
-                        coef_sm[NB + (5 + lv) * 32] = F.qk[lv];
+                        coef_sm[NB + lv * 32 + lane] = F.hk[lv];
+                        coef_sm[NB + (5 + lv) * 32 + lane] = F.qk[lv];
                     }
                     __syncwarp();
                 }
@@ -1157,7 +1412,13 @@ __global__ void __launch_bounds__(WPB * 32,
                 for (int istep = 0; istep < run_n; istep++) substep_pcr<SRC>(F, cc, N, *pcr_sm, lane);
             } else if (kSm) {
 #pragma unroll 2
-                for (int istep = 0; istep < run_n; istep++) substep_sm<SRC>(F, coef_sm, N);
+                for (int istep = 0; istep < run_n; istep++) substep_sm<SRC, false>(F, coef_sm, lane, N);
+            } else if (kRhs) {
+#pragma unroll 1
+                for (int istep = 0; istep < run_n; istep++) substep_sm<SRC, true>(F, coef_sm, lane, N);
+            } else if (SOLVER == kSolveScan4) {
+#pragma unroll 1
+                for (int istep = 0; istep < run_n; istep++) substep4<SRC>(F, R4, lane, N);
             } else {
                 // two sub-steps per trip: the carried spectrum keeps its
                 // registers across the loop (fewer copies per sub-step)
@@ -1168,8 +1429,7 @@ __global__ void __launch_bounds__(WPB * 32,
         }
     }
 #pragma unroll
-    for (int r = 0; r < kR; r += 2)
-        *reinterpret_cast<double2 *>(Nrow + r) = make_double2(N[r], N[r + 1]);
+    for (int r = 0; r < kR; r += 4) st4(Nrow + r, N + r);
 }
 
 // Per-step kernel (the plain path): warp w of block b advances tracer
@@ -1209,11 +1469,7 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 20 : 12)) plain_step
         // rows a, b, c of the set: A <- a, inv <- b, q <- c, then the pivots
         load_rows(fac_ptr(P, S, 0, set, tl), lane, F.h, F.inv, F.q);
 #pragma unroll
-        for (int r = 0; r < kR; r += 2) {
-            const double2 v = *reinterpret_cast<const double2 *>(Nrow + r);
-            N[r] = v.x;
-            N[r + 1] = v.y;
-        }
+        for (int r = 0; r < kR; r += 4) ld4(Nrow + r, N + r);
         const unsigned err = pivot_rows(F.h, F.inv, F.q, lane);
         if (__any_sync(kFull, err != 0)) {
             if (lane == 0) atomicOr(a.err, kErrSingular);
@@ -1222,8 +1478,7 @@ __global__ void __launch_bounds__(kWarps * 32, (NB <= 256 ? 20 : 12)) plain_step
         finish_coef<SRC>(F, src, dt, lane);
         substep<SRC>(F, N);
 #pragma unroll
-        for (int r = 0; r < kR; r += 2)
-            *reinterpret_cast<double2 *>(Nrow + r) = make_double2(N[r], N[r + 1]);
+        for (int r = 0; r < kR; r += 4) st4(Nrow + r, N + r);
     }
 }
 
@@ -1320,13 +1575,6 @@ struct GemmSmem {
     double A[2][kGM][kGPitchA];
     double B[2][kGK][kGPitchB];
 };
-
-__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    const int n = valid ? 16 : 0;   // 0 source bytes: the 16 destination bytes are zero-filled
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
-}
 
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 {
@@ -1486,7 +1734,9 @@ cudaError_t launch_steps_variant(cudaStream_t st, const FusedParams &P, int trac
     const int n = tracers > 0 ? min(tracers, P.nt) : P.nt;
     const int blocks = (n + WPB - 1) / WPB;
     const size_t smem = SOLVER == kSolvePcr ? WPB * sizeof(PcrSmem)
-                      : (SOLVER == kSolveScanShared ? (size_t)WPB * kCoefSmemDoubles * sizeof(double) : 0);
+                      : SOLVER == kSolveScanShared ? (size_t)WPB * kCoefSmemDoubles * sizeof(double)
+                      : SOLVER == kSolveScanRhs    ? (size_t)WPB * kRhsSmemDoubles * sizeof(double)
+                                                   : 0;
     if (smem > 48 * 1024) {
         static const cudaError_t attr = cudaFuncSetAttribute(steps_kernel<S, SRC, SOLVER, WPB>,
                                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1497,10 +1747,24 @@ cudaError_t launch_steps_variant(cudaStream_t st, const FusedParams &P, int trac
 }
 
 // Variants the autotuner chooses between: (solver, warps per block).
-constexpr int kStepVariants = 5;
+constexpr int kStepVariants = CROMA_B200_STEPS_VARIANTS;
 constexpr int kVariantSolver[kStepVariants] = {kSolveScan, kSolveScan, kSolveScanShared, kSolveScanShared,
-                                               kSolvePcr};
-constexpr int kVariantWpb[kStepVariants] = {1, 2, 1, 2, 1};
+                                               kSolvePcr, kSolveScanRhs, kSolveScanRhs, kSolveScan4,
+                                               kSolveScan4};
+constexpr int kVariantWpb[kStepVariants] = {1, 2, 1, 2, 1, 1, 2, 1, 2};
+
+// Arithmetic families: variants of one family compute bit-identical results
+// (the same operations in the same order; only where the constants live and
+// how many warps share a block differ), so the tuner's timing-based choice
+// within a family never changes a result.  0: the scan; 1: the short-chain
+// scan; 2: PCR.
+constexpr int kVariantFamily[kStepVariants] = {0, 0, 0, 0, 2, 0, 0, 1, 1};
+
+// The family the tuner times: PCR when CROMA_CUDA_TRIDIAG=pcr, else the
+// short-chain scan at 512 bins and more (measured faster there: its shorter
+// shuffle chain outweighs its extra instructions at 8 warps per SM) and the
+// scan below (where the short-chain form spills at the larger warp count).
+int tune_family(int env) { return env == 2 ? 2 : (NB >= 512 ? 1 : 0); }
 
 template <int S, bool SRC>
 cudaError_t launch_variant(cudaStream_t st, const FusedParams &P, int v, int tracers)
@@ -1510,6 +1774,10 @@ cudaError_t launch_variant(cudaStream_t st, const FusedParams &P, int v, int tra
     case 2: return launch_steps_variant<S, SRC, kSolveScanShared, 1>(st, P, tracers);
     case 3: return launch_steps_variant<S, SRC, kSolveScanShared, 2>(st, P, tracers);
     case 4: return launch_steps_variant<S, SRC, kSolvePcr, 1>(st, P, tracers);
+    case 5: return launch_steps_variant<S, SRC, kSolveScanRhs, 1>(st, P, tracers);
+    case 6: return launch_steps_variant<S, SRC, kSolveScanRhs, 2>(st, P, tracers);
+    case 7: return launch_steps_variant<S, SRC, kSolveScan4, 1>(st, P, tracers);
+    case 8: return launch_steps_variant<S, SRC, kSolveScan4, 2>(st, P, tracers);
     default: return launch_steps_variant<S, SRC, kSolveScan, 1>(st, P, tracers);
     }
 }
@@ -1527,12 +1795,23 @@ int tridiag_env()
 }
 
 // The autotuner: on the first chunk a context evolves, each admissible
-// variant runs the chunk's first tracers (at most 2,048) for their first 16
-// sub-steps on a copy of their spectra, timed with CUDA events; the fastest
-// is kept for the context's species.  Results are recorded in ctx.tune.
-// CROMA_B200_STEPS_VARIANT = 0..4 fixes the variant (scan x1, scan x2, shared
-// scan x1, shared scan x2, PCR)
+// variant of the family tune_family names runs the chunk's first tracers (at
+// most kTuneTracers) for their first 16 sub-steps on a copy of their spectra,
+// timed with CUDA events; the fastest is kept for the context's species.  Results are recorded in
+// ctx.tune.  kTuneTracers is several full waves of every variant (8 to 24
+// warps per SM on 148 SMs): a sample below one wave favours the variants
+// with more warps per SM, which lose at full size.  A calibration on the full
+// sample is kept for the process (per species, source and
+// CROMA_CUDA_TRIDIAG setting) and reused by later contexts with at least as
+// many tracers; smaller chunks calibrate on themselves.
+// CROMA_B200_STEPS_VARIANT = 0..8 fixes the variant (scan x1, scan x2, shared
+// scan x1, shared scan x2, PCR, rhs-shared scan x1, rhs-shared scan x2,
+// short-chain scan x1, short-chain scan x2)
 // without calibrating, for reproducible profiles; unset or out of range: tune.
+constexpr int kTuneTracers = 16384;
+TuneState g_tune[2][2][3];   // [species][source][CROMA_CUDA_TRIDIAG: unset, thomas, pcr]
+std::mutex g_tune_mu;
+
 int fixed_variant_env()
 {
     const char *e = getenv("CROMA_B200_STEPS_VARIANT");
@@ -1552,7 +1831,16 @@ int tune_steps(Context &ctx, const FusedParams &P, bool src)
         return 0;
     }
     const int env = tridiag_env();
-    const int T = min(P.nt, 2048), steps = 16;
+    const int T = min(P.nt, kTuneTracers), steps = 16;
+    TuneState *shared = nullptr;
+    if (T == kTuneTracers) {
+        shared = &g_tune[S][src ? 1 : 0][env];
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        if (shared->tuned) {
+            tu = *shared;
+            return 0;
+        }
+    }
     double *scratch = nullptr;
     CROMA_CUDA(dev_alloc(ctx, &scratch, (size_t)T * NB * sizeof(double)));
     struct Free {
@@ -1568,10 +1856,10 @@ int tune_steps(Context &ctx, const FusedParams &P, bool src)
     CROMA_CUDA(cudaEventCreate(&e0));
     CROMA_CUDA(cudaEventCreate(&e1));
     int best = -1;
+    const int family = tune_family(env);
     for (int v = 0; v < kStepVariants; v++) {
-        const bool pcr = kVariantSolver[v] == kSolvePcr;
         tu.ms[v] = -1.0;
-        if ((env == 1 && pcr) || (env == 2 && !pcr)) continue;
+        if (kVariantFamily[v] != family) continue;
         double ms_best = 1e30;
         for (int rep = 0; rep < 2; rep++) {   // the first run warms the code and L2
             CROMA_CUDA(cudaMemcpyAsync(scratch, real, (size_t)T * NB * sizeof(double), cudaMemcpyDeviceToDevice,
@@ -1593,6 +1881,10 @@ int tune_steps(Context &ctx, const FusedParams &P, bool src)
     tu.tuned = 1;
     tu.tracers = T;
     tu.steps = steps;
+    if (shared) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        if (!shared->tuned) *shared = tu;
+    }
     return 0;
 }
 
@@ -1800,6 +2092,13 @@ static int fused_chunks(Context &ctx, FusedParams &P, int nslots, bool perstep)
     const bool windows = P.explicit_seg ? P.ex.windowed != 0 : ctx.mp.window_centred != 0;
     if (windows && ctx.fused_sets < 2) {
         set_error("internal: windowed segments without an off-coefficient workspace");
+        return -1;
+    }
+    // the evolve kernels access rows with 32-byte vector loads and stores
+    auto misaligned = [](const void *p) { return ((uintptr_t)p & 31u) != 0; };
+    if (misaligned(P.a.crp) || misaligned(P.a.cre) || misaligned(P.a.qpi) || misaligned(P.a.qepri) ||
+        misaligned(ctx.d_fac) || misaligned(ctx.d_inje)) {
+        set_error("internal: spectra, sources or workspace not 32-byte aligned");
         return -1;
     }
     const bool cap = ctx.mp.eta_dpp_cap > 0.0 && isfinite(ctx.mp.eta_dpp_cap) && ctx.mp.dpp_model != kDppOff;

@@ -74,6 +74,7 @@ def load_library(nb: int) -> C.CDLL:
     L.croma_b200_kernel_stats.argtypes = [_vp, _i, P(_d), P(C.c_longlong)]
     L.croma_b200_reset_kernel_stats.argtypes = [_vp]
     L.croma_b200_fp64_peak.argtypes = [P(_d)]
+    L.croma_b200_rcp_check.argtypes = [C.c_longlong, _vp, _vp]
     L.croma_b200_get_sources.argtypes = [_vp, _vp, _vp, _vp]
     L.croma_b200_set_state_broadcast.argtypes = [_vp, _i, _vp, _vp, _d]
     L.croma_b200_set_dsa.argtypes = [_vp, P(CromaB200DsaParams)]
@@ -155,6 +156,17 @@ def fp64_peak(nb: int = 256) -> float:
     if L.croma_b200_fp64_peak(C.byref(t)) != 0:
         raise CromaError(L.croma_b200_last_error().decode())
     return t.value
+
+
+def rcp_check(x, nb: int = 256):
+    """The device reciprocal of the factor and per-step kernels applied to
+    the float64 array x (croma_b200_rcp_check)."""
+    L = load_library(nb)
+    xa = _c(x)
+    out = np.empty_like(xa)
+    if L.croma_b200_rcp_check(xa.size, _p(xa), _p(out)) != 0:
+        raise CromaError(L.croma_b200_last_error().decode())
+    return out
 
 
 def _shocks_struct(shocks: dict):
@@ -356,17 +368,19 @@ class TracerFP:
         self._check(self.lib.croma_b200_step_host(self.h, C.byref(snap), C.byref(io)))
         del keep
 
-    SOLVERS = {0: "thomas-scan", 1: "thomas-scan-fp32-refined", 2: "pcr", 3: "thomas-scan-smem"}
+    SOLVERS = {0: "thomas-scan", 1: "thomas-scan-fp32-refined", 2: "pcr", 3: "thomas-scan-smem",
+               4: "thomas-scan-rhs-smem", 5: "thomas-scan4"}
+    VARIANTS = ("scan x1", "scan x2", "smem scan x1", "smem scan x2", "pcr x1", "rhs scan x1", "rhs scan x2",
+                "scan4 x1", "scan4 x2")
 
     def tuning(self, species: int):
         """The steps-kernel autotuner's record for species 0 (protons) or 1
         (electrons): dict(tuned, solver, warps_per_block, variant_ms)."""
         t, so, w = _i(), _i(), _i()
-        ms = (_d * 5)()
+        ms = (_d * len(self.VARIANTS))()
         self._check(self.lib.croma_b200_get_tuning(self.h, species, C.byref(t), C.byref(so), C.byref(w), ms))
-        names = ("scan x1", "scan x2", "smem scan x1", "smem scan x2", "pcr x1")
         return {"tuned": t.value, "solver": self.SOLVERS.get(so.value, so.value), "warps_per_block": w.value,
-                "variant_ms": {n: (m if m >= 0 else None) for n, m in zip(names, list(ms))}}
+                "variant_ms": {n: (m if m >= 0 else None) for n, m in zip(self.VARIANTS, list(ms))}}
 
     def sync(self):
         self._check(self.lib.croma_b200_sync(self.h))

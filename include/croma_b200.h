@@ -316,21 +316,31 @@ typedef struct {
 } CromaB200StepHost;
 int croma_b200_step_host(CromaB200Context *ctx, const CromaB200Snapshot *snap, const CromaB200StepHost *io);
 
-/* The steps-kernel autotuner (the on-chip FP64 path).  On the first
- * workspace chunk a context evolves, per species, each admissible variant --
- * the warp-scan Thomas with its per-segment constants in registers or in
- * shared memory (fewer registers, more warps per SM), at 1 or 2 tracers
- * (warps) per block, and warp PCR (one warp per tracer, parallel cyclic
- * reduction in shared memory) -- runs the chunk's first tracers (up to 2,048)
- * for 16 sub-steps on a copy of their spectra, timed with CUDA events, and
- * the fastest is kept for the context.  CROMA_CUDA_TRIDIAG=thomas admits only
- * the scan variants, =pcr only PCR (src/fp_cuda_solver.cu:41-72 of the
- * reference).  Reported here: tuned (0 before the first snapshot), solver
- * (0 scan, 1 FP32-refined scan, 2 PCR, 3 scan with shared-memory constants),
- * tracers per block, and the calibration time of each variant in
- * milliseconds, variant_ms[5] in the order scan x1, scan x2, shared scan x1,
- * shared scan x2, PCR (-1 = not run).  CROMA_B200_STEPS_VARIANT=0..4 fixes
- * the variant in that order without calibrating (reproducible profiles). */
+/* The steps-kernel autotuner (the on-chip FP64 path).  The arithmetic is
+ * fixed by rule, so that no result depends on a timing: the short-chain warp
+ * scan (radix-4 warp scans, the back substitution's local pass overlapping
+ * the forward scan) at 512 bins and more, the warp scan below, warp PCR (one
+ * warp per tracer, parallel cyclic reduction in shared memory) when
+ * CROMA_CUDA_TRIDIAG=pcr (src/fp_cuda_solver.cu:41-72 of the reference).
+ * Within that family the variants compute bit-identical results and differ
+ * in where the per-segment constants live -- registers, partly shared memory
+ * (fewer registers, more warps per SM), or with each row's right-hand-side
+ * scaling in shared memory too -- and in tracers (warps) per block, 1 or 2.
+ * On the first workspace chunk a context evolves, per species, each of them
+ * runs the chunk's first tracers (up to 16,384, several full waves of every
+ * variant) for 16 sub-steps on a copy of their spectra, timed with CUDA
+ * events, and the fastest is kept for the context; a calibration on the full
+ * 16,384 tracers is reused by the process's later contexts (same species,
+ * source and CROMA_CUDA_TRIDIAG).  Reported here: tuned (0 before the first
+ * snapshot), solver (0 scan, 1 FP32-refined scan, 2 PCR, 3 scan with
+ * shared-memory constants, 4 scan with the right-hand-side scaling in shared
+ * memory, 5 short-chain scan), tracers per block, and the calibration time of
+ * each variant in milliseconds, variant_ms[CROMA_B200_STEPS_VARIANTS] in the
+ * order scan x1, scan x2, shared scan x1, shared scan x2, PCR, rhs-shared
+ * scan x1, rhs-shared scan x2, short-chain scan x1, short-chain scan x2
+ * (-1 = not run).  CROMA_B200_STEPS_VARIANT=0..8 fixes the variant in that
+ * order without calibrating (reproducible profiles). */
+#define CROMA_B200_STEPS_VARIANTS 9
 int croma_b200_get_tuning(CromaB200Context *ctx, int species, int *tuned, int *solver, int *warps_per_block,
                           double *variant_ms);
 
@@ -345,6 +355,11 @@ int croma_b200_host_free(void *p);
  * independent fused multiply-add chains on every SM (TFLOP/s, FMA = 2 flops);
  * the denominator of the fused evolve's roofline. */
 int croma_b200_fp64_peak(double *tflops);
+
+/* The device reciprocal of the factor and per-step kernels (an inline
+ * rcp.approx.ftz.f64 refined by two Newton-Raphson steps) applied to n host
+ * doubles x on the current device, for checking its error bound. */
+int croma_b200_rcp_check(long long n, const double *x, double *out);
 
 #ifdef __cplusplus
 }

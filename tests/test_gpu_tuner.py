@@ -1,8 +1,10 @@
 """The steps-kernel autotuner (fused path): after the first snapshot each
 evolving species has a tuned variant and a calibration time for every
-admissible variant; CROMA_CUDA_TRIDIAG=pcr restricts it to warp PCR and
-=thomas to the warp-scan variants, and whichever variant runs, the spectra
-match the reference's (golden fixture) to the FP64 bar."""
+variant of its arithmetic family (the short-chain scan at 512 bins, the scan
+below, PCR under CROMA_CUDA_TRIDIAG=pcr); =thomas keeps the scan families.
+Whichever variant runs, the spectra match the reference's (golden fixture) to
+the FP64 bar, and the variants of one family give bit-identical spectra, so
+the timing-based choice never changes a result."""
 import numpy as np
 import pytest
 
@@ -15,7 +17,15 @@ from croma_fp_b200 import native  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 
-def _run(name, env, monkeypatch):
+FAMILIES = {
+    "scan": ("scan x1", "scan x2", "smem scan x1", "smem scan x2", "rhs scan x1", "rhs scan x2"),
+    "scan4": ("scan4 x1", "scan4 x2"),
+}
+VARIANT_INDEX = {"scan x1": 0, "scan x2": 1, "smem scan x1": 2, "smem scan x2": 3, "pcr x1": 4,
+                 "rhs scan x1": 5, "rhs scan x2": 6, "scan4 x1": 7, "scan4 x2": 8}
+
+
+def _run(name, env, monkeypatch, state=False):
     if env is None:
         monkeypatch.delenv("CROMA_CUDA_TRIDIAG", raising=False)
     else:
@@ -33,21 +43,36 @@ def _run(name, env, monkeypatch):
     assert rel_err(cre, d["cre_0"]) <= 1e-10
     if np.any(d["crp_0"]):
         assert rel_err(crp, d["crp_0"]) <= 1e-10
-    return tunes
+    return (tunes, crp, cre) if state else tunes
 
 
-@pytest.mark.parametrize("name", ["c1_asa128", "c4_asa512"])
-def test_tuner_chooses_and_records(name, monkeypatch):
+@pytest.mark.parametrize("name,family", [("c1_asa128", "scan"), ("c4_asa512", "scan4")])
+def test_tuner_chooses_and_records(name, family, monkeypatch):
     tunes = _run(name, None, monkeypatch)
     for t in tunes:
         assert t["tuned"] == 1
         ms = t["variant_ms"]
-        assert all(v is not None and v > 0 for v in ms.values()), ms
+        timed = {k for k, v in ms.items() if v is not None}
+        assert timed == set(FAMILIES[family]), ms
+        assert all(ms[k] > 0 for k in timed)
         chosen = {("thomas-scan", 1): "scan x1", ("thomas-scan", 2): "scan x2",
                   ("thomas-scan-smem", 1): "smem scan x1", ("thomas-scan-smem", 2): "smem scan x2",
-                  ("pcr", 1): "pcr x1"}[(t["solver"], t["warps_per_block"])]
-        assert ms[chosen] == min(ms.values())
+                  ("pcr", 1): "pcr x1", ("thomas-scan-rhs-smem", 1): "rhs scan x1",
+                  ("thomas-scan-rhs-smem", 2): "rhs scan x2",
+                  ("thomas-scan4", 1): "scan4 x1", ("thomas-scan4", 2): "scan4 x2"}[(t["solver"], t["warps_per_block"])]
+        assert ms[chosen] == min(ms[k] for k in timed)
     print(name, tunes)
+
+
+@pytest.mark.parametrize("name,family", [("c1_asa256", "scan"), ("c4_asa512", "scan4")])
+def test_variants_of_a_family_are_bit_identical(name, family, monkeypatch):
+    states = []
+    for v in FAMILIES[family]:
+        monkeypatch.setenv("CROMA_B200_STEPS_VARIANT", str(VARIANT_INDEX[v]))
+        _, crp, cre = _run(name, None, monkeypatch, state=True)
+        states.append((v, crp, cre))
+    for v, crp, cre in states[1:]:
+        assert np.array_equal(crp, states[0][1]) and np.array_equal(cre, states[0][2]), v
 
 
 @pytest.mark.parametrize("env,solver", [("pcr", "pcr"), ("thomas", "thomas-scan")])
@@ -60,7 +85,7 @@ def test_tridiag_env_restricts_the_tuner(env, solver, monkeypatch):
             assert t["variant_ms"]["pcr x1"] is None
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8])
 @pytest.mark.parametrize("name", ["c1_asa256", "c4_asa512"])
 def test_every_steps_variant_matches_reference(name, variant, monkeypatch):
     monkeypatch.setenv("CROMA_B200_STEPS_VARIANT", str(variant))
