@@ -55,7 +55,7 @@ SHOCK_KEYS = ("mach", "prestemp", "presden", "shock_side_code")
 # tracer moves its own rows, so a launch's traffic is this figure times the
 # tracers it processes.  steps: mean of the proton and electron launches;
 # plain_steps: the electron launch of one segment slot.
-NCU_DRAM_BYTES_PER_TRACER = {"steps": (272.35e3 + 270.86e3) / 2, "plain_steps": 23.79e3}
+NCU_DRAM_BYTES_PER_TRACER = {"steps": (272.2e3 + 271.0e3) / 2, "plain_steps": 23.7e3}
 
 
 def load_package():
