@@ -811,11 +811,12 @@ __global__ void fp64_fma_probe(int iters, double seed, double *out)
     for (int k = 0; k < 8; k++) s += x[k];
     if (s == 12345.678) out[blockIdx.x] = s;
 }
-// rcp_nr (the factor and per-step kernels' reciprocal) element-wise.
-__global__ void rcp_probe(long long n, const double *x, double *out)
+// rcp_nr (the factor and per-step kernels' reciprocal) or exp_tab (their
+// exponential) element-wise.
+__global__ void math_probe(int which, long long n, const double *x, double *out)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        out[i] = croma::rcp_nr(x[i]);
+        out[i] = which == 0 ? croma::rcp_nr(x[i]) : croma::exp_tab(x[i]);
 }
 }  // namespace croma_probe
 
@@ -847,23 +848,26 @@ int croma_b200_host_free(void *p)
     return 0;
 }
 
-int croma_b200_rcp_check(long long n, const double *x, double *out)
+static int math_check(int which, long long n, const double *x, double *out)
 {
-    if (n < 0 || (n > 0 && (!x || !out))) { set_error("invalid rcp_check arguments"); return -1; }
+    if (n < 0 || (n > 0 && (!x || !out))) { set_error("invalid math check arguments"); return -1; }
     if (n == 0) return 0;
     double *d = nullptr;
     CROMA_CUDA(cudaMalloc(&d, 2 * (size_t)n * sizeof(double)));
     cudaError_t e = cudaMemcpy(d, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
         const long long blocks = (n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096;
-        croma_probe::rcp_probe<<<(unsigned)blocks, 256>>>(n, d, d + n);
+        croma_probe::math_probe<<<(unsigned)blocks, 256>>>(which, n, d, d + n);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpy(out, d + n, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
     cudaFree(d);
-    if (e != cudaSuccess) return cuda_fail(e, "rcp_check");
+    if (e != cudaSuccess) return cuda_fail(e, "math check");
     return 0;
 }
+
+int croma_b200_rcp_check(long long n, const double *x, double *out) { return math_check(0, n, x, out); }
+int croma_b200_exp_check(long long n, const double *x, double *out) { return math_check(1, n, x, out); }
 
 int croma_b200_fp64_peak(double *tflops)
 {

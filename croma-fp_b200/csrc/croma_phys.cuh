@@ -235,10 +235,60 @@ CROMA_HD double rcp_nr(double x)
 #endif
 }
 
+// FP64 exp for the factor kernels' face weights and Coulomb term: Tang's
+// table-driven method (P. T. P. Tang, "Table-driven implementation of the
+// exponential function in IEEE floating-point arithmetic", ACM TOMS 15(2),
+// 1989).  x = (32 m + j) ln2/32 + r with N = 32 m + j = rint(32 x / ln2)
+// (the 1.5 * 2^52 shifter leaves N in the low word), |r| <= ln2/64 by a
+// two-part reduction with ln2/32 = kExpLhi + kExpLlo, exp(r) - 1 by its
+// Taylor polynomial to degree 6 (truncation below 4e-18), and
+// exp(x) = 2^m (2^(j/32) + 2^(j/32) p), the scale applied as two exact
+// powers of two so that results down to the subnormal range are formed.
+// Within 1 ulp of the exact value in an exact-arithmetic emulation and on
+// the device (tested); about half the dependent depth of a general exp,
+// which is what the latency-bound factor kernel waits on.  x is clamped to
+// [-746, 709] (exp(-746) rounds to 0); a NaN stays a NaN.
+static __device__ const double kExp2J[32] = {
+    0x1.0000000000000p+0, 0x1.059b0d3158574p+0, 0x1.0b5586cf9890fp+0, 0x1.11301d0125b51p+0,
+    0x1.172b83c7d517bp+0, 0x1.1d4873168b9aap+0, 0x1.2387a6e756238p+0, 0x1.29e9df51fdee1p+0,
+    0x1.306fe0a31b715p+0, 0x1.371a7373aa9cbp+0, 0x1.3dea64c123422p+0, 0x1.44e086061892dp+0,
+    0x1.4bfdad5362a27p+0, 0x1.5342b569d4f82p+0, 0x1.5ab07dd485429p+0, 0x1.6247eb03a5585p+0,
+    0x1.6a09e667f3bcdp+0, 0x1.71f75e8ec5f74p+0, 0x1.7a11473eb0187p+0, 0x1.82589994cce13p+0,
+    0x1.8ace5422aa0dbp+0, 0x1.93737b0cdc5e5p+0, 0x1.9c49182a3f090p+0, 0x1.a5503b23e255dp+0,
+    0x1.ae89f995ad3adp+0, 0x1.b7f76f2fb5e47p+0, 0x1.c199bdd85529cp+0, 0x1.cb720dcef9069p+0,
+    0x1.d5818dcfba487p+0, 0x1.dfc97337b9b5fp+0, 0x1.ea4afa2a490dap+0, 0x1.f50765b6e4540p+0};
+constexpr double kExpInvL = 0x1.71547652b82fep+5;   // 32 / ln2
+constexpr double kExpLhi = 0x1.62e42fefa39efp-6;    // ln2 / 32, leading part
+constexpr double kExpLlo = 0x1.abc9e3b39803fp-61;   // ln2 / 32 - kExpLhi
+
+CROMA_HD double exp_tab(double x)
+{
+#ifdef __CUDA_ARCH__
+    x = x < -746.0 ? -746.0 : (x > 709.0 ? 709.0 : x);   // a NaN passes through
+    const double t = fma(x, kExpInvL, 0x1.8p52);
+    const double n = t - 0x1.8p52;
+    const int N = __double2loint(t);
+    double r = fma(-n, kExpLhi, x);
+    r = fma(-n, kExpLlo, r);
+    const double r2 = r * r;
+    const double u = fma(1.0 / 6.0, r, 0.5);
+    double v = fma(1.0 / 120.0, r, 1.0 / 24.0);
+    v = fma(1.0 / 720.0, r2, v);
+    const double p = fma(fma(v, r2, u), r2, r);
+    const double tj = __ldg(&kExp2J[N & 31]);
+    const int m = N >> 5, m1 = m >> 1, m2 = m - m1;
+    const double s1 = __hiloint2double((m1 + 1023) << 20, 0), s2 = __hiloint2double((m2 + 1023) << 20, 0);
+    return fma(tj, p, tj) * s1 * s2;
+#else
+    return exp(x);
+#endif
+}
+
 // The same weights with one exponential and one division per face and no
 // divergent branch (the evolve kernels' form): exp(-w/2) is taken as
-// 1/exp(w/2), the two quotients by the denominator share one reciprocal
-// (rcp_nr) and the series constants are multiplied in.  Agrees with
+// 1/exp(w/2), the exponential is exp_tab, the two quotients by the
+// denominator share one reciprocal (rcp_nr) and the series constants are
+// multiplied in.  Agrees with
 // face_weights to a few ulp.
 CROMA_HD void face_weights_fast(double w, double &wp, double &wm)
 {
@@ -246,7 +296,7 @@ CROMA_HD void face_weights_fast(double w, double &wp, double &wm)
     const bool series = aw < 0.1;
     const double w2 = w * w;
     const double dser = 1.0 + w2 * (1.0 / 24.0) + (w2 * w2) * (1.0 / 1920.0);
-    const double e = exp(series ? 0.5 * w : -aw);
+    const double e = exp_tab(series ? 0.5 * w : -aw);
     const double q = (series ? 1.0 : aw) * rcp_nr(series ? e * dser : 1.0 - e);
     const double s = q * e;
     // series: wm = 1 / (e dser), wp = e / dser; otherwise big = q, small = q e

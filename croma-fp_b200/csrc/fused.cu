@@ -181,7 +181,7 @@ __device__ __forceinline__ void rescale2(double &m00, double &m01, double &m10, 
 // outgrows the instruction cache.  Same arithmetic.
 __device__ __noinline__ double coulomb_slow(double x)
 {
-    return 0.5 * sqrt(kPi) * erf(sqrt(x)) - sqrt(x) * exp(-x);
+    return 0.5 * sqrt(kPi) * erf(sqrt(x)) - sqrt(x) * exp_tab(-x);
 }
 __device__ __forceinline__ double coulomb_one(double x)
 {

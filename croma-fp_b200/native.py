@@ -75,6 +75,7 @@ def load_library(nb: int) -> C.CDLL:
     L.croma_b200_reset_kernel_stats.argtypes = [_vp]
     L.croma_b200_fp64_peak.argtypes = [P(_d)]
     L.croma_b200_rcp_check.argtypes = [C.c_longlong, _vp, _vp]
+    L.croma_b200_exp_check.argtypes = [C.c_longlong, _vp, _vp]
     L.croma_b200_get_sources.argtypes = [_vp, _vp, _vp, _vp]
     L.croma_b200_set_state_broadcast.argtypes = [_vp, _i, _vp, _vp, _d]
     L.croma_b200_set_dsa.argtypes = [_vp, P(CromaB200DsaParams)]
@@ -158,15 +159,25 @@ def fp64_peak(nb: int = 256) -> float:
     return t.value
 
 
-def rcp_check(x, nb: int = 256):
-    """The device reciprocal of the factor and per-step kernels applied to
-    the float64 array x (croma_b200_rcp_check)."""
+def _math_check(fn: str, x, nb: int):
     L = load_library(nb)
     xa = _c(x)
     out = np.empty_like(xa)
-    if L.croma_b200_rcp_check(xa.size, _p(xa), _p(out)) != 0:
+    if getattr(L, fn)(xa.size, _p(xa), _p(out)) != 0:
         raise CromaError(L.croma_b200_last_error().decode())
     return out
+
+
+def rcp_check(x, nb: int = 256):
+    """The device reciprocal of the factor and per-step kernels applied to
+    the float64 array x (croma_b200_rcp_check)."""
+    return _math_check("croma_b200_rcp_check", x, nb)
+
+
+def exp_check(x, nb: int = 256):
+    """The factor kernels' table-driven exponential applied to the float64
+    array x (croma_b200_exp_check)."""
+    return _math_check("croma_b200_exp_check", x, nb)
 
 
 def _shocks_struct(shocks: dict):

@@ -360,6 +360,8 @@ int croma_b200_fp64_peak(double *tflops);
  * rcp.approx.ftz.f64 refined by two Newton-Raphson steps) applied to n host
  * doubles x on the current device, for checking its error bound. */
 int croma_b200_rcp_check(long long n, const double *x, double *out);
+/* The same for the factor kernels' table-driven exponential. */
+int croma_b200_exp_check(long long n, const double *x, double *out);
 
 #ifdef __cplusplus
 }
