@@ -142,7 +142,7 @@ __device__ __forceinline__ double sdn(double v, int d) { return __shfl_down_sync
 // 16-byte access per lane would touch 32 sectors and use half of each (a
 // scalar access a quarter); 32 bytes per lane use every sector fully.  The
 // asm is volatile so that the per-step path's re-reads stay in its loop.
-// ld4_cg: L2 only (rows and sources); ld4 / st4: the default caching.
+// ld4_cg / st4_cg: L2 only (rows and sources); ld4 / st4: the default caching.
 __device__ __forceinline__ void ld4_cg(const double *p, double *v)
 {
     asm volatile("ld.global.cg.v4.f64 {%0,%1,%2,%3}, [%4];"
@@ -156,6 +156,12 @@ __device__ __forceinline__ void ld4(const double *p, double *v)
 __device__ __forceinline__ void st4(double *p, const double *v)
 {
     asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]), "d"(v[2]), "d"(v[3])
+                 : "memory");
+}
+// st4 bypassing L1 (rows written for another kernel).
+__device__ __forceinline__ void st4_cg(double *p, const double *v)
+{
+    asm volatile("st.global.cg.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]), "d"(v[2]), "d"(v[3])
                  : "memory");
 }
 __device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid)
@@ -524,17 +530,17 @@ __device__ __forceinline__ unsigned pivot_rows(double A[kR], double Bd[kR], doub
     return err;
 }
 
-// Three row arrays of a lane to out[0..3nb): 64 contiguous bytes per array
-// per lane, 2 KB per array per warp.
+// Three row arrays of a lane to out[0..3nb): R contiguous doubles per array
+// per lane (32-byte stores), nb doubles per array per warp.
 __device__ __forceinline__ void store_rows(double *out, int lane, const double X[kR], const double Y[kR],
                                            const double Z[kR])
 {
     const int row0 = lane * kR;
 #pragma unroll
-    for (int r = 0; r < kR; r += 2) {
-        __stcg(reinterpret_cast<double2 *>(out + row0 + r), make_double2(X[r], X[r + 1]));
-        __stcg(reinterpret_cast<double2 *>(out + NB + row0 + r), make_double2(Y[r], Y[r + 1]));
-        __stcg(reinterpret_cast<double2 *>(out + 2 * NB + row0 + r), make_double2(Z[r], Z[r + 1]));
+    for (int r = 0; r < kR; r += 4) {
+        st4_cg(out + row0 + r, X + r);
+        st4_cg(out + NB + row0 + r, Y + r);
+        st4_cg(out + 2 * NB + row0 + r, Z + r);
     }
 }
 
@@ -1358,8 +1364,7 @@ __global__ void __launch_bounds__(WPB * 32,
         if (S == 0 && P.np_seg && !P.cal_spec) {
             double *o = P.np_seg + ((size_t)gi * P.nt + tl) * NB + row0;
 #pragma unroll
-            for (int r = 0; r < kR; r += 2)
-                __stcg(reinterpret_cast<double2 *>(o + r), make_double2(N[r], N[r + 1]));
+            for (int r = 0; r < kR; r += 4) st4_cg(o + r, N + r);
         }
         const double *src = nullptr;
         if (SRC) {
@@ -2097,7 +2102,7 @@ static int fused_chunks(Context &ctx, FusedParams &P, int nslots, bool perstep)
     // the evolve kernels access rows with 32-byte vector loads and stores
     auto misaligned = [](const void *p) { return ((uintptr_t)p & 31u) != 0; };
     if (misaligned(P.a.crp) || misaligned(P.a.cre) || misaligned(P.a.qpi) || misaligned(P.a.qepri) ||
-        misaligned(ctx.d_fac) || misaligned(ctx.d_inje)) {
+        misaligned(ctx.d_fac) || misaligned(ctx.d_inje) || misaligned(ctx.d_np_seg)) {
         set_error("internal: spectra, sources or workspace not 32-byte aligned");
         return -1;
     }
