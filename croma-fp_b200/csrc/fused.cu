@@ -801,7 +801,7 @@ __device__ __forceinline__ void substep(const Coef<SRC> &F, double N[kR])
 // row there, as (1 / d, dt src / d) pairs ([r][lane], one conflict-free
 // 16-byte read per row and sub-step): the lane then holds only N, h and q
 // (about 100 registers at 512 bins), for 16 warps per SM at 512 bins and 24
-// at 256.
+// at 256 with one warp per block (12 and 20 with two).
 constexpr int kCoefSmemDoubles = NB + 10 * 32;       // per warp: dt src / d, hk, qk
 constexpr int kRhsSmemDoubles = 2 * NB + 10 * 32;    // per warp: (1 / d, dt src / d), hk, qk
 
@@ -878,19 +878,17 @@ __device__ __forceinline__ void load_coef_rhs(Coef<SRC> &F, const double *fac, c
     double2 *rhs = reinterpret_cast<double2 *>(wsm) + lane;
     __syncwarp();   // the previous run's reads of the slice are done
 #pragma unroll
-    for (int r = 0; r < kR; r += 2) {
-        const double2 vi = __ldcg(reinterpret_cast<const double2 *>(fac + row0 + r));
-        const double s0 = SRC ? (dt * src[row0 + r]) * vi.x : 0.0;
-        const double s1 = SRC ? (dt * src[row0 + r + 1]) * vi.y : 0.0;
-        rhs[r * 32] = make_double2(vi.x, s0);
-        rhs[(r + 1) * 32] = make_double2(vi.y, s1);
+    for (int r = 0; r < kR; r += 4) {
+        double vi[4], vs[4] = {0.0, 0.0, 0.0, 0.0};
+        ld4_cg(fac + row0 + r, vi);
+        if (SRC) ld4_cg(src + row0 + r, vs);
+#pragma unroll
+        for (int i = 0; i < 4; i++) rhs[(r + i) * 32] = make_double2(vi[i], SRC ? (dt * vs[i]) * vi[i] : 0.0);
     }
 #pragma unroll
-    for (int r = 0; r < kR; r += 2) {
-        const double2 vh = __ldcg(reinterpret_cast<const double2 *>(fac + NB + row0 + r));
-        const double2 vq = __ldcg(reinterpret_cast<const double2 *>(fac + 2 * NB + row0 + r));
-        F.h[r] = vh.x; F.h[r + 1] = vh.y;
-        F.q[r] = vq.x; F.q[r + 1] = vq.y;
+    for (int r = 0; r < kR; r += 4) {
+        ld4_cg(fac + NB + row0 + r, F.h + r);
+        ld4_cg(fac + 2 * NB + row0 + r, F.q + r);
     }
     if (lane == 0) F.h[0] = 0.0;
     if (lane == 31) F.q[kR - 1] = 0.0;

@@ -90,3 +90,29 @@ def test_tridiag_env_restricts_the_tuner(env, solver, monkeypatch):
 def test_every_steps_variant_matches_reference(name, variant, monkeypatch):
     monkeypatch.setenv("CROMA_B200_STEPS_VARIANT", str(variant))
     _run(name, None, monkeypatch)
+
+
+def test_full_size_calibration_is_reused_by_later_contexts(monkeypatch):
+    """A context whose first chunk holds the full 16,384-tracer sample
+    calibrates once; a later context of the same species, source and
+    CROMA_CUDA_TRIDIAG setting in the same process reports the same record
+    (the same per-variant times) instead of timing again."""
+    from croma_fp_b200 import config, synth
+    monkeypatch.delenv("CROMA_CUDA_TRIDIAG", raising=False)
+    monkeypatch.delenv("CROMA_B200_STEPS_VARIANT", raising=False)
+    cfg = config.config1(nb=128)
+    nt = 16384
+    w = synth.Workload(cfg, nt, 100, seed=717)
+    records = []
+    for _ in range(2):
+        fp = native.TracerFP(cfg, path="fused")
+        try:
+            gp, ge = fp.grid(0), fp.grid(1)
+            crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), nt, cfg.species)
+            fp.set_state(crp, cre, mass=w.mass)
+            fp.snapshot(*w.snapshot_args(40), sync=True)
+            records.append([fp.tuning(s) for s in (0, 1)])
+        finally:
+            fp.close()
+    for a, b in zip(*records):
+        assert a["tuned"] == 1 and a == b
