@@ -623,6 +623,14 @@ def run_gpu_arm(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
+    def rank_max(x):
+        """The largest x over the ranks (x itself on one GPU)."""
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     cfg = workload_config()
     nt = args.tracers
     nsteps = args.warmup + args.steps
@@ -646,22 +654,24 @@ def run_gpu_arm(args):
                                  emission=not args.no_emission, kernel_timing=True, clock_dev=local, keep_open=True)
     if dist:
         dist.barrier()
-    ms_max = res["ms"]
-    if dist:
-        t = torch.tensor([ms_max], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = rank_max(res["ms"])
     value = world * nt * args.steps / (ms_max / 1e3)
 
     # ---- e2e through host memory, on the same context ----
     e2e = None
     if not args.no_e2e:
-        r = run_e2e(fp, cfg, nt, w, bgs, shocks, snaps, args.e2e_steps)
-        e2e_s = statistics.median(r["times"])
-        if dist:
-            t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        # every rank pins ~44 GB of host buffers; the ranks agree on success
+        # before the timing reduction, so that one rank's failure cannot
+        # leave the others waiting in a collective
+        try:
+            r, e2e_err = run_e2e(fp, cfg, nt, w, bgs, shocks, snaps, args.e2e_steps), None
+        except (MemoryError, RuntimeError) as ex:
+            r, e2e_err = None, f"{type(ex).__name__}: {ex}"
+        failed = rank_max(1.0 if r is None else 0.0)
+        if failed:
+            e2e = {"value": None, "unit": UNIT, "error": e2e_err or "failed on another rank"}
+    if not args.no_e2e and e2e is None:
+        e2e_s = rank_max(statistics.median(r["times"]))
         e2e = {"value": world * nt / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(r["h2d"]),
                "d2h_bytes_per_step": int(r["d2h"]), "host_buffers": "page-locked (croma_b200_host_alloc)",
                "api": "croma_b200_step_host: backgrounds and shock fields up, emissivities and evolved spectra "
@@ -678,6 +688,7 @@ def run_gpu_arm(args):
     if not args.no_plain:
         pr = run_resident("plain", cfg, nt, w, bg_dev, sh_dev, snaps, args.plain_warmup, args.plain_steps,
                           emission=not args.no_emission, kernel_timing=True)
+        pr["ms"] = rank_max(pr["ms"])
         pv = world * nt * args.plain_steps / (pr["ms"] / 1e3)
         peaks, peak_kind = measured_peaks()
         plain = {"value": pv, "ms_per_step": pr["ms"] / args.plain_steps, "steps": args.plain_steps,
@@ -688,6 +699,7 @@ def run_gpu_arm(args):
     if not args.no_fp32r:
         fr = run_resident("fp32r", cfg, nt, w, bg_dev, sh_dev, snaps, 1, args.fp32r_steps,
                           emission=not args.no_emission, kernel_timing=True)
+        fr["ms"] = rank_max(fr["ms"])
         fv = world * nt * args.fp32r_steps / (fr["ms"] / 1e3)
         fp32r = {"value": fv, "ms_per_step": fr["ms"] / args.fp32r_steps, "steps": args.fp32r_steps, "warmup": 1,
                  "over_fused_fp64": fv / value, "over_plain": (fv / plain["value"]) if plain else None,
