@@ -22,7 +22,7 @@ LIBDIR = os.path.join(HERE, "lib")
 OBJROOT = os.path.join(HERE, "_build")
 NBS = (128, 256, 512)
 SOURCES = ("api.cu", "tables.cu", "schedule.cu", "fused.cu", "dsa.cu", "serve.cu",
-           "ref_abi.cu", "noalloc.cu", "output.cu", "emission.cu")
+           "ref_abi.cu", "noalloc.cu", "output.cu", "emission.cu", "h5lite.cpp", "background.cu")
 NO_FMAD = {"schedule.cu"}
 
 
@@ -52,7 +52,7 @@ def _newer(target: str, deps) -> bool:
 def _compile(nb: int, src: str, verbose: bool):
     objdir = os.path.join(OBJROOT, f"np{nb}")
     os.makedirs(objdir, exist_ok=True)
-    obj = os.path.join(objdir, src.replace(".cu", ".o"))
+    obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
     deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".cuh")]
     deps.append(os.path.join(os.path.dirname(HERE), "include", "croma_b200.h"))
     if _newer(obj, deps):

@@ -86,6 +86,18 @@ def config4(**kw) -> RunConfig:
     return RunConfig(**base)
 
 
+def tracer_10k(**kw) -> RunConfig:
+    """The reference's run of its real tracer histories (params_tracer_10k.txt
+    in kosukenishiwaki/croma-fp): electron_only seeds, p_p in [1e-1, 1e8],
+    p_e in [10^-0.5, 1e6], ASA reacceleration in a centred window, eta cap
+    0.1, sub-step safety 0.5."""
+    base = dict(nb=128, species="electron_only", pmin=-1.0, pmax=8.0, pemin=-0.5, pemax=6.0,
+                dpp_mode="asa", reacc_window_mode=1, eta_dpp_cap=0.1, nsub_safety=0.5, mach_limit=0.5, psi=0.5,
+                nsub_max=0)
+    base.update(kw)
+    return RunConfig(**base)
+
+
 DSA_MODELS = ("KR07", "KR07r", "KR13", "KR13r", "CS14", "CS14r", "Ryu19", "Ryu19r")
 DSA_MODE = {"off": 0, "tracer_state": 1, "tracer_source": 2}
 DSA_REACC = {"off": 0, "positive_delta": 1, "drury83": 2}

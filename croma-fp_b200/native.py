@@ -36,6 +36,18 @@ class CromaB200Snapshot(C.Structure):
                 ("z_next", _d), ("allow_interp", _i), ("dt_snap", _d), ("elapsed_gyr", _d)]
 
 
+class CromaB200RawSnapshot(C.Structure):
+    _fields_ = [("temp_K", _vp), ("density", _vp), ("bx", _vp), ("by", _vp), ("bz", _vp), ("div_v", _vp),
+                ("curl_v_prev", _vp), ("curl_v", _vp), ("curl_v_next", _vp), ("l_turb_cm", _vp),
+                ("c_dens", _d), ("c_mag", _d), ("z_prev", _d), ("z_curr", _d), ("z_next", _d),
+                ("apply_temp_floor", _i), ("allow_curl_interp", _i)]
+
+
+class CromaB200BackgroundParams(C.Structure):
+    _fields_ = [("bfield_mode", _i), ("mu_mol", _d), ("eta_B", _d), ("mach_limit", _d),
+                ("l_turb_target_kpc", _d)]
+
+
 _LIBS: dict = {}
 
 
@@ -76,6 +88,11 @@ def load_library(nb: int) -> C.CDLL:
     L.croma_b200_fp64_peak.argtypes = [P(_d)]
     L.croma_b200_rcp_check.argtypes = [C.c_longlong, _vp, _vp]
     L.croma_b200_exp_check.argtypes = [C.c_longlong, _vp, _vp]
+    L.croma_b200_h5_shape.argtypes = [C.c_char_p, C.c_char_p, P(_i), P(C.c_longlong), _i, P(_i), P(_i)]
+    L.croma_b200_h5_read_f64.argtypes = [C.c_char_p, C.c_char_p, C.c_longlong, C.c_longlong, _vp]
+    L.croma_b200_h5_read_i64.argtypes = [C.c_char_p, C.c_char_p, C.c_longlong, C.c_longlong, _vp]
+    L.croma_b200_background_prepare.argtypes = [_vp, _i, P(CromaB200RawSnapshot), P(CromaB200BackgroundParams),
+                                                _i, _vp]
     L.croma_b200_get_sources.argtypes = [_vp, _vp, _vp, _vp]
     L.croma_b200_set_state_broadcast.argtypes = [_vp, _i, _vp, _vp, _d]
     L.croma_b200_set_dsa.argtypes = [_vp, P(CromaB200DsaParams)]
@@ -157,6 +174,73 @@ def fp64_peak(nb: int = 256) -> float:
     if L.croma_b200_fp64_peak(C.byref(t)) != 0:
         raise CromaError(L.croma_b200_last_error().decode())
     return t.value
+
+
+def h5_shape(path: str, dataset: str, nb: int = 256):
+    """(dims tuple, 'float' | 'int', element bytes) of an HDF5 dataset."""
+    L = load_library(nb)
+    rank, cls, size = _i(), _i(), _i()
+    dims = (C.c_longlong * 32)()
+    if L.croma_b200_h5_shape(path.encode(), dataset.encode(), C.byref(rank), dims, 32, C.byref(cls),
+                             C.byref(size)) != 0:
+        raise CromaError(L.croma_b200_last_error().decode())
+    return tuple(dims[i] for i in range(rank.value)), ("float" if cls.value == 1 else "int"), size.value
+
+
+def h5_read(path: str, dataset: str, offset: int = 0, count=None, integer: bool = False, nb: int = 256):
+    """Elements [offset, offset + count) of an HDF5 dataset as float64 (or
+    int64 for integer=True); count None reads to the end."""
+    L = load_library(nb)
+    dims, _, _ = h5_shape(path, dataset, nb)
+    n = int(np.prod(dims)) if dims else 1
+    if count is None:
+        count = n - offset
+    out = np.empty(count, np.int64 if integer else np.float64)
+    fn = L.croma_b200_h5_read_i64 if integer else L.croma_b200_h5_read_f64
+    if fn(path.encode(), dataset.encode(), int(offset), int(count), _p(out)) != 0:
+        raise CromaError(L.croma_b200_last_error().decode())
+    return out
+
+
+def background_prepare(raw: dict, params: dict, ctx=None, nb: int = 256, on_device: bool = False, out=None):
+    """croma_b200_background_prepare: the [8][ntracer] background block from
+    one snapshot's raw fields.  raw maps the CromaB200RawSnapshot fields to
+    arrays (host, or device addresses with on_device) and scalars; params the
+    CromaB200BackgroundParams fields.  Returns the host block (or None when
+    out is a device address)."""
+    L = load_library(nb)
+    r = CromaB200RawSnapshot()
+    keep = []
+    n = None
+    for name, typ in CromaB200RawSnapshot._fields_:
+        v = raw.get(name)
+        if typ is _vp:
+            if v is None:
+                setattr(r, name, None)
+            elif on_device:
+                setattr(r, name, int(v))
+            else:
+                a = _c(v)
+                keep.append(a)
+                n = a.shape[0] if n is None else n
+                if a.shape != (n,):
+                    raise ValueError(f"raw field {name} must be [ntracer]")
+                setattr(r, name, a.ctypes.data)
+        else:
+            setattr(r, name, v if v is not None else 0)
+    if on_device:
+        n = int(raw["ntracer"])
+    prm = CromaB200BackgroundParams(**params)
+    if out is None:
+        if on_device:
+            raise ValueError("on_device needs an output address")
+        out = np.empty((8, n))
+    dst = out if on_device else out.ctypes.data
+    h = ctx.h if ctx is not None else None
+    rc = L.croma_b200_background_prepare(h, n, C.byref(r), C.byref(prm), int(bool(on_device)), dst)
+    if rc != 0:
+        raise CromaError(L.croma_b200_last_error().decode())
+    return None if on_device else out
 
 
 def _math_check(fn: str, x, nb: int):

@@ -351,6 +351,60 @@ int croma_b200_get_tuning(CromaB200Context *ctx, int species, int *tuned, int *s
 int croma_b200_host_alloc(size_t bytes, void **out);
 int croma_b200_host_free(void *p);
 
+/* ---- tracer snapshots from HDF5 and their backgrounds ---------------- */
+
+/* Reader of the HDF5 tracer snapshots CROMA takes as input (the reference
+ * reads them with libhdf5: tracer_load_hdf5_raw_snapshot_slice,
+ * src/tracer_fp_background.c:1003-1204).  It reads the format subset those
+ * files use -- superblock 0/1, symbol-table groups, version-1 object
+ * headers, compact or contiguous datasets of fixed-point or IEEE
+ * floating-point elements -- and refuses the rest with an error naming it.
+ * dataset may be a '/'-separated path.  h5_shape: rank, up to max_rank
+ * dimensions, datatype class (0 fixed-point, 1 floating-point) and element
+ * size.  h5_read_f64 / _i64: elements [offset, offset + count) of the
+ * dataset in storage order, converted to double / int64 (_i64 only for
+ * fixed-point datasets). */
+int croma_b200_h5_shape(const char *path, const char *dataset, int *rank, long long *dims, int max_rank,
+                        int *type_class, int *type_size);
+int croma_b200_h5_read_f64(const char *path, const char *dataset, long long offset, long long count, double *out);
+int croma_b200_h5_read_i64(const char *path, const char *dataset, long long offset, long long count,
+                           long long *out);
+
+/* The raw fields of one tracer snapshot, as the snapshot files hold them:
+ * temperature [K], density [code units], B_x/y/z [code units], div_v and
+ * curl_v [s^-1] (curl_v also of the previous and next snapshots when
+ * allow_curl_interp), dx_phys [cm] (NULL or <= 0: the target scale), and the
+ * snapshot's unit factors c_dens = dUnit and c_mag = sqrt(4 pi dUnit) vUnit
+ * (src/tracer_fp_background.c:955-957, 1189-1197). */
+typedef struct {
+    const double *temp_K, *density, *bx, *by, *bz, *div_v;
+    const double *curl_v_prev, *curl_v, *curl_v_next;
+    const double *l_turb_cm;
+    double c_dens, c_mag;
+    double z_prev, z_curr, z_next;
+    int apply_temp_floor;    /* T < 1e4 K -> 1e4 K */
+    int allow_curl_interp;   /* curl_v == 0 -> interpolated in z from prev / next */
+} CromaB200RawSnapshot;
+
+/* The run parameters the background reads (src/params.c): bfield_mode
+ * 0 max(dynamo, simulation), 1 simulation, 2 dynamo; mu_mol 0.59; eta_B
+ * 0.05; mach_limit 0.5; L_turb_target_kpc 150 are the reference's defaults. */
+typedef struct {
+    int bfield_mode;
+    double mu_mol, eta_B, mach_limit, l_turb_target_kpc;
+} CromaB200BackgroundParams;
+
+/* The background block [8][ntracer] (n_gas, kT GeV, B_eff, div v Gyr^-1,
+ * L_turb Mpc, dv_imc, c_s, beta_pl) that croma_b200_snapshot reads, from one
+ * snapshot's raw fields: prepare_background_cell (src/fp_shared_core.c:866-932)
+ * per tracer, as tracer_prepare_background_from_raw (src/tracer_fp_background.c:
+ * 1206-1263) applies it, one device thread per tracer.  on_device: raw arrays
+ * and bg are device pointers (else host).  ctx (may be NULL) supplies the
+ * stream.  Returns 0, -1 on invalid arguments or a CUDA error, -2 when a
+ * tracer has density <= 0 (the reference aborts; its fields are set to 0). */
+int croma_b200_background_prepare(CromaB200Context *ctx, int ntracer, const CromaB200RawSnapshot *raw,
+                                  const CromaB200BackgroundParams *prm, int on_device, double *bg);
+
 /* FP64 FMA throughput of the current device, measured by a kernel of
  * independent fused multiply-add chains on every SM (TFLOP/s, FMA = 2 flops);
  * the denominator of the fused evolve's roofline. */

@@ -139,6 +139,14 @@ int or_dsa_inject(const OrDsaParams *prm, int nb, const double *p_p, const doubl
                   int reacc_mode, double *crp, double *cre, double *qpi, double *qepri,
                   unsigned char *dis, int *ninjected);
 
+/* ---- background preparation (croma_oracle_background.c) ---- */
+/* bg[8][n] from one snapshot's raw fields; -2 if a tracer has density <= 0. */
+int or_background(int n, const double *temp_K, const double *density, const double *bx, const double *by,
+                  const double *bz, const double *div_v, const double *curl_prev, const double *curl,
+                  const double *curl_next, const double *l_turb_cm, double c_dens, double c_mag, double z_prev,
+                  double z_curr, double z_next, int apply_temp_floor, int allow_curl_interp, int bfield_mode,
+                  double mu_mol, double eta_B, double mach_limit, double l_turb_target_kpc, double *bg);
+
 #ifdef __cplusplus
 }
 #endif

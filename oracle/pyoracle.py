@@ -323,6 +323,74 @@ def synch_emission_theta(cre, dp, b_dyn, logb, logy, w, xmin, logx_tab, logfx_ta
     return out
 
 
+_BG_ARGS = ("temp_K", "density", "bx", "by", "bz", "div_v", "curl_v_prev", "curl_v", "curl_v_next", "l_turb_cm")
+
+
+def background(raw: dict, params: dict) -> np.ndarray:
+    """or_background (oracle/croma_oracle_background.c): the [8][n]
+    background block from one snapshot's raw fields (the keys of
+    CromaB200RawSnapshot) and the run parameters (CromaB200BackgroundParams)."""
+    L = C.CDLL(os.path.join(HERE, "_build", "liboracle.so"))
+    arrs = [None if raw.get(k) is None else np.ascontiguousarray(raw[k], dtype=np.float64) for k in _BG_ARGS]
+    n = arrs[0].shape[0]
+    bg = np.empty((8, n))
+    L.or_background.restype = _i
+    L.or_background.argtypes = [_i] + [_vp] * 10 + [_d] * 5 + [_i, _i, _i] + [_d] * 4 + [_vp]
+    rc = L.or_background(n, *[None if a is None else a.ctypes.data for a in arrs], raw["c_dens"], raw["c_mag"],
+                         raw["z_prev"], raw["z_curr"], raw["z_next"], int(raw["apply_temp_floor"]),
+                         int(raw["allow_curl_interp"]), int(params["bfield_mode"]), params["mu_mol"],
+                         params["eta_B"], params["mach_limit"], params["l_turb_target_kpc"], bg.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"or_background returned {rc}")
+    return bg
+
+
+class _BgCellIn(C.Structure):   # FpBackgroundCellInput, include/fp_shared_core.h:207-224
+    _fields_ = [(k, _d) for k in ("density_gcc", "temp_K", "bx_G", "by_G", "bz_G", "divv_gyr", "curl_v_s",
+                                 "curl_v_prev_s", "curl_v_next_s", "z_prev", "z_curr", "z_next", "l_turb_cm",
+                                 "target_l_turb_cm")] + [("apply_temp_floor", _i), ("allow_curl_interp", _i)]
+
+
+class _BgCellOut(C.Structure):   # FpBackgroundCellOutput, include/fp_shared_core.h:226-239
+    _fields_ = [(k, _d) for k in ("n_gas", "kbt_GeV", "b_sim_G", "b_dyn_G", "b_eff_G", "divv_gyr", "l_turb_mpc",
+                                 "dv_imc_cms", "cs_cms", "beta_pl", "curl_v_used_s", "temp_used_K")]
+
+
+def reference_background(raw: dict, params: dict, nb: int = 128) -> np.ndarray:
+    """The reference's own prepare_background_cell (compiled in
+    oracle/_ref) per tracer, with the raw scaling and the argument forms of
+    tracer_load_hdf5_raw_snapshot_slice and tracer_prepare_background_from_raw
+    (src/tracer_fp_background.c:1189-1197, 1206-1263) and the stored fields of
+    tracer_store_background_history_slot (:324-342)."""
+    L = C.CDLL(os.path.join(HERE, "_ref", f"libcroma_ref_np{nb}.so"))
+    _i.in_dll(L, "bfield_mode").value = int(params["bfield_mode"])
+    _d.in_dll(L, "mu_mol").value = params["mu_mol"]
+    _d.in_dll(L, "eta_B").value = params["eta_B"]
+    _d.in_dll(L, "mach_limit").value = params["mach_limit"]
+    L.prepare_background_cell.restype = _i
+    L.prepare_background_cell.argtypes = [C.POINTER(_BgCellIn), C.POINTER(_BgCellOut)]
+    n = len(raw["temp_K"])
+    target = params["l_turb_target_kpc"] * 3.0857e21
+    bg = np.empty((8, n))
+    prev = raw.get("curl_v_prev")
+    nxt = raw.get("curl_v_next")
+    lt = raw.get("l_turb_cm")
+    for i in range(n):
+        a = _BgCellIn(density_gcc=raw["density"][i] * raw["c_dens"], temp_K=raw["temp_K"][i],
+                      bx_G=raw["bx"][i] * raw["c_mag"], by_G=raw["by"][i] * raw["c_mag"],
+                      bz_G=raw["bz"][i] * raw["c_mag"], divv_gyr=1.0 * raw["div_v"][i] * 3.1536e16,
+                      curl_v_s=1.0 * raw["curl_v"][i], curl_v_prev_s=1.0 * (prev[i] if prev is not None else 0.0),
+                      curl_v_next_s=1.0 * (nxt[i] if nxt is not None else 0.0), z_prev=raw["z_prev"],
+                      z_curr=raw["z_curr"], z_next=raw["z_next"], l_turb_cm=(lt[i] if lt is not None else 0.0),
+                      target_l_turb_cm=target, apply_temp_floor=int(raw["apply_temp_floor"]),
+                      allow_curl_interp=int(raw["allow_curl_interp"]))
+        o = _BgCellOut()
+        if L.prepare_background_cell(C.byref(a), C.byref(o)) != 0:
+            raise RuntimeError(f"prepare_background_cell failed at tracer {i}")
+        bg[:, i] = (o.n_gas, o.kbt_GeV, o.b_eff_G, o.divv_gyr, o.l_turb_mpc, o.dv_imc_cms, o.cs_cms, o.beta_pl)
+    return bg
+
+
 def reference_available(nb: int) -> bool:
     return os.path.exists(os.path.join(HERE, "_ref", f"libcroma_ref_np{nb}.so"))
 

@@ -5,7 +5,8 @@ its own CPU implementation -- compiled from its sources by
 `make -C oracle ref` into oracle/_ref/libcroma_ref_np<N>.so -- is run here on
 seeded synthetic tracers, and its outputs are stored with their inputs.
 
-Run from the repository root (needs the reference tree at build time):
+Run from the repository root (needs the reference tree at build time; its
+location is CROMA_REFERENCE_ROOT):
 
     make -C oracle ref && python tests/golden/make_golden.py
 
@@ -259,10 +260,41 @@ def make_emission_tables(name="emission_tables"):
     print(name, "written")
 
 
+HISTORY_SNAPS = (0, 1, 2, 3, 97, 98, 99)   # of the 100-file series: its start and its end
+
+
+def make_histories(name="histories"):
+    """Real tracer histories: the reference's tracer_10k snapshot series
+    (dump0025 .. dump0124) read by the library's HDF5 reader, every 39th of
+    the 10,000 tracers (256), snapshots HISTORY_SNAPS of the series.  Stored:
+    the raw fields each snapshot's background reads (with the previous and
+    next snapshots' curl_v), the unit factors, redshifts and run-loop flags,
+    the timeline (z, z_next, dt), the masses, and the reference's own
+    prepare_background_cell outputs (oracle/_ref) for the default run
+    parameters."""
+    from croma_fp_b200 import histories
+    refroot = os.environ.get("CROMA_REFERENCE_ROOT", "/root/reference")
+    S = histories.SnapshotSeries(os.path.join(refroot, "tracer_10k"))
+    idx = np.arange(0, S.ntracer, 39)[:256]
+    out = {"tracers": idx, "mass": S.mass()[idx], "z": S.z, "z_next": S.z_next, "dt": S.dt,
+           "snaps": np.array(HISTORY_SNAPS), "params": json.dumps(histories.DEFAULT_BACKGROUND)}
+    for i in HISTORY_SNAPS:
+        raw = S.raw_snapshot(i)
+        sel = {k: (np.ascontiguousarray(v[idx]) if isinstance(v, np.ndarray) else v) for k, v in raw.items()}
+        for k, v in sel.items():
+            out[f"s{i}_{k}"] = np.asarray(v)
+        out[f"s{i}_bg_ref"] = pyoracle.reference_background(sel, histories.DEFAULT_BACKGROUND)
+    np.savez_compressed(os.path.join(HERE, f"golden_{name}.npz"), **out)
+    print(name, "written")
+
+
 if __name__ == "__main__":
-    names = sys.argv[1:] or list(CASES) + list(DSA_CASES) + ["emission_ic", "emission_synch", "emission_tables"]
+    names = sys.argv[1:] or list(CASES) + list(DSA_CASES) + ["emission_ic", "emission_synch", "emission_tables",
+                                                              "histories"]
     for n in names:
-        if n in DSA_CASES:
+        if n == "histories":
+            make_histories(n)
+        elif n in DSA_CASES:
             make_dsa_case(n, DSA_CASES[n])
         elif n == "emission_ic":
             make_ic_emission(n)

@@ -1,0 +1,110 @@
+"""Real tracer histories on the GPU: the device background
+(croma_b200_background_prepare) of the committed tracer_10k fixture
+(tests/golden/golden_histories.npz: the reference's own
+prepare_background_cell outputs) and three snapshots of those tracers
+evolved with it, against the oracle evolving the same tracers on the
+reference's backgrounds.
+
+The device background repeats the reference's operations in its order
+without contraction; only pow(L_target / L, 0.3333) comes from CUDA's libm,
+so the fields that do not depend on it (n_gas, kT, div v, L_turb, c_s) are
+bit-identical and the rest agree to a few ulp."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_package
+from golden_io import GOLDEN_DIR, rel_err
+
+load_package()
+from croma_fp_b200 import config, native, synth  # noqa: E402
+
+import sys  # noqa: E402
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import pyoracle  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+FIX = np.load(os.path.join(GOLDEN_DIR, "golden_histories.npz"))
+PRM = json.loads(str(FIX["params"]))
+KEYS = ("temp_K", "density", "bx", "by", "bz", "div_v", "curl_v_prev", "curl_v", "curl_v_next", "l_turb_cm",
+        "c_dens", "c_mag", "z_prev", "z_curr", "z_next", "apply_temp_floor", "allow_curl_interp")
+
+
+def raw(i, sel=slice(None)):
+    r = {}
+    for k in KEYS:
+        v = FIX[f"s{i}_{k}"]
+        if v.ndim:
+            r[k] = np.ascontiguousarray(v[sel])
+        else:
+            r[k] = int(v) if k in ("apply_temp_floor", "allow_curl_interp") else float(v)
+    return r
+
+
+def test_device_background_matches_reference():
+    for i in FIX["snaps"]:
+        i = int(i)
+        got = native.background_prepare(raw(i), PRM)
+        ref = FIX[f"s{i}_bg_ref"]
+        for f in (0, 1, 3, 4, 6):
+            assert np.array_equal(got[f], ref[f]), (i, f)
+        assert float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300))) <= 1e-14, i
+
+
+def test_device_pointers_equal_host_call():
+    torch = pytest.importorskip("torch")
+    r = raw(2)
+    host = native.background_prepare(r, PRM)
+    dev = {k: (torch.from_numpy(v).cuda() if isinstance(v, np.ndarray) else v) for k, v in r.items()}
+    out = torch.empty((8, host.shape[1]), dtype=torch.float64, device="cuda")
+    addr = {k: (v.data_ptr() if hasattr(v, "data_ptr") else v) for k, v in dev.items()}
+    addr["ntracer"] = host.shape[1]
+    native.background_prepare(addr, PRM, on_device=True, out=out.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), host)
+
+
+def test_nonpositive_density_is_reported():
+    r = raw(1, slice(0, 16))
+    r["density"] = r["density"].copy()
+    r["density"][3] = 0.0
+    with pytest.raises(native.CromaError, match="density <= 0"):
+        native.background_prepare(r, PRM)
+
+
+@pytest.mark.parametrize("path", ["fused", "plain"])
+def test_real_histories_evolve_like_the_oracle(path):
+    """64 tracers of the real series, electron_only as the reference's
+    tracer_10k run configures them (config.tracer_10k), three snapshots from
+    the start of the series: the GPU on its own device backgrounds, the
+    oracle on the reference's."""
+    cfg = config.tracer_10k(nb=128)
+    n = 64
+    sel = slice(0, n)
+    mass = np.ascontiguousarray(FIX["mass"][sel])
+    fp = native.TracerFP(cfg, path=path)
+    o = pyoracle.Oracle(cfg)
+    try:
+        gp, ge = fp.grid(0), fp.grid(1)
+        crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), n, cfg.species)
+        fp.set_state(crp, cre, mass=mass)
+        o_crp, o_cre = crp.copy(), cre.copy()
+        q = np.zeros_like(crp)
+        dev_bg = [native.background_prepare(raw(k, sel), PRM) for k in range(4)]
+        ref_bg = [np.ascontiguousarray(FIX[f"s{k}_bg_ref"][:, sel]) for k in range(4)]
+        z, dt = FIX["z"], FIX["dt"]
+        elapsed = 0.0
+        for k in range(3):
+            fp.snapshot(dev_bg[k], dev_bg[k + 1], float(z[k]), float(z[k + 1]), True, float(dt[k]), elapsed,
+                        sync=True)
+            o.snapshot(ref_bg[k], ref_bg[k + 1], float(z[k]), float(z[k + 1]), True, float(dt[k]), elapsed,
+                       q, q, o_crp, o_cre, mass=mass)
+            elapsed += float(dt[k])
+            g_crp, g_cre = fp.get_state()
+            assert rel_err(g_cre, o_cre) <= 1e-10, k
+            assert np.any(g_cre != cre)
+    finally:
+        fp.close()

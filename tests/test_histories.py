@@ -1,0 +1,146 @@
+"""Real tracer histories (HDF5 input), on the CPU.
+
+* The library's HDF5 reader (croma_b200_h5_*) on the reference's own
+  tracer_10k snapshot series, where the reference tree is present
+  (CROMA_REFERENCE_ROOT): every file opens, every field the background reads
+  has one element per tracer, the tracer ids agree across the series, the
+  redshifts fall by 0.01 per file from 1, the fields are finite and the
+  positive ones positive, a scalar reads as one element, and damaged or
+  foreign files are refused with an error instead of a crash.
+* The background restatement (oracle/croma_oracle_background.c) is pinned
+  bit for bit to the reference's own prepare_background_cell (oracle/_ref)
+  on those files, and to the committed fixture golden_histories.npz
+  (tests/golden/make_golden.py) everywhere.
+"""
+import json
+import os
+import shutil
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_package
+from golden_io import GOLDEN_DIR
+
+load_package()
+from croma_fp_b200 import config, histories, native  # noqa: E402
+
+import sys  # noqa: E402
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import pyoracle  # noqa: E402
+
+REF = os.environ.get("CROMA_REFERENCE_ROOT", "/root/reference")
+SERIES = os.path.join(REF, "tracer_10k")
+FIX = np.load(os.path.join(GOLDEN_DIR, "golden_histories.npz"))
+PRM = json.loads(str(FIX["params"]))
+have_series = pytest.mark.skipif(not os.path.isdir(SERIES), reason="reference tracer series not present")
+
+
+def fixture_raw(i):
+    keys = ("temp_K", "density", "bx", "by", "bz", "div_v", "curl_v_prev", "curl_v", "curl_v_next", "l_turb_cm",
+            "c_dens", "c_mag", "z_prev", "z_curr", "z_next", "apply_temp_floor", "allow_curl_interp")
+    raw = {k: FIX[f"s{i}_{k}"] for k in keys}
+    for k in ("c_dens", "c_mag", "z_prev", "z_curr", "z_next"):
+        raw[k] = float(raw[k])
+    for k in ("apply_temp_floor", "allow_curl_interp"):
+        raw[k] = int(raw[k])
+    return raw
+
+
+@have_series
+def test_reader_on_the_reference_snapshot_series():
+    S = histories.SnapshotSeries(SERIES)
+    assert len(S) == 100 and S.index[0] == 25 and S.ntracer == 10000
+    assert np.allclose(S.z, 1.0 - 0.01 * np.arange(100), atol=2e-5)
+    assert np.all(np.diff(S.z) < 0) and np.all(S.dt > 0) and np.all(S.c_dens > 0) and np.all(S.c_mag > 0)
+    ids0 = S.particle_ids(0)
+    assert len(np.unique(ids0)) == S.ntracer
+    for i in (0, 1, 50, 99):
+        assert np.array_equal(S.particle_ids(i), ids0)
+        raw = S.raw(i)
+        for k, v in raw.items():
+            assert v.shape == (S.ntracer,) and np.all(np.isfinite(v)), k
+        for k in ("temperature", "density", "dx_phys"):
+            assert np.all(raw[k] > 0), k
+    f = S.files[0]
+    assert native.h5_shape(f, "Redshift") == ((), "float", 8)
+    assert native.h5_shape(f, "particle_ID") == ((10000,), "int", 8)
+    # a slice equals the same elements of the whole dataset
+    whole = native.h5_read(f, "density")
+    assert np.array_equal(native.h5_read(f, "density", 1234, 777), whole[1234:1234 + 777])
+    m = S.mass()
+    assert np.all((m >= 1e7) & (m <= 1e9))
+
+
+@have_series
+def test_reader_refuses_damaged_and_foreign_files(tmp_path):
+    src = histories.SnapshotSeries(SERIES, first=25, last=26).files[0]
+    with pytest.raises(native.CromaError, match="no dataset or group"):
+        native.h5_read(src, "no_such_field")
+    with pytest.raises(native.CromaError):
+        native.h5_read(src, "density", 9990, 20)   # past the end
+    with pytest.raises(native.CromaError, match="not an integer dataset"):
+        native.h5_read(src, "density", integer=True)
+    data = open(src, "rb").read()
+    for cut in (16, 700, 6000, len(data) // 2):   # truncated copies: headers or data cut off
+        p = tmp_path / f"cut{cut}.h5"
+        p.write_bytes(data[:cut])
+        with pytest.raises(native.CromaError):
+            native.h5_read(str(p), "z_coordinate")
+    p = tmp_path / "foreign.h5"
+    p.write_bytes(b"not an HDF5 file" * 100)
+    with pytest.raises(native.CromaError, match="not an HDF5 file"):
+        native.h5_shape(str(p), "density")
+    # a corrupted B-tree signature
+    bad = bytearray(data)
+    pos = bad.find(b"TREE")
+    bad[pos:pos + 4] = b"XXXX"
+    p = tmp_path / "badtree.h5"
+    p.write_bytes(bytes(bad))
+    with pytest.raises(native.CromaError, match="B-tree"):
+        native.h5_read(str(p), "density")
+    shutil.rmtree(tmp_path, ignore_errors=True)
+
+
+@have_series
+@pytest.mark.skipif(not pyoracle.reference_available(128), reason="oracle/_ref not built")
+def test_background_restatement_matches_reference_on_the_series():
+    S = histories.SnapshotSeries(SERIES, first=25, last=125, ntracer=3000)
+    for i in (0, 1, 57, 99):   # first snapshot (no floor, no interpolation), middle, last (no next)
+        raw = S.raw_snapshot(i)
+        for prm in (PRM, dict(PRM, bfield_mode=1), dict(PRM, bfield_mode=2, mach_limit=0.0)):
+            assert np.array_equal(pyoracle.background(raw, prm), pyoracle.reference_background(raw, prm)), (i, prm)
+
+
+def test_background_restatement_matches_fixture():
+    for i in FIX["snaps"]:
+        assert np.array_equal(pyoracle.background(fixture_raw(int(i)), PRM), FIX[f"s{int(i)}_bg_ref"]), i
+
+
+def test_background_curl_interpolation_and_floor():
+    """A zero curl_v is interpolated in z between the neighbours when allowed,
+    and the temperature floor lifts T below 1e4 K (prepare_background_cell,
+    src/fp_shared_core.c:883-892)."""
+    raw = fixture_raw(1)
+    raw = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in raw.items()}
+    raw["curl_v"][:8] = 0.0
+    raw["temp_K"][8:16] = 5.0e3
+    bg = pyoracle.background(raw, PRM)
+    off = pyoracle.background(dict(raw, allow_curl_interp=0, apply_temp_floor=0), PRM)
+    assert np.all(bg[5, :8] != off[5, :8])                       # dv from the interpolated curl
+    assert np.allclose(bg[1, 8:16], 8.62e-5 * 1.0e4 * 1.0e-9, rtol=1e-15)
+    assert np.allclose(off[1, 8:16], 8.62e-5 * 5.0e3 * 1.0e-9, rtol=1e-15)
+
+
+def test_timeline_restates_the_reference_cosmology():
+    """dt of a snapshot = dz / H(z) / (1 + z) in Gyr (src/COSFUNC.c:64-67):
+    the step between z = 1 and 0.99 is about 41 Myr and within 1 % of the
+    exact cosmic-time integral over the step."""
+    z0, z1 = 1.0, 0.99
+    dt = histories.dz_to_dt(z0 - z1, z0)
+    zs = np.linspace(z1, z0, 20001)
+    f = 1.0 / ((1.0 + zs) * np.array([histories.hubble(z) for z in zs]))
+    exact = np.trapezoid(f, zs) / histories.GYR * histories.MPC * 1.0e-5
+    assert 0.035 < dt < 0.045 and abs(dt / exact - 1.0) < 0.01
+    cfg = config.tracer_10k()
+    assert cfg.species == "electron_only" and cfg.reacc_window_mode == 1 and cfg.eta_dpp_cap == 0.1
