@@ -721,7 +721,8 @@ def run_gpu_arm(args):
                    "sample": f"{type(e).__name__}: {e}"}
     secondary = None
     if rank == 0 and world == 1 and not args.no_secondary:
-        secondary = {"config1": run_config1(args), "heavy_tail": run_heavy_tail(args)}
+        secondary = {"config1": run_config1(args), "heavy_tail": run_heavy_tail(args),
+                     "real_histories": run_real_histories(args)}
     serving = None
     if rank == 0 and world == 1 and args.serving_requests > 0:
         serving = run_serving(args)
@@ -794,6 +795,61 @@ def run_serving(args):
     for path in args.serving_paths.split(","):
         out[path] = serve_bench.run(nrequests=args.serving_requests, path=path)
     return out
+
+
+def run_real_histories(args):
+    """Real tracer histories: the 256 tracers of the reference's tracer_10k
+    series in tests/golden/golden_histories.npz (raw snapshot fields read by
+    the library's HDF5 reader when the fixture was made), tiled to 65,536
+    tracers, backgrounds derived on the device from the raw fields
+    (croma_b200_background_prepare), three snapshots from the start of the
+    series with the reference's tracer_10k run settings (electron_only, ASA in
+    a centred window, eta cap 0.1, no sub-step cap), on-chip FP64 path."""
+    import torch
+    from croma_fp_b200 import config, native, synth
+    fix = np.load(os.path.join(ROOT, "tests", "golden", "golden_histories.npz"))
+    prm = json.loads(str(fix["params"]))
+    cfg = config.tracer_10k(nb=128)
+    reps = 256
+    keys = ("temp_K", "density", "bx", "by", "bz", "div_v", "curl_v_prev", "curl_v", "curl_v_next", "l_turb_cm",
+            "c_dens", "c_mag", "z_prev", "z_curr", "z_next", "apply_temp_floor", "allow_curl_interp")
+    bgs = []
+    for k in range(4):
+        raw = {}
+        for key in keys:
+            v = fix[f"s{k}_{key}"]
+            raw[key] = np.tile(v, reps) if v.ndim else (int(v) if key.startswith(("apply", "allow")) else float(v))
+        bgs.append(native.background_prepare(raw, prm, nb=cfg.nb))
+    nt = bgs[0].shape[1]
+    mass = np.tile(fix["mass"], reps)
+    z, dt = fix["z"], fix["dt"]
+    fp = native.TracerFP(cfg, path="fused")
+    try:
+        gp, ge = fp.grid(0), fp.grid(1)
+        crp1, cre1 = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), 1, cfg.species)
+        fp.set_state(np.repeat(crp1, nt, axis=0), np.repeat(cre1, nt, axis=0), mass=mass)
+        bg_dev = [torch.from_numpy(b).cuda() for b in bgs]
+        stream = torch.cuda.ExternalStream(fp.stream())
+        fp.snapshot(bg_dev[0].data_ptr(), bg_dev[1].data_ptr(), float(z[0]), float(z[1]), True, float(dt[0]),
+                    0.0, sync=True)   # warm-up: snapshot 0 -> 1 (and the tuner)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        elapsed = float(dt[0])
+        e0.record(stream)
+        for k in (1, 2):
+            fp.snapshot(bg_dev[k].data_ptr(), bg_dev[k + 1].data_ptr(), float(z[k]), float(z[k + 1]), True,
+                        float(dt[k]), elapsed, sync=False)
+            elapsed += float(dt[k])
+        e1.record(stream)
+        e1.synchronize()
+        fp.sync()
+        ms = e0.elapsed_time(e1)
+        nsub = fp.schedule()["nsub"]
+    finally:
+        fp.close()
+    return {"workload": f"{nt} tracers = the fixture's 256 tracer_10k tracers x {reps}, 128 bins, electron_only, "
+                        "ASA centred window, eta cap 0.1, snapshots 1 -> 3 of the series (dump0026-0028)",
+            "value": nt * 2 / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / 2,
+            "nsub_percentiles_0_10_50_90_100": [float(np.percentile(nsub, q)) for q in (0, 10, 50, 90, 100)]}
 
 
 def run_config1(args):
