@@ -1,0 +1,63 @@
+"""The HDF5 reader (croma_b200_h5_*) on files written by tests/h5write.py,
+an independent writer of the same format subset: every element type
+(float32/64, int16/32/64, uint16/32/64) in both byte orders, scalars and
+rank 2, compact and contiguous storage, object headers continued in a second
+block, nested groups, and groups large enough for their B-tree to split into
+several symbol table nodes and two levels.  Each dataset read back equals
+what was written; slices equal the whole dataset's elements; a missing path
+element, a non-integer dataset read as integers and a read past the end are
+refused."""
+import numpy as np
+import pytest
+
+from conftest import load_package
+import h5write
+
+load_package()
+from croma_fp_b200 import native  # noqa: E402
+
+
+def test_round_trip_of_types_layouts_and_groups(tmp_path):
+    rng = np.random.default_rng(5)
+    data = {
+        "f64": rng.normal(size=1000),
+        "f32_be": rng.normal(size=33).astype(">f4"),
+        "f64_be": rng.normal(size=17).astype(">f8"),
+        "i64": rng.integers(-2**62, 2**62, size=50, dtype=np.int64),
+        "i32_be": rng.integers(-2**31, 2**31, size=20, dtype=np.int64).astype(">i4"),
+        "i16": rng.integers(-2**15, 2**15, size=7, dtype=np.int64).astype("<i2"),
+        "u16": rng.integers(0, 2**16, size=9, dtype=np.int64).astype("<u2"),
+        "u32_be": rng.integers(0, 2**32, size=9, dtype=np.int64).astype(">u4"),
+        "u64": rng.integers(0, 2**62, size=9, dtype=np.int64).astype("<u8"),
+        "scalar": np.array(0.85),
+        "matrix": rng.normal(size=(6, 5)),
+        "small": np.arange(5, dtype=np.float64),
+        "group": {"inner": rng.normal(size=64), "deeper": {"leaf": np.arange(12, dtype=np.int64)}},
+    }
+    for k in range(40):   # forces several symbol table nodes and a two-level B-tree (leaf K = 4)
+        data[f"many_{k:02d}"] = np.full(3, float(k))
+    path = str(tmp_path / "t.h5")
+    h5write.write(path, data, leaf_k=4, compact={"small", "scalar"}, split={"f64", "group/inner", "matrix"})
+
+    def check(name, arr):
+        dims, cls, size = native.h5_shape(path, name)
+        assert dims == arr.shape and size == arr.dtype.itemsize, name
+        assert cls == ("float" if arr.dtype.kind == "f" else "int"), name
+        got = native.h5_read(path, name, integer=arr.dtype.kind in "iu")
+        assert np.array_equal(got, arr.reshape(-1).astype(got.dtype)), name
+
+    for name, arr in data.items():
+        if isinstance(arr, dict):
+            continue
+        check(name, arr)
+    check("group/inner", data["group"]["inner"])
+    check("/group/deeper/leaf", data["group"]["deeper"]["leaf"])
+    assert np.array_equal(native.h5_read(path, "f64", 100, 37), data["f64"][100:137])
+    with pytest.raises(native.CromaError, match="no dataset or group 'nope'"):
+        native.h5_read(path, "group/nope")
+    with pytest.raises(native.CromaError, match="not an integer dataset"):
+        native.h5_read(path, "f64", integer=True)
+    with pytest.raises(native.CromaError, match="past the dataset's end"):
+        native.h5_read(path, "i16", 5, 3, integer=True)
+    with pytest.raises(native.CromaError, match="not a dataset"):
+        native.h5_read(path, "group")
