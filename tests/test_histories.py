@@ -144,3 +144,39 @@ def test_timeline_restates_the_reference_cosmology():
     assert 0.035 < dt < 0.045 and abs(dt / exact - 1.0) < 0.01
     cfg = config.tracer_10k()
     assert cfg.species == "electron_only" and cfg.reacc_window_mode == 1 and cfg.eta_dpp_cap == 0.1
+
+
+@have_series
+@pytest.mark.skipif(not pyoracle.reference_available(128), reason="oracle/_ref not built")
+def test_oracle_evolves_real_histories_like_the_reference():
+    """Ten consecutive snapshots of 24 real tracers (every 400th of the
+    series) with the reference's tracer_10k settings: the oracle on its own
+    backgrounds and the reference's compiled code on the reference's
+    backgrounds agree bit for bit, nsub included."""
+    from croma_fp_b200 import synth
+    cfg = config.tracer_10k(nb=128)
+    S = histories.SnapshotSeries(SERIES, first=40, last=51)
+    idx = np.arange(0, S.ntracer, 400)
+    o, ref = pyoracle.Oracle(cfg), pyoracle.ReferenceCPU(cfg)
+    gp, ge = o.grid(0), o.grid(1)
+    crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), len(idx), cfg.species)
+    mass = np.ascontiguousarray(S.mass()[idx])
+    q = np.zeros_like(crp)
+    a = [crp.copy(), cre.copy()]
+    b = [crp.copy(), cre.copy()]
+    elapsed = 0.0
+
+    def bg(i, fn):
+        raw = S.raw_snapshot(i)
+        sel = {k: (np.ascontiguousarray(v[idx]) if isinstance(v, np.ndarray) else v) for k, v in raw.items()}
+        return fn(sel, PRM)
+
+    for i in range(1, 10):
+        args_o = (bg(i, pyoracle.background), bg(i + 1, pyoracle.background))
+        args_r = (bg(i, pyoracle.reference_background), bg(i + 1, pyoracle.reference_background))
+        common = (float(S.z[i]), float(S.z[i + 1]), True, float(S.dt[i]), elapsed)
+        n_o = o.snapshot(*args_o, *common, q, q, a[0], a[1], mass=mass)[0]
+        n_r = ref.snapshot(*args_r, *common, q, q, b[0], b[1], mass=mass)[0]
+        elapsed += float(S.dt[i])
+        assert np.array_equal(n_o, n_r) and np.array_equal(a[1], b[1]), i
+    assert np.any(a[1] != cre)
