@@ -1420,7 +1420,7 @@ __global__ void __launch_bounds__(WPB * 32,
 #pragma unroll 1
                 for (int istep = 0; istep < run_n; istep++) substep_sm<SRC, true>(F, coef_sm, lane, N);
             } else if (SOLVER == kSolveScan4) {
-#pragma unroll 1
+#pragma unroll 2   // two sub-steps per trip, as for substep (no spills at 254 registers)
                 for (int istep = 0; istep < run_n; istep++) substep4<SRC>(F, R4, lane, N);
             } else {
                 // two sub-steps per trip: the carried spectrum keeps its
