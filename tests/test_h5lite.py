@@ -61,3 +61,32 @@ def test_round_trip_of_types_layouts_and_groups(tmp_path):
         native.h5_read(path, "i16", 5, 3, integer=True)
     with pytest.raises(native.CromaError, match="not a dataset"):
         native.h5_read(path, "group")
+
+
+def test_corrupted_metadata_gives_errors_not_crashes(tmp_path):
+    """Single bytes of the metadata (superblock, object headers, B-tree, symbol
+    table nodes, local heap) replaced at random: every read either returns
+    the dataset's elements or raises CromaError -- the reader bounds every
+    offset, length, count and recursion depth it takes from the file."""
+    rng = np.random.default_rng(11)
+    data = {f"d{k}": rng.normal(size=64) for k in range(12)}
+    data["grp"] = {"x": np.arange(16, dtype=np.int64)}
+    path = str(tmp_path / "base.h5")
+    h5write.write(path, data, leaf_k=2, split={"d3"})
+    raw = open(path, "rb").read()
+    # metadata lies before the first dataset's elements and in the tail
+    meta = [i for i in range(len(raw)) if i < 96 or raw[i:i + 4] in (b"TREE", b"SNOD", b"HEAP")]
+    positions = sorted(set(rng.integers(0, len(raw), 400).tolist()) | set(meta))
+    ok = errors = 0
+    for n, pos in enumerate(positions[:600]):
+        bad = bytearray(raw)
+        bad[pos] = (bad[pos] + 1 + int(rng.integers(0, 255))) % 256
+        p = tmp_path / f"f{n % 8}.h5"
+        p.write_bytes(bytes(bad))
+        for name in ("d7", "grp/x"):
+            try:
+                native.h5_read(str(p), name, integer=(name == "grp/x"))
+                ok += 1
+            except native.CromaError:
+                errors += 1
+    assert ok > 0 and errors > 0
