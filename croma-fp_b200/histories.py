@@ -59,6 +59,24 @@ def dz_to_dt(dz: float, z: float) -> float:
 DEFAULT_BACKGROUND = dict(bfield_mode=0, mu_mol=0.59, eta_B=0.05, mach_limit=0.5, l_turb_target_kpc=150.0)
 
 
+def run_loop_raw(i: int, nsnap: int, raw_of, z, c_dens, c_mag) -> dict:
+    """The CromaB200RawSnapshot fields of snapshot i of an nsnap-snapshot
+    series as the run loop forms them (src/tracer_fp.c:917-1015): raw_of(k)
+    gives snapshot k's raw fields (RAW_FIELDS), z / c_dens / c_mag its
+    redshift and unit factors."""
+    if i == 0:
+        ip, ic, inx = 0, 0, (1 if nsnap > 1 else 0)
+        floor, interp = 0, 0
+    else:
+        ip, ic, inx = i - 1, i, (i + 1 if i + 1 < nsnap else i)
+        floor, interp = 1, int(i + 1 < nsnap)
+    cur, prev, nxt = raw_of(ic), raw_of(ip), raw_of(inx)
+    return dict(temp_K=cur["temperature"], density=cur["density"], bx=cur["B_x"], by=cur["B_y"], bz=cur["B_z"],
+                div_v=cur["div_v"], curl_v_prev=prev["curl_v"], curl_v=cur["curl_v"], curl_v_next=nxt["curl_v"],
+                l_turb_cm=cur["dx_phys"], c_dens=float(c_dens[ic]), c_mag=float(c_mag[ic]), z_prev=float(z[ip]),
+                z_curr=float(z[ic]), z_next=float(z[inx]), apply_temp_floor=floor, allow_curl_interp=interp)
+
+
 class SnapshotSeries:
     """The snapshot files base + NNNN + ext under directory, indices
     [first, last) (all present ones when not given), tracers
@@ -118,19 +136,7 @@ class SnapshotSeries:
 
     def raw_snapshot(self, i: int) -> dict:
         """The CromaB200RawSnapshot fields of snapshot i as the run loop forms them."""
-        n = len(self.files)
-        if i == 0:
-            ip, ic, inx = 0, 0, (1 if n > 1 else 0)
-            floor, interp = 0, 0
-        else:
-            ip, ic, inx = i - 1, i, (i + 1 if i + 1 < n else i)
-            floor, interp = 1, int(i + 1 < n)
-        cur, prev, nxt = self.raw(ic), self.raw(ip), self.raw(inx)
-        return dict(temp_K=cur["temperature"], density=cur["density"], bx=cur["B_x"], by=cur["B_y"],
-                    bz=cur["B_z"], div_v=cur["div_v"], curl_v_prev=prev["curl_v"], curl_v=cur["curl_v"],
-                    curl_v_next=nxt["curl_v"], l_turb_cm=cur["dx_phys"], c_dens=float(self.c_dens[ic]),
-                    c_mag=float(self.c_mag[ic]), z_prev=float(self.z[ip]), z_curr=float(self.z[ic]),
-                    z_next=float(self.z[inx]), apply_temp_floor=floor, allow_curl_interp=interp)
+        return run_loop_raw(i, len(self.files), self.raw, self.z, self.c_dens, self.c_mag)
 
     def background(self, i: int, params: dict | None = None, ctx=None) -> np.ndarray:
         """The [8][ntracer] background of snapshot i, derived on the device."""

@@ -261,6 +261,7 @@ def make_emission_tables(name="emission_tables"):
 
 
 HISTORY_SNAPS = (0, 1, 2, 3, 97, 98, 99)   # of the 100-file series: its start and its end
+LONG_SNAPS = 20
 
 
 def make_histories(name="histories"):
@@ -271,7 +272,9 @@ def make_histories(name="histories"):
     next snapshots' curl_v), the unit factors, redshifts and run-loop flags,
     the timeline (z, z_next, dt), the masses, and the reference's own
     prepare_background_cell outputs (oracle/_ref) for the default run
-    parameters."""
+    parameters; and the raw fields of the first 64 of those tracers over the
+    first LONG_SNAPS snapshots (long<k>_<field>), with every snapshot's unit
+    factors."""
     from croma_fp_b200 import histories
     refroot = os.environ.get("CROMA_REFERENCE_ROOT", "/root/reference")
     S = histories.SnapshotSeries(os.path.join(refroot, "tracer_10k"))
@@ -284,6 +287,13 @@ def make_histories(name="histories"):
         for k, v in sel.items():
             out[f"s{i}_{k}"] = np.asarray(v)
         out[f"s{i}_bg_ref"] = pyoracle.reference_background(sel, histories.DEFAULT_BACKGROUND)
+    # the first 64 of those tracers over the first LONG_SNAPS snapshots, raw
+    long_idx = idx[:64]
+    out["c_dens"], out["c_mag"] = S.c_dens, S.c_mag
+    for k in range(LONG_SNAPS):
+        for f, v in S.raw(k).items():
+            out[f"long{k}_{f}"] = np.ascontiguousarray(v[long_idx])
+    out["long_mass"] = S.mass()[long_idx]
     np.savez_compressed(os.path.join(HERE, f"golden_{name}.npz"), **out)
     print(name, "written")
 

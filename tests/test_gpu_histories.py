@@ -108,3 +108,43 @@ def test_real_histories_evolve_like_the_oracle(path):
             assert np.any(g_cre != cre)
     finally:
         fp.close()
+
+
+def test_real_histories_over_twenty_snapshots():
+    """The fixture's first 64 tracers over the first 20 snapshots of the
+    series (treated as a 20-snapshot run), on-chip FP64 path on the device
+    backgrounds against the oracle on its own: within the FP64 bar after
+    every snapshot, so no error builds up along real histories."""
+    from croma_fp_b200 import histories
+    cfg = config.tracer_10k(nb=128)
+    nlong = 20
+    raw_of = lambda k: {f: FIX[f"long{k}_{f}"] for f in histories.RAW_FIELDS}   # noqa: E731
+    z, dt, c_dens, c_mag = FIX["z"], FIX["dt"], FIX["c_dens"], FIX["c_mag"]
+    mass = np.ascontiguousarray(FIX["long_mass"])
+    n = mass.shape[0]
+    fp = native.TracerFP(cfg, path="fused")
+    o = pyoracle.Oracle(cfg)
+    try:
+        gp, ge = fp.grid(0), fp.grid(1)
+        crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), n, cfg.species)
+        fp.set_state(crp, cre, mass=mass)
+        o_crp, o_cre = crp.copy(), cre.copy()
+        q = np.zeros_like(crp)
+        raws = [histories.run_loop_raw(k, nlong, raw_of, z, c_dens, c_mag) for k in range(nlong)]
+        dev_bg = [native.background_prepare(r, PRM) for r in raws]
+        ora_bg = [pyoracle.background(r, PRM) for r in raws]
+        elapsed = 0.0
+        worst = 0.0
+        for k in range(nlong - 1):
+            fp.snapshot(dev_bg[k], dev_bg[k + 1], float(z[k]), float(z[k + 1]), True, float(dt[k]), elapsed,
+                        sync=True)
+            o.snapshot(ora_bg[k], ora_bg[k + 1], float(z[k]), float(z[k + 1]), True, float(dt[k]), elapsed,
+                       q, q, o_crp, o_cre, mass=mass)
+            elapsed += float(dt[k])
+            g_crp, g_cre = fp.get_state()
+            err = rel_err(g_cre, o_cre)
+            worst = max(worst, err)
+            assert err <= 1e-10, (k, err)
+        print("worst over 19 snapshots", worst)
+    finally:
+        fp.close()
