@@ -1,9 +1,10 @@
 """Real tracer histories on the GPU: the device background
 (croma_b200_background_prepare) of the committed tracer_10k fixture
 (tests/golden/golden_histories.npz: the reference's own
-prepare_background_cell outputs) and three snapshots of those tracers
-evolved with it, against the oracle evolving the same tracers on the
-reference's backgrounds.
+prepare_background_cell outputs), and those tracers evolved with it over
+three snapshots (both paths) and over twenty (on-chip path), against the
+oracle evolving the same tracers on the reference's (or its own)
+backgrounds.
 
 The device background repeats the reference's operations in its order
 without contraction; only pow(L_target / L, 0.3333) comes from CUDA's libm,
