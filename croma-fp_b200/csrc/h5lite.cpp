@@ -201,13 +201,19 @@ std::string heap_name(const File &f, uint64_t heap_addr, uint64_t off)
 }
 
 // Look name up among the links of the group whose symbol table is (btree, heap).
-bool find_link(const File &f, uint64_t btree, uint64_t heap, const std::string &name, Entry &hit, int depth = 0)
+// A child node's level is one below its parent's (so no walk can cycle), and
+// the walk visits at most kMaxNodes nodes (so no file can make it long).
+constexpr int kMaxNodes = 1 << 16;
+
+bool find_link(const File &f, uint64_t btree, uint64_t heap, const std::string &name, Entry &hit,
+               int &visits, int expect_level = -1)
 {
-    if (depth > 64) fail("'" + f.path + "': group B-tree deeper than 64 levels");
+    if (++visits > kMaxNodes) fail("'" + f.path + "': group B-tree with more than 65536 nodes");
     const std::vector<uint8_t> hdr = f.read(btree, 8 + 2 * (uint64_t)f.so);
     if (std::memcmp(hdr.data(), "TREE", 4) != 0) fail("'" + f.path + "': B-tree node signature missing");
     if (hdr[4] != 0) fail("'" + f.path + "': not a group B-tree node");
     const int level = hdr[5];
+    if (expect_level >= 0 && level != expect_level) fail("'" + f.path + "': B-tree child at the wrong level");
     const uint64_t nent = (uint64_t)hdr[6] | ((uint64_t)hdr[7] << 8);
     const uint64_t body = 8 + 2 * (uint64_t)f.so;
     const std::vector<uint8_t> node = f.read(btree, body + nent * (f.sl + f.so) + f.sl);
@@ -216,7 +222,7 @@ bool find_link(const File &f, uint64_t btree, uint64_t heap, const std::string &
         c.len();   // key: heap offset of the child's smallest name (not needed: every child is searched)
         const uint64_t child = c.off();
         if (level > 0) {
-            if (find_link(f, child, heap, name, hit, depth + 1)) return true;
+            if (find_link(f, child, heap, name, hit, visits, level - 1)) return true;
             continue;
         }
         const std::vector<uint8_t> sh = f.read(child, 8);
@@ -261,13 +267,26 @@ struct Dataset {
     int layout = -1;               // 0 compact, 1 contiguous
     uint64_t addr = kUndef, bytes = 0;
     std::vector<uint8_t> compact;
-    uint64_t nelem() const
+    uint64_t nelem() const   // checked against overflow when the dataset is opened
     {
         uint64_t n = 1;
         for (uint64_t d : dims) n *= d;
         return n;
     }
 };
+
+// The element count of dims, failing where it or its byte size exceeds 2^62
+// (so that offsets and byte counts derived from it cannot wrap).
+void check_extent(const File &f, const std::vector<uint64_t> &dims, int elem_size)
+{
+    constexpr uint64_t kMax = 1ull << 62;
+    uint64_t n = 1;
+    for (uint64_t d : dims) {
+        if (d != 0 && n > kMax / d) fail("'" + f.path + "': dataspace too large");
+        n *= d;
+    }
+    if (elem_size > 0 && n > kMax / (uint64_t)elem_size) fail("'" + f.path + "': dataspace too large");
+}
 
 Dataset open_dataset(File &f, const char *name)
 {
@@ -311,7 +330,8 @@ Dataset open_dataset(File &f, const char *name)
         uint64_t bt = kUndef, hp = kUndef;
         group_table(f, cur, bt, hp);
         Entry hit;
-        if (!find_link(f, bt, hp, part, hit)) fail("'" + f.path + "': no dataset or group '" + part + "'");
+        int visits = 0;
+        if (!find_link(f, bt, hp, part, hit, visits)) fail("'" + f.path + "': no dataset or group '" + part + "'");
         cur = hit;
     }
 
@@ -372,6 +392,7 @@ Dataset open_dataset(File &f, const char *name)
           (d.cls == 1 && (d.size == 4 || d.size == 8))))
         fail("'" + f.path + "': datatype class " + std::to_string(d.cls) + " size " + std::to_string(d.size) +
              " is not read here");
+    check_extent(f, d.dims, d.size);
     if (d.layout == 1 && d.addr != kUndef && d.bytes < d.nelem() * (uint64_t)d.size)
         fail("'" + f.path + "': contiguous storage smaller than the dataspace");
     return d;

@@ -90,3 +90,35 @@ def test_corrupted_metadata_gives_errors_not_crashes(tmp_path):
             except native.CromaError:
                 errors += 1
     assert ok > 0 and errors > 0
+
+
+def test_cyclic_btree_and_oversized_dataspace_are_refused(tmp_path, monkeypatch):
+    """A B-tree whose internal node names itself as a child, and a dataspace
+    whose element count overflows, are refused with an error (the walk checks
+    that each child sits one level below its parent and bounds the nodes it
+    visits; extents are checked against 2^62 elements and bytes)."""
+    data = {f"d{k:02d}": np.full(4, float(k)) for k in range(24)}
+    path = tmp_path / "tree.h5"
+    h5write.write(str(path), data, leaf_k=2)
+    raw = bytearray(path.read_bytes())
+    pos, roots = 0, []
+    while (pos := raw.find(b"TREE", pos)) >= 0:
+        if raw[pos + 5] == 1:
+            roots.append(pos)
+        pos += 4
+    assert roots, "the writer made no two-level B-tree"
+    root = roots[0]
+    raw[root + 32:root + 40] = root.to_bytes(8, "little")   # first child := the node itself
+    bad = tmp_path / "cycle.h5"
+    bad.write_bytes(bytes(raw))
+    with pytest.raises(native.CromaError, match="wrong level"):
+        native.h5_read(str(bad), "d23")
+
+    monkeypatch.setattr(h5write, "_space_msg", lambda shape: h5write.struct.pack("<BBBB4x", 1, 3, 0, 0) +
+                        h5write.struct.pack("<QQQ", 2**31, 2**31, 2**31))
+    big = tmp_path / "big.h5"
+    h5write.write(str(big), {"x": np.zeros(4)})
+    with pytest.raises(native.CromaError, match="dataspace too large"):
+        native.h5_shape(str(big), "x")
+    with pytest.raises(native.CromaError, match="dataspace too large"):
+        native.h5_read(str(big), "x", 2**62 - 1, 1)
