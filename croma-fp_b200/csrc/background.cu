@@ -42,7 +42,8 @@ __global__ void __launch_bounds__(256) background_kernel(BgArgs a)
     const CromaB200RawSnapshot &r = a.r;
     const CromaB200BackgroundParams &p = a.p;
     const double target = p.l_turb_target_kpc * kBgKpc;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
         const double rho = r.density[i] * r.c_dens;
         const double bx = r.bx[i] * r.c_mag, by = r.by[i] * r.c_mag, bz = r.bz[i] * r.c_mag;
         if (!(rho > 0.0) || !(target > 0.0)) {   // prepare_background_cell returns -1
@@ -115,45 +116,46 @@ extern "C" int croma_b200_background_prepare(CromaB200Context *ctx, int ntracer,
     cudaStream_t st = ctx ? ctx->impl.stream : nullptr;
     const size_t n = (size_t)ntracer;
     // host arrays go up into one device block: 10 raw fields, the output, the error word
-    double *blk = nullptr;
+    double *blk = nullptr, *d_host_out = nullptr;
     unsigned *d_err = nullptr;
     CromaB200RawSnapshot d = r;
-    double *d_out = bg;
+    unsigned herr = 0;
+    cudaError_t e = cudaSuccess;
+    const char *what = "background_prepare";
     if (!on_device) {
-        CROMA_CUDA(cudaMallocAsync(&blk, (11 * n) * sizeof(double) + 256, st));
+        e = cudaMallocAsync(&blk, (10 * n) * sizeof(double) + 256, st);
+        if (e == cudaSuccess) e = cudaMallocAsync(&d_host_out, 8 * n * sizeof(double), st);
         const double *src[10] = {r.temp_K, r.density, r.bx, r.by, r.bz, r.div_v, r.curl_v_prev, r.curl_v,
                                  r.curl_v_next, r.l_turb_cm};
         const double **dst[10] = {&d.temp_K, &d.density, &d.bx, &d.by, &d.bz, &d.div_v, &d.curl_v_prev, &d.curl_v,
                                   &d.curl_v_next, &d.l_turb_cm};
-        for (int f = 0; f < 10; f++) {
+        for (int f = 0; f < 10 && e == cudaSuccess; f++) {
             if (!src[f]) { *dst[f] = nullptr; continue; }
             double *p = blk + (size_t)f * n;
-            CROMA_CUDA(cudaMemcpyAsync(p, src[f], n * sizeof(double), cudaMemcpyHostToDevice, st));
+            e = cudaMemcpyAsync(p, src[f], n * sizeof(double), cudaMemcpyHostToDevice, st);
             *dst[f] = p;
         }
-        d_out = nullptr;
-        CROMA_CUDA(cudaMallocAsync(&d_out, 8 * n * sizeof(double), st));
-        d_err = reinterpret_cast<unsigned *>(blk + 10 * n);
+        if (e == cudaSuccess) d_err = reinterpret_cast<unsigned *>(blk + 10 * n);
     } else {
-        CROMA_CUDA(cudaMallocAsync(&d_err, 256, st));
+        e = cudaMallocAsync(&d_err, 256, st);
     }
-    CROMA_CUDA(cudaMemsetAsync(d_err, 0, sizeof(unsigned), st));
-    BgArgs a{d, *prm, ntracer, d_out, d_err};
-    const int blocks = (int)std::min<size_t>((n + 255) / 256, 65535);
-    background_kernel<<<blocks, 256, 0, st>>>(a);
-    unsigned herr = 0;
-    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_err, 0, sizeof(unsigned), st);
+    if (e == cudaSuccess) {
+        BgArgs a{d, *prm, ntracer, on_device ? bg : d_host_out, d_err};
+        const int blocks = (int)std::min<size_t>((n + 255) / 256, 65535);
+        background_kernel<<<blocks, 256, 0, st>>>(a);
+        e = cudaGetLastError();
+        what = "background_kernel";
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess && !on_device)
-        e = cudaMemcpyAsync(bg, d_out, 8 * n * sizeof(double), cudaMemcpyDeviceToHost, st);
+        e = cudaMemcpyAsync(bg, d_host_out, 8 * n * sizeof(double), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (!on_device) {
-        cudaFreeAsync(d_out, st);
-        cudaFreeAsync(blk, st);
-    } else {
-        cudaFreeAsync(d_err, st);
-    }
-    if (e != cudaSuccess) return cuda_fail(e, "background_prepare");
+    // released on every path
+    if (d_host_out) cudaFreeAsync(d_host_out, st);
+    if (blk) cudaFreeAsync(blk, st);
+    if (on_device && d_err) cudaFreeAsync(d_err, st);
+    if (e != cudaSuccess) return cuda_fail(e, what);
     if (herr) {
         set_error("background_prepare: a tracer has density <= 0 (or the target turbulence scale <= 0); "
                   "its fields are set to 0");
