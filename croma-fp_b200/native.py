@@ -231,10 +231,15 @@ def background_prepare(raw: dict, params: dict, ctx=None, nb: int = 256, on_devi
     if on_device:
         n = int(raw["ntracer"])
     prm = CromaB200BackgroundParams(**params)
+    if n is None:
+        raise ValueError("raw has no per-tracer field")
     if out is None:
         if on_device:
             raise ValueError("on_device needs an output address")
         out = np.empty((8, n))
+    elif not on_device and (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.shape != (8, n)
+                            or not out.flags.c_contiguous or not out.flags.writeable):
+        raise ValueError(f"out must be a writeable C-contiguous float64 array of shape (8, {n})")
     dst = out if on_device else out.ctypes.data
     h = ctx.h if ctx is not None else None
     rc = L.croma_b200_background_prepare(h, n, C.byref(r), C.byref(prm), int(bool(on_device)), dst)
