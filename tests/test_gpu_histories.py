@@ -1,4 +1,4 @@
-"""Real tracer histories on the GPU: the device background
+"""Real tracer histories on the GPU (HDF5 tracer input): the device background
 (croma_b200_background_prepare) of the committed tracer_10k fixture
 (tests/golden/golden_histories.npz: the reference's own
 prepare_background_cell outputs), and those tracers evolved with it over

@@ -1,4 +1,4 @@
-"""Real tracer histories (HDF5 input), on the CPU.
+"""Real tracer histories (HDF5 tracer input), on the CPU.
 
 * The library's HDF5 reader (croma_b200_h5_*) on the reference's own
   tracer_10k snapshot series, where the reference tree is present
