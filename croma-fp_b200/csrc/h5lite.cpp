@@ -3,7 +3,7 @@
 // libhdf5 in tracer_load_hdf5_raw_snapshot_slice,
 // src/tracer_fp_background.c:1003-1204, and read_redshift_hdf5, :70-146).
 //
-// libhdf5 is not part of this build, so this file reads the subset of the
+// libhdf5 is not linked into this library, so this file reads the subset of the
 // HDF5 format (File Format Specification version 3.0) that those files use:
 //   * superblock version 0 or 1 (signature at offset 0 or at a user-block
 //     boundary 512 * 2^k), 8-byte offsets and lengths;

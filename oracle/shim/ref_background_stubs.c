@@ -15,7 +15,7 @@ void tracer_copy_background_slot(int ntracer, const TracerFpBackgroundSlot *dst,
                                  const TracerFpBackgroundSlot *src)
 {
     (void)ntracer; (void)dst; (void)src;
-    fprintf(stderr, "oracle/_ref: tracer_copy_background_slot is not part of this build\n");
+    fprintf(stderr, "oracle/_ref: tracer_copy_background_slot is not compiled into this checker\n");
 }
 
 int tracer_load_hdf5_raw_snapshot_slice(const TracerFpHdf5Meta *meta, int snap_id, long int tracer_start,
