@@ -21,7 +21,8 @@ background block is derived on the device (croma_b200_background_prepare):
   temperature floor and no curl interpolation; for i >= 1 snapshots i-1, i
   and i+1 (i again at the end), the temperature floor on, curl
   interpolation where a next snapshot exists;
-* tracer masses: ``M_tracer`` of the first snapshot (variable_tracer_mass).
+* tracer masses: ``M_tracer`` of the first snapshot (variable_tracer_mass);
+* the snapshot loop (include/tracer_fp_solve.inc): SnapshotSeries.evolve.
 """
 from __future__ import annotations
 
@@ -141,3 +142,35 @@ class SnapshotSeries:
     def background(self, i: int, params: dict | None = None, ctx=None) -> np.ndarray:
         """The [8][ntracer] background of snapshot i, derived on the device."""
         return native.background_prepare(self.raw_snapshot(i), params or DEFAULT_BACKGROUND, ctx=ctx, nb=self.nb)
+
+    def evolve(self, fp, start: int = 0, stop: int | None = None, params: dict | None = None,
+               elapsed: float = 0.0, background=None, after=None) -> float:
+        """Advance the tracers fp holds (a native.TracerFP over this series'
+        tracers, or anything with its snapshot method) through snapshots
+        [start, stop) as the reference's snapshot loop does
+        (include/tracer_fp_solve.inc:1-20, :1676-1779): snapshot i goes from
+        background i to background i + 1 over dt[i], interpolating between
+        them; the series' last snapshot has no next one and runs on its own
+        background with z_next = z and no interpolation; elapsed (Gyr)
+        accumulates dt.  background(i) gives snapshot i's [8][ntracer] block
+        (default: derived on the device with params); after(i, elapsed) runs
+        after snapshot i.  Returns the elapsed time.  Shock fields are not
+        read: the tracer_10k run has DSA off (params_tracer_10k.txt:70-72)."""
+        n = len(self)
+        stop = n if stop is None else stop
+        if not 0 <= start <= stop <= n:
+            raise ValueError(f"snapshots [{start}, {stop}) outside the series' {n}")
+        if start == stop:
+            return elapsed
+        bg_of = background if background is not None else (lambda i: self.background(i, params))
+        curr = bg_of(start)
+        for i in range(start, stop):
+            has_next = i + 1 < n
+            nxt = bg_of(i + 1) if has_next else curr
+            z_next = float(self.z[i + 1]) if has_next else float(self.z[i])
+            fp.snapshot(curr, nxt, float(self.z[i]), z_next, has_next, float(self.dt[i]), elapsed)
+            elapsed += float(self.dt[i])
+            if after is not None:
+                after(i, elapsed)
+            curr = nxt
+        return elapsed

@@ -149,3 +149,50 @@ def test_real_histories_over_twenty_snapshots():
         print("worst over 19 snapshots", worst)
     finally:
         fp.close()
+
+
+def test_snapshot_series_from_files(tmp_path):
+    """End to end from files: the fixture's 20 snapshots written as a
+    snapshot series (series_io), read by the library's HDF5 reader, each
+    snapshot's background derived on the device, and the 64 tracers evolved
+    on the GPU through all 20 snapshots by SnapshotSeries.evolve (the last
+    one without a next snapshot), against the oracle running the same loop on
+    its background restatement: within the FP64 bar after every snapshot."""
+    import series_io
+    from croma_fp_b200 import histories
+    series_io.write_series(str(tmp_path))
+    S = histories.SnapshotSeries(str(tmp_path), nb=128)
+    cfg = config.tracer_10k(nb=128)
+    n = S.ntracer
+    mass = S.mass()
+    fp = native.TracerFP(cfg, path="fused")
+    o = pyoracle.Oracle(cfg)
+    try:
+        gp, ge = fp.grid(0), fp.grid(1)
+        crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), n, cfg.species)
+        fp.set_state(crp, cre, mass=mass)
+        q = np.zeros_like(crp)
+
+        class OracleFP:
+            state = [crp.copy(), cre.copy()]
+
+            def snapshot(self, bc, bn, z, zn, allow, dt, elapsed):
+                o.snapshot(bc, bn, z, zn, allow, dt, elapsed, q, q, self.state[0], self.state[1], mass=mass)
+
+        ref = []
+        ofp = OracleFP()
+        S.evolve(ofp, background=lambda i: pyoracle.background(S.raw_snapshot(i), PRM),
+                 after=lambda i, el: ref.append(ofp.state[1].copy()))
+        errs = []
+
+        def check(i, el):
+            _, g_cre = fp.get_state()
+            errs.append(rel_err(g_cre, ref[i]))
+            assert errs[-1] <= 1e-10, (i, errs[-1])
+
+        end = S.evolve(fp, params=PRM, after=check)
+        assert len(errs) == len(S) == 20 and end > 0.0
+        assert np.any(fp.get_state()[1] != cre)
+        print("worst over the written series", max(errs))
+    finally:
+        fp.close()

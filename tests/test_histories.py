@@ -180,3 +180,71 @@ def test_oracle_evolves_real_histories_like_the_reference():
         elapsed += float(S.dt[i])
         assert np.array_equal(n_o, n_r) and np.array_equal(a[1], b[1]), i
     assert np.any(a[1] != cre)
+
+
+def test_series_loader_and_snapshot_loop_on_a_written_series(tmp_path):
+    """The fixture's 20 snapshots written as a snapshot series (series_io),
+    read back through SnapshotSeries: redshifts, snapshot steps, unit
+    factors, raw fields and masses are the fixture's.  evolve() runs the
+    reference's snapshot loop: its calls (backgrounds, z_next, interpolation
+    flag, dt, elapsed) over the series' end, and on the oracle over five
+    snapshots the same spectra, bit for bit, as the loop written out by hand
+    (the real-history GPU tests' form)."""
+    import series_io
+    series_io.write_series(str(tmp_path))
+    n = series_io.NLONG
+    S = histories.SnapshotSeries(str(tmp_path), nb=128)
+    assert len(S) == n and S.ntracer == 64 and S.index[0] == series_io.FIRST
+    assert np.array_equal(S.z, FIX["z"][:n])
+    assert np.array_equal(S.dt[:n - 1], FIX["dt"][:n - 1])   # the last step differs: the series ends there
+    assert np.array_equal(S.c_dens, FIX["c_dens"][:n])
+    assert np.allclose(S.c_mag, FIX["c_mag"][:n], rtol=1e-15, atol=0.0)
+    for k in (0, 7, n - 1):
+        raw = S.raw(k)
+        for f in histories.RAW_FIELDS:
+            assert np.array_equal(raw[f], FIX[f"long{k}_{f}"]), (k, f)
+    assert np.array_equal(S.mass(), FIX["long_mass"])
+    assert np.array_equal(S.particle_ids(3), np.arange(100, 164))
+
+    calls = []
+
+    class Recorder:
+        def snapshot(self, bc, bn, z, zn, allow, dt, elapsed):
+            calls.append((bc, bn, z, zn, allow, dt, elapsed))
+
+    blocks = {i: np.full((8, 64), float(i)) for i in range(n)}
+    end = S.evolve(Recorder(), start=n - 3, background=blocks.__getitem__, elapsed=1.0)
+    assert [c[0] is blocks[i] for c, i in zip(calls, range(n - 3, n))] == [True] * 3
+    assert calls[0][1] is blocks[n - 2] and calls[0][3] == S.z[n - 2] and calls[0][4] is True
+    assert calls[-1][1] is blocks[n - 1] and calls[-1][3] == calls[-1][2] == S.z[n - 1] and calls[-1][4] is False
+    assert [c[5] for c in calls] == [float(S.dt[i]) for i in range(n - 3, n)]
+    assert calls[1][6] == 1.0 + float(S.dt[n - 3])
+    assert end == (1.0 + float(S.dt[n - 3])) + float(S.dt[n - 2]) + float(S.dt[n - 1])
+    with pytest.raises(ValueError):
+        S.evolve(Recorder(), start=3, stop=2)
+
+    from croma_fp_b200 import synth
+    cfg = config.tracer_10k(nb=128)
+    S16 = histories.SnapshotSeries(str(tmp_path), nb=128, ntracer=16)
+    mass = S16.mass()
+    o = pyoracle.Oracle(cfg)
+    gp, ge = o.grid(0), o.grid(1)
+    crp0, cre0 = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), 16, cfg.species)
+    q = np.zeros_like(crp0)
+
+    class OracleFP:
+        def __init__(self):
+            self.crp, self.cre = crp0.copy(), cre0.copy()
+
+        def snapshot(self, bc, bn, z, zn, allow, dt, elapsed):
+            o.snapshot(bc, bn, z, zn, allow, dt, elapsed, q, q, self.crp, self.cre, mass=mass)
+
+    bg = [pyoracle.background(S16.raw_snapshot(i), PRM) for i in range(6)]
+    a = OracleFP()
+    S16.evolve(a, stop=5, background=bg.__getitem__)
+    b = OracleFP()
+    elapsed = 0.0
+    for k in range(5):
+        b.snapshot(bg[k], bg[k + 1], float(S16.z[k]), float(S16.z[k + 1]), True, float(S16.dt[k]), elapsed)
+        elapsed += float(S16.dt[k])
+    assert np.array_equal(a.cre, b.cre) and np.any(a.cre != cre0)
