@@ -142,11 +142,15 @@ def _group(buf: _Buf, children: dict, leaf_k: int):
     return tree(leaves, 1), heap_at
 
 
-def write(path: str, tree: dict, leaf_k: int = 4, compact=(), split=()):
+def write(path: str, tree: dict, leaf_k: int = 4, compact=(), split=(), sb_version: int = 0,
+          userblock: int = 0):
     """tree: {name: ndarray | dict (a subgroup)}; names in compact are
-    stored compact, those in split with a continuation block."""
+    stored compact, those in split with a continuation block.  sb_version 0
+    or 1 (version 1 adds the indexed-storage K); userblock bytes (0 or
+    512 * 2^k) of filler before the superblock, whose base address then
+    points at it."""
     buf = _Buf()
-    buf.alloc(96)   # superblock + root entry, written last
+    buf.alloc(104)   # superblock + root entry, written last
 
     def build(node: dict, prefix: str) -> tuple:
         children = {}
@@ -161,9 +165,11 @@ def write(path: str, tree: dict, leaf_k: int = 4, compact=(), split=()):
 
     bt, hp = build(tree, "")
     root_oh = _object_header(buf, [_msg(0x11, struct.pack("<QQ", bt, hp))])
-    sb = b"\x89HDF\r\n\x1a\n" + struct.pack("<BBBBBBBBHHI", 0, 0, 0, 0, 0, 8, 8, 0, leaf_k, 16, 0)
-    sb += struct.pack("<QQQQ", 0, UNDEF, len(buf.b), UNDEF)
+    sb = b"\x89HDF\r\n\x1a\n" + struct.pack("<BBBBBBBBHHI", sb_version, 0, 0, 0, 0, 8, 8, 0, leaf_k, 16, 0)
+    if sb_version == 1:
+        sb += struct.pack("<HH", 32, 0)   # indexed storage internal node K, reserved
+    sb += struct.pack("<QQQQ", userblock, UNDEF, len(buf.b), UNDEF)
     sb += struct.pack("<QQII", 0, root_oh, 1, 0) + struct.pack("<QQ", bt, hp)
     buf.put(0, sb)
     with open(path, "wb") as f:
-        f.write(bytes(buf.b))
+        f.write(b"U" * userblock + bytes(buf.b))

@@ -122,3 +122,17 @@ def test_cyclic_btree_and_oversized_dataspace_are_refused(tmp_path, monkeypatch)
         native.h5_shape(str(big), "x")
     with pytest.raises(native.CromaError, match="dataspace too large"):
         native.h5_read(str(big), "x", 2**62 - 1, 1)
+
+
+@pytest.mark.parametrize("sb_version,userblock", [(1, 0), (0, 512), (1, 2048)])
+def test_superblock_version_1_and_user_blocks(tmp_path, sb_version, userblock):
+    """A version-1 superblock (four more bytes before the addresses) and a
+    user block before the superblock (signature searched at 512 * 2^k, every
+    address relative to the superblock) read the same as the plain layout."""
+    rng = np.random.default_rng(sb_version + userblock)
+    data = {"a": rng.normal(size=40), "g": {"b": np.arange(9, dtype=np.int64)}, "s": np.array(2.5)}
+    path = str(tmp_path / "v.h5")
+    h5write.write(path, data, sb_version=sb_version, userblock=userblock, compact={"s"})
+    assert np.array_equal(native.h5_read(path, "a"), data["a"])
+    assert np.array_equal(native.h5_read(path, "g/b", integer=True), data["g"]["b"])
+    assert native.h5_shape(path, "s") == ((), "float", 8) and native.h5_read(path, "s")[0] == 2.5
