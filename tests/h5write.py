@@ -55,8 +55,14 @@ def _dtype_msg(dt: np.dtype) -> bytes:
     return head + struct.pack("<I", dt.itemsize) + struct.pack("<HH", 0, dt.itemsize * 8)
 
 
-def _space_msg(shape) -> bytes:
-    out = struct.pack("<BBBB4x", 1, len(shape), 0, 0)
+def _space_msg(shape, version: int = 1, null: bool = False) -> bytes:
+    if version == 2:   # version 2: no reserved bytes, an explicit scalar / simple / null type
+        kind = 2 if null else (0 if len(shape) == 0 else 1)
+        out = struct.pack("<BBBB", 2, 0 if null else len(shape), 0, kind)
+        if null:
+            return out
+    else:
+        out = struct.pack("<BBBB4x", 1, len(shape), 0, 0)
     for d in shape:
         out += struct.pack("<Q", d)
     return out
@@ -80,15 +86,17 @@ def _object_header(buf: _Buf, messages, split: int | None = None) -> int:
     return at
 
 
-def _dataset(buf: _Buf, arr: np.ndarray, compact: bool, split: bool) -> int:
-    raw = arr.tobytes()
+def _dataset(buf: _Buf, arr: np.ndarray, compact: bool, split: bool, space_version: int = 1,
+             null: bool = False) -> int:
+    raw = b"" if null else arr.tobytes()
     if compact:
         layout = struct.pack("<BBH", 3, 0, len(raw)) + raw
     else:
         data_at = buf.alloc(len(raw))
         buf.put(data_at, raw)
         layout = struct.pack("<BBQQ", 3, 1, data_at, len(raw))
-    msgs = [_msg(0x01, _space_msg(arr.shape)), _msg(0x03, _dtype_msg(arr.dtype)), _msg(0x08, layout)]
+    msgs = [_msg(0x01, _space_msg(arr.shape, space_version, null)), _msg(0x03, _dtype_msg(arr.dtype)),
+            _msg(0x08, layout)]
     return _object_header(buf, msgs, split=1 if split else None)
 
 
@@ -143,12 +151,13 @@ def _group(buf: _Buf, children: dict, leaf_k: int):
 
 
 def write(path: str, tree: dict, leaf_k: int = 4, compact=(), split=(), sb_version: int = 0,
-          userblock: int = 0):
+          userblock: int = 0, space_version: int = 1, null=()):
     """tree: {name: ndarray | dict (a subgroup)}; names in compact are
     stored compact, those in split with a continuation block.  sb_version 0
     or 1 (version 1 adds the indexed-storage K); userblock bytes (0 or
     512 * 2^k) of filler before the superblock, whose base address then
-    points at it."""
+    points at it.  space_version 1 or 2 for every dataspace; names in null
+    get a null dataspace (no elements)."""
     buf = _Buf()
     buf.alloc(104)   # superblock + root entry, written last
 
@@ -160,7 +169,8 @@ def write(path: str, tree: dict, leaf_k: int = 4, compact=(), split=(), sb_versi
                 bt, hp = build(v, full + "/")
                 children[name] = _object_header(buf, [_msg(0x11, struct.pack("<QQ", bt, hp))])
             else:
-                children[name] = _dataset(buf, np.asarray(v), full in compact, full in split)
+                children[name] = _dataset(buf, np.asarray(v), full in compact, full in split, space_version,
+                                          full in null)
         return _group(buf, children, leaf_k)
 
     bt, hp = build(tree, "")

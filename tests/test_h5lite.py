@@ -114,7 +114,7 @@ def test_cyclic_btree_and_oversized_dataspace_are_refused(tmp_path, monkeypatch)
     with pytest.raises(native.CromaError, match="wrong level"):
         native.h5_read(str(bad), "d23")
 
-    monkeypatch.setattr(h5write, "_space_msg", lambda shape: h5write.struct.pack("<BBBB4x", 1, 3, 0, 0) +
+    monkeypatch.setattr(h5write, "_space_msg", lambda shape, *a: h5write.struct.pack("<BBBB4x", 1, 3, 0, 0) +
                         h5write.struct.pack("<QQQ", 2**31, 2**31, 2**31))
     big = tmp_path / "big.h5"
     h5write.write(str(big), {"x": np.zeros(4)})
@@ -136,3 +136,18 @@ def test_superblock_version_1_and_user_blocks(tmp_path, sb_version, userblock):
     assert np.array_equal(native.h5_read(path, "a"), data["a"])
     assert np.array_equal(native.h5_read(path, "g/b", integer=True), data["g"]["b"])
     assert native.h5_shape(path, "s") == ((), "float", 8) and native.h5_read(path, "s")[0] == 2.5
+
+
+def test_version_2_dataspaces_scalar_simple_and_null(tmp_path):
+    """Version-2 dataspace messages (an explicit scalar / simple / null type
+    and no reserved bytes): a scalar reads as one element, rank 1 and 2 as
+    their elements, and a null dataspace as no elements."""
+    data = {"x": np.linspace(0.0, 1.0, 11), "m": np.arange(12, dtype=np.int64).reshape(3, 4),
+            "s": np.array(-7.25), "none": np.zeros(3)}
+    path = str(tmp_path / "s2.h5")
+    h5write.write(path, data, space_version=2, null={"none"}, compact={"s"})
+    assert np.array_equal(native.h5_read(path, "x"), data["x"])
+    assert native.h5_shape(path, "m") == ((3, 4), "int", 8)
+    assert np.array_equal(native.h5_read(path, "m", integer=True), data["m"].reshape(-1))
+    assert native.h5_shape(path, "s") == ((), "float", 8) and native.h5_read(path, "s")[0] == -7.25
+    assert native.h5_shape(path, "none")[0] == (0,) and native.h5_read(path, "none").size == 0
