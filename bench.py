@@ -721,8 +721,8 @@ def run_gpu_arm(args):
                    "sample": f"{type(e).__name__}: {e}"}
     secondary = None
     if rank == 0 and world == 1 and not args.no_secondary:
-        secondary = {"config1": run_config1(args), "heavy_tail": run_heavy_tail(args),
-                     "real_histories": run_real_histories(args)}
+        secondary = {"config1": run_config1(args), "config2": run_config2(args),
+                     "heavy_tail": run_heavy_tail(args), "real_histories": run_real_histories(args)}
     serving = None
     if rank == 0 and world == 1 and args.serving_requests > 0:
         serving = run_serving(args)
@@ -850,6 +850,57 @@ def run_real_histories(args):
                         "ASA centred window, eta cap 0.1, snapshots 1 -> 3 of the series (dump0026-0028)",
             "value": nt * 2 / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / 2,
             "nsub_percentiles_0_10_50_90_100": [float(np.percentile(nsub, q)) for q in (0, 10, 50, 90, 100)]}
+
+
+def run_config2(args):
+    """The precision workload (1,048,576 tracers, electron_only, 128 bins,
+    TTD, DSA tracer_state on 5 % of tracer-snapshots, the 50-snapshot
+    timeline), device-resident: the on-chip FP64, FP32-refined and plain
+    paths on the same inputs, and the FP32-refined spectra against the
+    on-chip FP64 ones after the same steps (max and median relative error
+    over bins above 1e-12 of each tracer's peak, particle-number drift) --
+    the FP64 path is held to the reference's own code by the config-2 parity
+    test (1,024 tracers x 10 snapshots)."""
+    import torch
+    from croma_fp_b200 import config, synth
+    cfg = config.config2()
+    nt, nsnap_timeline = 1 << 20, 50
+    snaps = [20 + k for k in range(5)]
+    w = synth.Workload(cfg, nt, nsnap_timeline, seed=SEED)
+    isn = list(range(snaps[0], snaps[-1] + 2))
+    with cf.ThreadPoolExecutor(min(16, os.cpu_count() or 4)) as ex:
+        bgs = list(ex.map(w.background, isn))
+        shocks = list(ex.map(lambda k: synth.shocks(bgs[k], isn[k], SEED, fraction=DSA_FRACTION),
+                             range(len(snaps))))
+    bg = torch.stack([torch.from_numpy(b) for b in bgs]).cuda()
+    sh = torch.empty((len(snaps), len(SHOCK_KEYS), nt), dtype=torch.float64, device="cuda")
+    for k in range(len(snaps)):
+        for i, key in enumerate(SHOCK_KEYS):
+            sh[k, i].copy_(torch.from_numpy(np.ascontiguousarray(shocks[k][key])))
+    rate, states, ms = {}, {}, {}
+    for path, warm, steps in (("fused", 1, 4), ("fp32r", 1, 4), ("plain", 1, 2)):
+        r, fp, _ = run_resident(path, cfg, nt, w, bg, sh, snaps, warm, steps, emission=False, dsa=True,
+                                keep_open=True)
+        try:
+            if path != "plain":
+                states[path] = fp.get_state() + (fp.schedule()["nsub"],)
+            dp = (fp.grid(0)[1], fp.grid(1)[1])
+        finally:
+            fp.close()
+        rate[path] = nt * steps / (r["ms"] / 1e3)
+        ms[path] = r["ms"] / steps
+    del bg, sh
+    f, q = states["fused"], states["fp32r"]
+    err = compare_spectra(q[0], q[1], f[0], f[1], dp[0], dp[1], q[2], f[2])
+    return {"workload": "precision: 1,048,576 tracers, electron_only, 128 bins, TTD, DSA tracer_state on 5 % of "
+                        "tracer-snapshots (Mach U[2,5]), snapshots 20.. of the z=1->0 50-snapshot timeline, no "
+                        "emission", "fused": rate["fused"], "fp32r": rate["fp32r"], "plain": rate["plain"],
+            "chosen_over_plain": rate["fused"] / rate["plain"], "ms_per_step": ms,
+            "fp32r_vs_fused_fp64": {"after_steps": 5, "max_rel_err": err["max_rel_err"],
+                                    "median_rel_err": err["median_rel_err"],
+                                    "max_particle_number_drift": err["drift"],
+                                    "nsub_mismatches": err["nsub_mismatches"], "bar": 1e-6},
+            "steps": {"fused": 4, "fp32r": 4, "plain": 2}}
 
 
 def run_config1(args):
