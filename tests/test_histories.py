@@ -248,3 +248,24 @@ def test_series_loader_and_snapshot_loop_on_a_written_series(tmp_path):
         b.snapshot(bg[k], bg[k + 1], float(S16.z[k]), float(S16.z[k + 1]), True, float(S16.dt[k]), elapsed)
         elapsed += float(S16.dt[k])
     assert np.array_equal(a.cre, b.cre) and np.any(a.cre != cre0)
+
+
+def test_series_refuses_gaps_and_tracer_ranges_outside_the_files(tmp_path):
+    """A missing snapshot file inside the requested range, a directory without
+    snapshot files, and a tracer range past the files' tracers are refused
+    before anything is read past them."""
+    import os as _os
+    import series_io
+    paths = series_io.write_series(str(tmp_path), nsnap=4)
+    S = histories.SnapshotSeries(str(tmp_path), first=26, last=28, nb=128)
+    assert S.index == [26, 27] and len(S) == 2 and S.ntracer == 64
+    with pytest.raises(ValueError, match="outside"):
+        histories.SnapshotSeries(str(tmp_path), tracer_start=60, ntracer=8, nb=128)
+    _os.remove(paths[2])
+    with pytest.raises(FileNotFoundError, match="missing"):
+        histories.SnapshotSeries(str(tmp_path), nb=128)
+    assert len(histories.SnapshotSeries(str(tmp_path), last=27, nb=128)) == 2
+    empty = tmp_path / "empty"
+    empty.mkdir()
+    with pytest.raises(FileNotFoundError, match="no snapshot files"):
+        histories.SnapshotSeries(str(empty), nb=128)
