@@ -21,9 +21,15 @@ the on-chip FP64 path with every input resident in HBM; ``plain`` the
 per-step FP64 path (the reference's data contract) on the same steps;
 ``e2e`` the same steps through croma_b200_step_host with the inputs read from
 and every output (emissivities, evolved spectra) written to page-locked host
-memory.  ``secondary.config1`` repeats the measurement on the 65,536-tracer,
-256-bin batching workload; ``heavy_tail`` runs a workload whose sub-step
-counts spread over 12..500.
+memory.  ``fp32r`` is the FP32-refined form on the same steps, ``accuracy``
+both forms against the reference's own CPU code on the first 4,096 tracers
+over 5 snapshots.  ``secondary.config1`` repeats the measurement on the
+65,536-tracer, 256-bin batching workload; ``config2`` runs the
+1,048,576-tracer precision workload and compares the FP32-refined spectra
+with the FP64 ones on every tracer; ``heavy_tail`` runs a workload whose
+sub-step counts spread over 12..500; ``real_histories`` evolves real tracer
+histories on backgrounds derived on the device.  ``serving`` is the request
+server under a Poisson stream.
 """
 from __future__ import annotations
 
