@@ -55,6 +55,23 @@ def test_device_background_matches_reference():
         assert float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300))) <= 1e-14, i
 
 
+@pytest.mark.parametrize("prm", [dict(bfield_mode=1), dict(bfield_mode=2, mach_limit=0.0),
+                                 dict(bfield_mode=0, l_turb_target_kpc=40.0, mu_mol=0.6)])
+def test_device_background_matches_restatement_in_every_field_mode(prm):
+    """The B-field modes (simulation field, dynamo field, the larger of the
+    two), no Mach limit and another turbulence scale and molecular weight:
+    the device background against the oracle's restatement (itself bit-exact
+    to the reference's prepare_background_cell) on the fixture's first and
+    middle snapshots."""
+    p = dict(PRM, **prm)
+    for i in (0, 2):
+        got = native.background_prepare(raw(i), p)
+        ref = pyoracle.background(raw(i), p)
+        for f in (0, 1, 3, 4, 6):
+            assert np.array_equal(got[f], ref[f]), (i, f)
+        assert float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300))) <= 1e-14, i
+
+
 def test_device_pointers_equal_host_call():
     torch = pytest.importorskip("torch")
     r = raw(2)
