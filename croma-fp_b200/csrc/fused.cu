@@ -6,10 +6,12 @@
 //   0. seg_pre_kernel, one thread per (segment, tracer): the segment's
 //      interpolated background and the scalars of its coefficients, once for
 //      both species.
-//   1. factor_kernel, one warp per (segment, tracer[, on/off set]): the loss /
-//      diffusion terms of every bin and the Chang-Cooper face weights in
-//      rolled lane-strided loops into the warp's slice of shared memory
-//      (losses / Dpp / CC assembly of src/fp_shared_core.c:729-842,
+//   1. factor_kernel, persistent: each warp takes tracers from an atomic
+//      counter and factors every (segment[, on/off set]) of each: the loss /
+//      diffusion terms of every bin in lane-strided loops into the warp's
+//      slice of shared memory, the Chang-Cooper face weights (at 512 bins in
+//      registers, where the rows use them; below, lane-strided into shared
+//      memory) (losses / Dpp / CC assembly of src/fp_shared_core.c:729-842,
 //      1241-1317, 2358-2431 and src/Chang_Cooper.c:22-184); rows a, b, c in
 //      registers -- lane l owns rows [l*R, (l+1)*R), R = nb/32 -- and the
 //      Thomas pivots d_i = b_i - a_i c_{i-1}/d_{i-1}, a chain of Moebius maps
@@ -23,12 +25,15 @@
 //      factored rows (and the segment's source), and runs each sub-step as
 //      the two first-order linear recurrences of fp_thomas_solve_ws
 //      (src/fp_shared_core.c:226-257), each an affine warp scan: a local pass
-//      per lane, five shuffle levels, a second local pass.  The proton kernel
+//      per lane, five shuffle levels, a second local pass (substep); at 512
+//      bins radix-4 scans of three shuffle levels with the back pass run
+//      while the forward scan is in flight (substep4).  The proton kernel
 //      records the spectrum at each segment start for the secondaries.
 //   3. secondary_kernel: the electron source of every segment from those
 //      proton spectra (prepare_secondary_sources_cell_major,
 //      src/fp_shared_core.c:1591-1672), a tiled [segments*tracers x nb] .
-//      [nb x nb] product, between the proton and the electron steps.
+//      [nb x nb] product on the FP64 tensor cores, between the proton and
+//      the electron steps.
 //
 // Shared-memory rows are stored at (m % R) * kPitch + m / R, so the blocked reads
 // of step 1 (lane l, row l*R + r and its neighbours) hit 32 distinct banks.
