@@ -1306,8 +1306,9 @@ __device__ __forceinline__ void substep_pcr(const Coef<SRC> &F, const double cc[
 
 // Sub-step solvers of the steps kernel: the FP64 warp-scan Thomas (its
 // per-segment constants in registers, or in shared memory to leave registers
-// for more warps), the same with FP32 solves refined by an FP64 residual, and
-// warp PCR.
+// for more warps), the short-chain FP64 form (radix-4 scans, back pass
+// overlapping the forward scan), the warp scan with FP32 solves refined by
+// an FP64 residual, and warp PCR.
 enum { kSolveScan = 0, kSolveRefined = 1, kSolvePcr = 2, kSolveScanShared = 3, kSolveScanRhs = 4,
        kSolveScan4 = 5 };
 
