@@ -33,3 +33,24 @@ def test_reference_arm_prints_the_contract_line():
     e = line["e2e"]
     assert e["value"] == line["value"] and e["unit"] == line["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+
+
+@pytest.mark.skipif(not pyoracle.reference_available(512), reason="oracle/_ref not built")
+def test_reference_arm_under_torchrun_prints_one_line_from_rank_0():
+    """Launched as the multi-GPU bench is (torchrun, two ranks on 127.0.0.1),
+    the reference arm runs on rank 0 alone, which prints the one line; the
+    other rank exits 0 without work."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+                        "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"),
+                        "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1",
+                        "--reference-tracers", "16"],
+                       capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
