@@ -144,7 +144,7 @@ class SnapshotSeries:
         return native.background_prepare(self.raw_snapshot(i), params or DEFAULT_BACKGROUND, ctx=ctx, nb=self.nb)
 
     def evolve(self, fp, start: int = 0, stop: int | None = None, params: dict | None = None,
-               elapsed: float = 0.0, background=None, after=None) -> float:
+               elapsed: float = 0.0, background=None, before=None, after=None) -> float:
         """Advance the tracers fp holds (a native.TracerFP over this series'
         tracers, or anything with its snapshot method) through snapshots
         [start, stop) as the reference's snapshot loop does
@@ -153,8 +153,11 @@ class SnapshotSeries:
         them; the series' last snapshot has no next one and runs on its own
         background with z_next = z and no interpolation; elapsed (Gyr)
         accumulates dt.  background(i) gives snapshot i's [8][ntracer] block
-        (default: derived on the device with params); after(i, elapsed) runs
-        after snapshot i.  Returns the elapsed time.  Shock fields are not
+        (default: derived on the device with params); before(i, bg) runs
+        before snapshot i with its background, on the spectra the snapshot
+        starts from (where the reference computes the emission,
+        include/tracer_fp_solve.inc:117-426); after(i, elapsed) runs after
+        snapshot i.  Returns the elapsed time.  Shock fields are not
         read: the tracer_10k run has DSA off (params_tracer_10k.txt:70-72)."""
         n = len(self)
         stop = n if stop is None else stop
@@ -168,6 +171,8 @@ class SnapshotSeries:
             has_next = i + 1 < n
             nxt = bg_of(i + 1) if has_next else curr
             z_next = float(self.z[i + 1]) if has_next else float(self.z[i])
+            if before is not None:
+                before(i, curr)
             fp.snapshot(curr, nxt, float(self.z[i]), z_next, has_next, float(self.dt[i]), elapsed)
             elapsed += float(self.dt[i])
             if after is not None:

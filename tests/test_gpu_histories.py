@@ -213,3 +213,37 @@ def test_snapshot_series_from_files(tmp_path):
         print("worst over the written series", max(errs))
     finally:
         fp.close()
+
+
+def test_series_emission_before_each_snapshot(tmp_path):
+    """The series loop's before-hook sees the spectra a snapshot starts from,
+    where the reference computes the emission: synchrotron and IC of the
+    written series' tracers (the tracer_10k run's bands) from the hook at
+    snapshot 0 equal those of the initial spectra computed on their own, and
+    change once the spectra have evolved."""
+    import series_io
+    from croma_fp_b200 import histories
+    series_io.write_series(str(tmp_path), nsnap=4)
+    S = histories.SnapshotSeries(str(tmp_path), nb=128)
+    cfg = config.tracer_10k(nb=128)
+    emis = dict(nfreq=16, nu_min_s=5.5, nu_max_s=10.5, ntheta_pitch=512, nlogb=512, logb_min=-6.0, logb_max=2.0,
+                nbins_ic=16, nu_min_ic=13.0, nu_max_ic=28.0)
+    n = S.ntracer
+    fp, alone = native.TracerFP(cfg, path="fused"), native.TracerFP(cfg, path="fused")
+    try:
+        gp, ge = fp.grid(0), fp.grid(1)
+        crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), n, cfg.species)
+        for f in (fp, alone):
+            f.set_state(crp, cre, mass=S.mass())
+            f.emission_setup(**emis)
+        seen = {}
+        S.evolve(fp, stop=3, params=PRM, before=lambda i, bg: seen.__setitem__(i, fp.emission_run(bg, S.z[i],
+                                                                                                     kinds=("syn", "ic"))))
+        first = alone.emission_run(S.background(0, PRM), S.z[0], kinds=("syn", "ic"))
+        for k in ("syn", "ic"):
+            assert np.array_equal(seen[0][k], first[k]), k
+            assert np.all(np.isfinite(seen[2][k])) and np.any(seen[2][k] != seen[0][k]), k
+        assert np.all(seen[0]["syn"] >= 0.0) and np.any(seen[0]["syn"] > 0.0)
+    finally:
+        fp.close()
+        alone.close()

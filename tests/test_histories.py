@@ -213,7 +213,10 @@ def test_series_loader_and_snapshot_loop_on_a_written_series(tmp_path):
             calls.append((bc, bn, z, zn, allow, dt, elapsed))
 
     blocks = {i: np.full((8, 64), float(i)) for i in range(n)}
-    end = S.evolve(Recorder(), start=n - 3, background=blocks.__getitem__, elapsed=1.0)
+    seen = []
+    end = S.evolve(Recorder(), start=n - 3, background=blocks.__getitem__, elapsed=1.0,
+                   before=lambda i, bg: seen.append((i, bg, len(calls))))
+    assert [(i, bg is blocks[i], k) for i, bg, k in seen] == [(n - 3, True, 0), (n - 2, True, 1), (n - 1, True, 2)]
     assert [c[0] is blocks[i] for c, i in zip(calls, range(n - 3, n))] == [True] * 3
     assert calls[0][1] is blocks[n - 2] and calls[0][3] == S.z[n - 2] and calls[0][4] is True
     assert calls[-1][1] is blocks[n - 1] and calls[-1][3] == calls[-1][2] == S.z[n - 1] and calls[-1][4] is False
