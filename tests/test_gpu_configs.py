@@ -7,9 +7,12 @@ snapshot.
 * config 0 (plain FP64 method): 1,024 tracers x the full 100-snapshot
   timeline, electron-only, 128 bins, direct t_acc = 0.3 Gyr; the plain and
   the on-chip path in lockstep with the oracle.
+* config 1 (batching): 256 tracers, e+p, 256 bins, ASA, nsub <= 500, 6
+  snapshots; all three paths.
 * config 2 (precision): TTD, 128 bins, DSA tracer_state injection on 5 % of
-  tracer-snapshots (Mach U[2, 5]) before each of 10 snapshots; FP64 paths
-  at 1e-10, the FP32-refined path at 1e-6.
+  tracer-snapshots (Mach U[2, 5]) before each of 10 snapshots of the
+  configuration's 50-snapshot timeline; FP64 paths at 1e-10, the
+  FP32-refined path at 1e-6.
 * config 4 (full pipeline): 64 tracers, e+p with secondaries, 512 bins, ASA,
   DSA on 10 % of tracer-snapshots, 3 snapshots; all three paths.
 
@@ -41,11 +44,12 @@ def _drift(g, r, dp):
     return float(np.max(np.abs(ng[ok] - nr[ok]) / np.abs(nr[ok]))) if ok.any() else 0.0
 
 
-def _lockstep(cfg, nt, first, nsnap, seed, paths, dsa_fraction=0.0):
-    """Runs the oracle and one GPU context per path side by side; returns
-    the worst spectral error per path."""
+def _lockstep(cfg, nt, first, nsnap, seed, paths, dsa_fraction=0.0, timeline=100):
+    """Runs the oracle and one GPU context per path side by side over
+    snapshots [first, first + nsnap) of a timeline-snapshot z = 1 -> 0
+    timeline; returns the worst spectral error per path."""
     o = _oracle(cfg)
-    w = synth.Workload(cfg, nt, 100, seed=seed)
+    w = synth.Workload(cfg, nt, timeline, seed=seed)
     gp, ge = o.grid(0), o.grid(1)
     crp, cre = synth.initial_state((gp[0], gp[1]), (ge[0], ge[1]), nt, cfg.species)
     qpi, qepri = np.zeros_like(crp), np.zeros_like(cre)
@@ -99,9 +103,15 @@ def test_config0_full_timeline_1024_tracers():
     print("config 0, 1024 tracers x 100 snapshots, worst rel err:", worst)
 
 
+def test_config1_batching_256_tracers_6_snapshots():
+    worst = _lockstep(config.config1(), 256, 5, 6, 20263, ["plain", "fused", "fp32r"])
+    print("config 1, 256 tracers x 6 snapshots, worst rel err:", worst)
+
+
 def test_config2_ttd_with_dsa_10_snapshots():
-    worst = _lockstep(config.config2(), 1024, 20, 10, 20262, ["plain", "fused", "fp32r"], dsa_fraction=0.05)
-    print("config 2, 1024 tracers x 10 snapshots with DSA, worst rel err:", worst)
+    worst = _lockstep(config.config2(), 1024, 20, 10, 20262, ["plain", "fused", "fp32r"], dsa_fraction=0.05,
+                      timeline=50)
+    print("config 2, 1024 tracers x 10 snapshots of the 50-snapshot timeline with DSA, worst rel err:", worst)
 
 
 def test_config4_full_pipeline_64_tracers():
