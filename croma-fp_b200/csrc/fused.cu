@@ -40,6 +40,7 @@
 // Divisions by grid quantities use reciprocals tabulated on the host; the
 // results agree with the reference's divisions to an ulp per operation.
 // Spectra are cell-major [tracer][nb] so that a warp's rows are contiguous.
+#include <cstddef>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -1360,6 +1361,9 @@ __global__ void __launch_bounds__(WPB * 32,
         // segment's sub-steps run: its loads then wait on L2, not on DRAM
         if (gi + 1 < nslot) {
             const double *nf = fac_ptr(P, S, gi + 1, 0, tl) + row0;
+            if (lane < 2)   // and the next segment's scalars this loop reads (dt .. steps of its SegPre)
+                prefetch_l2(reinterpret_cast<const char *>(P.pre + (size_t)(gi + 1) * P.nt + tl) +
+                            (lane ? offsetof(SegPre, steps) : offsetof(SegPre, dt)));
             prefetch_l2(nf);
             prefetch_l2(nf + NB);
             prefetch_l2(nf + 2 * NB);
