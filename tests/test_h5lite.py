@@ -151,3 +151,40 @@ def test_version_2_dataspaces_scalar_simple_and_null(tmp_path):
     assert np.array_equal(native.h5_read(path, "m", integer=True), data["m"].reshape(-1))
     assert native.h5_shape(path, "s") == ((), "float", 8) and native.h5_read(path, "s")[0] == -7.25
     assert native.h5_shape(path, "none")[0] == (0,) and native.h5_read(path, "none").size == 0
+
+
+def test_c_host_reads_through_the_c_abi(tmp_path):
+    """Every public header compiles as C99 (-Wall -Wextra -pedantic, no
+    warnings), and a C program linked against the library reads a snapshot
+    file through croma_b200_h5_*: the values equal the written ones, and a
+    missing dataset comes back as an error message."""
+    import os
+    import shutil
+    import subprocess
+    from conftest import ROOT
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    inc = os.path.join(ROOT, "include")
+    for h in sorted(os.listdir(inc)):
+        src = tmp_path / "h.c"
+        src.write_text(f'#include "{h}"\nint main(void) {{ return 0; }}\n')
+        r = subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-Dnp=128", "-Dnpe=128",
+                            f"-I{inc}", "-c", str(src), "-o", str(tmp_path / "h.o")], capture_output=True, text=True)
+        assert r.returncode == 0, (h, r.stderr)
+    libdir = os.path.dirname(native.library_path(128))
+    exe = tmp_path / "c_host"
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", f"-I{inc}", os.path.join(ROOT, "tests", "c_host_h5.c"),
+                        f"-L{libdir}", "-lcroma_b200_np128", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    dens = np.linspace(1.0e-28, 2.0e-27, 10)
+    path = str(tmp_path / "snap.h5")
+    h5write.write(path, {"density": dens, "particle_ID": np.arange(7, 17, dtype=np.int64)})
+    r = subprocess.run([str(exe), path], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    first, msg = r.stdout.strip().splitlines()
+    f = first.split()
+    assert f[:4] == ["1", "10", "1", "8"]
+    assert [float(x) for x in f[4:7]] == list(dens[2:5]) and f[7:] == ["7", "8"]
+    assert "no_such_field" in msg
