@@ -309,6 +309,55 @@ def run_resident(path, cfg, nt, w, bg_dev, sh_dev, snaps, warmup, steps, emissio
 
 
 # ---------------------------------------------------------------- e2e through host memory
+# share of the host memory left that the e2e measurement's page-locked
+# buffers may take (all local ranks together)
+E2E_HOST_SHARE = 0.6
+
+
+def host_bytes_available():
+    """Bytes the host can still give this job: MemAvailable of /proc/meminfo,
+    capped by the memory cgroup's limit less its usage where one is set
+    (cgroup v2, else v1); None when neither can be read."""
+    avail = None
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    avail = int(line.split()[1]) * 1024
+                    break
+    except (OSError, ValueError, IndexError):
+        pass
+    for lim_f, use_f in (("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory.current"),
+                         ("/sys/fs/cgroup/memory/memory.limit_in_bytes", "/sys/fs/cgroup/memory/memory.usage_in_bytes")):
+        try:
+            with open(lim_f) as f:
+                lim = f.read().strip()
+            if lim == "max":
+                break
+            with open(use_f) as f:
+                left = int(lim) - int(f.read().strip())
+            avail = left if avail is None else min(avail, left)
+            break
+        except (OSError, ValueError):
+            continue
+    return avail
+
+
+def e2e_tracers(cfg, nt, steps, local_ranks, avail):
+    """Tracers of the e2e measurement: all nt, unless the page-locked host
+    buffers of the local ranks (spectra and emissivities out, backgrounds and
+    shock fields in) would take more than E2E_HOST_SHARE of the host memory
+    left (avail bytes); then the largest multiple of 4,096 that fits."""
+    from croma_fp_b200 import native
+    e = native.EMISSION_CONFIG4
+    per_tracer = 8 * (2 * cfg.nb + e["nfreq"] + e["nbins_ic"] + e["nbins_gamma"] + e["nbins_nu"]
+                      + 8 * (steps + 2) + len(SHOCK_KEYS) * (steps + 1))
+    if avail is None:
+        return nt
+    fit = int(E2E_HOST_SHARE * avail / max(1, local_ranks) / per_tracer)
+    return nt if fit >= nt else max(4096, fit // 4096 * 4096)
+
+
 def run_e2e(fp, cfg, nt, w, bgs, shocks, snaps, steps):
     """croma_b200_step_host on page-locked host buffers: per step the
     backgrounds and shock fields go up, the emissivities and the evolved
@@ -663,30 +712,58 @@ def run_gpu_arm(args):
     ms_max = rank_max(res["ms"])
     value = world * nt * args.steps / (ms_max / 1e3)
 
-    # ---- e2e through host memory, on the same context ----
+    fp64_peak = native.fp64_peak(cfg.nb)
+    tuning = {"protons": fp.tuning(0), "electrons": fp.tuning(1)}
+
+    # ---- e2e through host memory: on the same context, or, where the host
+    # memory left cannot hold every rank's page-locked buffers for all
+    # tracers, on a context of fewer tracers (the same for every rank) ----
     e2e = None
     if not args.no_e2e:
-        # every rank pins ~44 GB of host buffers; the ranks agree on success
-        # before the timing reduction, so that one rank's failure cannot
-        # leave the others waiting in a collective
+        from croma_fp_b200 import config
+        local_ranks = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
+        ne = int(-rank_max(-float(e2e_tracers(cfg, nt, args.e2e_steps, local_ranks, host_bytes_available()))))
+        ctx, bgs_e, shocks_e = fp, bgs, shocks
+        r, e2e_err = None, None
         try:
-            r, e2e_err = run_e2e(fp, cfg, nt, w, bgs, shocks, snaps, args.e2e_steps), None
+            if ne < nt:
+                fp.close()
+                fp = None
+                del _eps
+                torch.cuda.empty_cache()
+                ctx = native.TracerFP(cfg, path="fused")
+                crp1, cre1 = seed_rows(ctx, cfg)
+                ctx.set_state_broadcast(ne, crp1, cre1, 1.0e7)
+                ctx.set_dsa(config.DsaParams())
+                ctx.emission_setup(**native.EMISSION_CONFIG4)
+                bgs_e = [np.ascontiguousarray(b[:, :ne]) for b in bgs]
+                shocks_e = [{k: (np.ascontiguousarray(v[:ne]) if isinstance(v, np.ndarray) else v)
+                             for k, v in sh.items()} for sh in shocks]
+            # every rank pins its host buffers; the ranks agree on success
+            # before the timing reduction, so that one rank's failure cannot
+            # leave the others waiting in a collective
+            r = run_e2e(ctx, cfg, ne, w, bgs_e, shocks_e, snaps, args.e2e_steps)
         except (MemoryError, RuntimeError) as ex:
             r, e2e_err = None, f"{type(ex).__name__}: {ex}"
+        finally:
+            if ctx is not fp:
+                ctx.close()
         failed = rank_max(1.0 if r is None else 0.0)
         if failed:
             e2e = {"value": None, "unit": UNIT, "error": e2e_err or "failed on another rank"}
     if not args.no_e2e and e2e is None:
         e2e_s = rank_max(statistics.median(r["times"]))
-        e2e = {"value": world * nt / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(r["h2d"]),
+        e2e = {"value": world * ne / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(r["h2d"]),
                "d2h_bytes_per_step": int(r["d2h"]), "host_buffers": "page-locked (croma_b200_host_alloc)",
                "api": "croma_b200_step_host: backgrounds and shock fields up, emissivities and evolved spectra "
                       "down every step, copies overlapped with the kernels",
-               "steps": len(r["times"]), "ms_per_step": e2e_s * 1e3}
-    fp64_peak = native.fp64_peak(cfg.nb)
-    tuning = {"protons": fp.tuning(0), "electrons": fp.tuning(1)}
-    fp.close()
-    del _eps
+               "steps": len(r["times"]), "ms_per_step": e2e_s * 1e3, "tracers_per_gpu": ne}
+        if ne < nt:
+            e2e["note"] = (f"{ne} of the {nt} tracers per GPU: the host memory left could not hold the "
+                           f"page-locked buffers of all of them for the {local_ranks} rank(s) on this host")
+    if fp is not None:
+        fp.close()
+        del _eps
     torch.cuda.empty_cache()
 
     # ---- the plain per-step path on the same workload ----
