@@ -54,3 +54,28 @@ def test_reference_arm_under_torchrun_prints_one_line_from_rank_0():
     assert len(lines) == 1
     line = json.loads(lines[0])
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
+
+
+def test_e2e_tracer_count_fits_the_host_memory_left():
+    """The e2e measurement keeps every tracer when the page-locked buffers of
+    the host's ranks fit in 60 % of the memory left, else the largest
+    multiple of 4,096 that does; the host figure is a positive byte count
+    where /proc/meminfo or the memory cgroup can be read."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    bench.load_package()
+    from croma_fp_b200 import config
+    cfg = config.config4()
+    nt = 4194304
+    per_rank = bench.e2e_tracers(cfg, nt, 3, 1, None)
+    assert per_rank == nt
+    assert bench.e2e_tracers(cfg, nt, 3, 1, 1.0e12) == nt
+    small = bench.e2e_tracers(cfg, nt, 3, 8, 196.0e9)
+    assert 4096 <= small < nt and small % 4096 == 0
+    per_tracer = 8 * (2 * 512 + 4 * 64 + 8 * 5 + 4 * 4)
+    assert small * per_tracer * 8 <= 0.6 * 196.0e9 < (small + 4096) * per_tracer * 8
+    assert bench.e2e_tracers(cfg, nt, 3, 8, 1.0e6) == 4096
+    avail = bench.host_bytes_available()
+    assert avail is None or avail > 0
