@@ -272,3 +272,18 @@ def test_series_refuses_gaps_and_tracer_ranges_outside_the_files(tmp_path):
     empty.mkdir()
     with pytest.raises(FileNotFoundError, match="no snapshot files"):
         histories.SnapshotSeries(str(empty), nb=128)
+
+
+@pytest.mark.skipif(not pyoracle.reference_available(128), reason="oracle/_ref not built")
+def test_nonpositive_density_refused_like_the_reference():
+    """A tracer with zero density: the reference's prepare_background_cell
+    fails on it (src/fp_shared_core.c:866-932 returns -1), and the
+    restatement refuses the block too (the device path reports -2 with the
+    tracer's fields zeroed, tests/test_gpu_histories.py)."""
+    raw = fixture_raw(1)
+    raw = {k: (v[:8].copy() if isinstance(v, np.ndarray) else v) for k, v in raw.items()}
+    raw["density"][2] = 0.0
+    with pytest.raises(RuntimeError, match="tracer 2"):
+        pyoracle.reference_background(raw, PRM)
+    with pytest.raises(RuntimeError, match="-2"):
+        pyoracle.background(raw, PRM)
